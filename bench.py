@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the finite-difference LLG hot path (H_eff + demag +
+RK4) on B200 through libmmcuda's C ABI.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c5|c1]
+                    [--impl native|reference]
+
+One JSON line on rank 0.  Metric: LLG cell-steps/s = cells x RK4 steps / s,
+whole job (N replicas of the mesh under torchrun: the path has no exchange
+step between meshes, so ranks run independent replicas, scaling "weak").
+
+Workloads (seeded synthetic inputs, numpy PCG64):
+  c2  256x256x64 cells, 2 nm: exchange A=1e-11, bulk DMI 3e-3, Ku=5e5 along z,
+      Ms=5.8e5, demag; random unit m (seed 102); alpha=0.1, gamma=2.211e5;
+      RK4 with dt = 5e-14 s (the default).
+  c5  1024x1024x16 cells, 3 nm: exchange A=1.3e-11, Ms=8e5, demag (padded
+      2048x2048x32); random unit m (seed 105); alpha=0.1, gamma=2.211e5.
+  c1  200x50x1, 2.5x2.5x3 nm: A=1.3e-11, Ms=8e5, demag, in-plane Zeeman
+      |B| <= 30 mT (seed 101); alpha=0.02, gamma=2.211e5, dt=1e-13.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "micromagnetic.jl_b200"))
+sys.path.insert(0, ROOT)
+
+MU0 = 4 * math.pi * 1e-7
+
+WORKLOADS = {
+    "c2": dict(nx=256, ny=256, nz=64, dx=2e-9, dy=2e-9, dz=2e-9, Ms=5.8e5, A=1e-11, Dbulk=3e-3, Ku=5e5,
+               axis=(0, 0, 1), demag=True, alpha=0.1, gamma=2.211e5, dt=5e-14, seed=102, zeeman=None),
+    "c5": dict(nx=1024, ny=1024, nz=16, dx=3e-9, dy=3e-9, dz=3e-9, Ms=8e5, A=1.3e-11, Dbulk=None, Ku=None,
+               axis=(0, 0, 1), demag=True, alpha=0.1, gamma=2.211e5, dt=5e-14, seed=105, zeeman=None),
+    "c1": dict(nx=200, ny=50, nz=1, dx=2.5e-9, dy=2.5e-9, dz=3e-9, Ms=8e5, A=1.3e-11, Dbulk=None, Ku=None,
+               axis=(0, 0, 1), demag=True, alpha=0.02, gamma=2.211e5, dt=1e-13, seed=101, zeeman="inplane30mT"),
+}
+# the CPU baseline times a bounded block of the same physics
+CPU_SAMPLE = {"c2": (128, 128, 32), "c5": (256, 256, 16), "c1": (200, 50, 1)}
+
+
+def synth_inputs(w, shape=None):
+    nx, ny, nz = shape or (w["nx"], w["ny"], w["nz"])
+    n = nx * ny * nz
+    rng = np.random.default_rng(w["seed"])
+    m = rng.standard_normal((n, 3))
+    m /= np.linalg.norm(m, axis=1, keepdims=True)
+    H = None
+    if w["zeeman"] == "inplane30mT":
+        r = 0.03 * math.sqrt(rng.uniform())
+        phi = rng.uniform(0, 2 * math.pi)
+        H = (r * math.cos(phi) / MU0, r * math.sin(phi) / MU0, 0.0)
+    return m.reshape(-1), H
+
+
+def setup_native(w, form, device):
+    from mmcuda import _lib
+
+    h = _lib.Handle(w["nx"], w["ny"], w["nz"], w["dx"], w["dy"], w["dz"], 0, form, device)
+    m, H = synth_inputs(w)
+    h.call("mm_set_Ms", None, w["Ms"])
+    h.set_m(m)
+    h.call("mm_set_llg", w["alpha"], w["gamma"], 1)
+    h.call("mm_add_exch", None, w["A"], w["A"], w["A"])
+    if w["Dbulk"]:
+        h.call("mm_add_dmi_bulk", w["Dbulk"], w["Dbulk"], w["Dbulk"])
+    if w["Ku"]:
+        h.call("mm_add_anis", None, w["Ku"], *w["axis"])
+    if H is not None:
+        h.call("mm_add_zeeman", None, *H)
+    if w["demag"]:
+        h.call("mm_add_demag", 0, 0, 0)
+    return h, m
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and "Active" in s[5 + i]
+                          and "Not" not in s[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline(wname, steps=1):
+    """FP64 oracle (CPU restatement of the reference path), all host threads,
+    on a bounded block of the workload's physics."""
+    from oracle.oracle import OracleSim, max_threads
+
+    w = WORKLOADS[wname]
+    shape = CPU_SAMPLE[wname]
+    nx, ny, nz = shape
+    m, H = synth_inputs(w, shape)
+    n = nx * ny * nz
+    s = OracleSim(nx, ny, nz, w["dx"], w["dy"], w["dz"])
+    s.set_Ms(w["Ms"])
+    s.set_m(m)
+    s.set_llg(w["alpha"], w["gamma"])
+    s.add_exch(Ax=w["A"], Ay=w["A"], Az=w["A"])
+    if w["Dbulk"]:
+        s.add_dmi_bulk(w["Dbulk"], w["Dbulk"], w["Dbulk"])
+    if w["Ku"]:
+        s.add_anis(np.full(n, w["Ku"]), w["axis"])
+    if H is not None:
+        s.add_zeeman(np.asarray(H))
+    if w["demag"]:
+        s.add_demag()
+    s.rk4(w["dt"], 1)  # warm-up (plans, pages)
+    t0 = time.perf_counter()
+    s.rk4(w["dt"], steps)
+    dt = time.perf_counter() - t0
+    return {"value": n * steps / dt, "unit": "cell-steps/s", "cores": max_threads(), "kind": "port",
+            "sample": f"{nx}x{ny}x{nz} block of the {wname} physics, FP64, {steps} RK4 step(s) after 1 warm-up, "
+                      f"{dt:.1f} s"}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0, None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return rank, ws, local, dist
+
+
+def measured_peak():
+    try:
+        p = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(wname, form_name):
+    """ncu DRAM bytes per launch of each kernel, from the committed summary."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        return d.get(f"{wname}/{form_name}", {})
+    except Exception:
+        return {}
+
+
+def run_reference(args):
+    rank, ws, local, dist = dist_init()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    wname = args.workload
+    w = WORKLOADS[wname]
+    vals = []
+    for _ in range(max(1, args.warmup // 3)):
+        cpu_baseline(wname, 1)
+    base = None
+    for _ in range(max(1, min(args.steps, 3))):
+        base = cpu_baseline(wname, 1)
+        vals.append(base["value"])
+    v = statistics.median(vals)
+    n = w["nx"] * w["ny"] * w["nz"]
+    line = {"metric": "LLG cell-steps/s (H_eff+demag+RK4)", "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
+            "steps": len(vals), "warmup": args.warmup, "ms_per_step": 1e3 * n / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy PCG64)",
+            "config": {"workload": f"{wname}: {w['nx']}x{w['ny']}x{w['nz']} RK4", "form": "fp64", "sample": base["sample"]},
+            "impl": "reference",
+            "cpu_baseline": {**base, "value": v},
+            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_native(args):
+    import torch
+
+    rank, ws, local, dist = dist_init()
+    device = local
+    torch.cuda.set_device(device)
+    from mmcuda import _lib
+
+    wname = args.workload
+    w = WORKLOADS[wname]
+    n = w["nx"] * w["ny"] * w["nz"]
+    dt = w["dt"]
+    forms = {"fp32": _lib.MM_FP32, "fp64": _lib.MM_FP64}
+    results = {}
+    for fname in ("fp32", "fp64"):
+        h, m0 = setup_native(w, forms[fname], device)
+        stream = torch.cuda.ExternalStream(h.stream(), device=device)
+        for _ in range(args.warmup):
+            h.call("mm_rk4_run", dt, 1)
+        h.call("mm_synchronize")
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(device) if fname == "fp32" else None
+        if sampler:
+            sampler.__enter__()
+        e0.record(stream)
+        h.call("mm_rk4_run", dt, args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        if sampler:
+            sampler.__exit__()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        ms = e0.elapsed_time(e1)
+        t = torch.tensor([ms], device=f"cuda:{device}")
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        res = {"ms_per_step": ms_max / args.steps, "value": ws * n * args.steps / (ms_max / 1e3),
+               "launches_per_step": h.rk4_launches(), "device_bytes": h.device_bytes()}
+        if sampler:
+            res["clocks"] = sampler.summary()
+        # per-kernel CUDA-event timing on the handle's stream (same kernels as the step)
+        kern = {}
+        for kid, kname in enumerate(_lib.KERNELS):
+            kms, kb = h.kernel_time(kid, reps=10)
+            if kb > 0:
+                kern[kname] = {"ms": kms, "alg_bytes": kb, "GBps": kb / (kms * 1e6) if kms > 0 else None}
+        res["kernels"] = kern
+        if fname == "fp32":
+            # end to end through the public API with host buffers: per step,
+            # H2D of m from pinned memory, one RK4 step, D2H of m
+            pin_in = torch.from_numpy(m0.copy()).pin_memory()
+            pin_out = torch.empty(3 * n, dtype=torch.float64).pin_memory()
+            pin_in_p = ctypes.cast(pin_in.data_ptr(), ctypes.POINTER(ctypes.c_double))
+            pin_out_p = ctypes.cast(pin_out.data_ptr(), ctypes.POINTER(ctypes.c_double))
+            k2 = max(3, args.steps // 10)
+            for _ in range(2):
+                h.call("mm_set_m", pin_in_p)
+                h.call("mm_rk4_run", dt, 1)
+                h.call("mm_get_m", pin_out_p)
+            if dist is not None:
+                dist.barrier()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(k2):
+                h.call("mm_set_m", pin_in_p)
+                h.call("mm_rk4_run", dt, 1)
+                h.call("mm_get_m", pin_out_p)
+            e1.record(stream)
+            e1.synchronize()
+            t = torch.tensor([e0.elapsed_time(e1)], device=f"cuda:{device}")
+            if dist is not None:
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            res["e2e"] = {"value": ws * n * k2 / (float(t.item()) / 1e3), "unit": "cell-steps/s",
+                          "h2d_bytes_per_step": 8 * 3 * n, "d2h_bytes_per_step": 8 * 3 * n, "steps": k2}
+        results[fname] = res
+        h.close()
+        del stream
+    if rank == 0:
+        r = results["fp32"]
+        peak, peak_kind = measured_peak()
+        kern = {k: v for k, v in r["kernels"].items() if k != "rk4_step"}
+        # dominant kernel: largest time share of one RK4 step (4 launches of each)
+        dom = max(kern, key=lambda k: kern[k]["ms"])
+        traffic = profiled_traffic(wname, "fp32").get(dom)
+        ach = kern[dom]["alg_bytes"] / (kern[dom]["ms"] * 1e-3) / 1e9
+        step = r["kernels"].get("rk4_step", {})
+        line = {
+            "metric": "LLG cell-steps/s (H_eff+demag+RK4)",
+            "value": r["value"], "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy PCG64)",
+            "config": {"workload": f"{wname}: {w['nx']}x{w['ny']}x{w['nz']} cells, exch"
+                                   + (" + bulk DMI" if w["Dbulk"] else "") + (" + anis" if w["Ku"] else "")
+                                   + (" + zeeman" if w["zeeman"] else "") + " + demag, RK4 dt=%g" % dt,
+                       "form": "fp32 (compensated RK state; fp64 tensor/energies)",
+                       "parallelism": f"replicas x{ws}", "l2": "working set > 126 MB L2 (inputs larger than L2)"},
+            "e2e": r["e2e"],
+            "gpu_launches": r["launches_per_step"] * args.steps,
+            "fp64": {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
+                     "fp32_over_fp64": r["value"] / results["fp64"]["value"]},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "peak_kind": peak_kind,
+                         "traffic": traffic},
+            "step_roofline": {"alg_bytes": step.get("alg_bytes"), "ms": step.get("ms"),
+                              "GBps": step.get("GBps"), "frac": (step.get("GBps") or 0) / peak},
+            "kernels": {k: {"ms": round(v["ms"], 5), "GBps": round(v["GBps"] or 0, 1)} for k, v in r["kernels"].items()},
+            "clocks": r.get("clocks"),
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(wname, 1)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_native(args)
+
+
+if __name__ == "__main__":
+    main()

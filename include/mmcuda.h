@@ -1,0 +1,181 @@
+/*
+ * mmcuda.h -- C ABI of libmmcuda.so, a B200 (sm_100a) implementation of the
+ * MicroMagnetic.jl finite-difference hot path: effective field (exchange,
+ * bulk / interfacial DMI, uniaxial anisotropy, Zeeman, FFT demag), LLG
+ * right-hand side, RK4 and Dormand-Prince integration, steepest-descent relax.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  Host arrays are float64, cell id
+ *    (k*ny + j)*nx + i with x fastest; vector fields are AoS
+ *    [x1, y1, z1, x2, ...] exactly like MicroMagnetic.jl's `sim.spin` /
+ *    `sim.field` (src/micro/mesh.jl:24-29).
+ *  - A handle owns its device memory and a CUDA stream; the state stays on
+ *    the device between calls.  Calls on one handle must come from one host
+ *    thread at a time.  Compute calls are asynchronous unless they return
+ *    data to the host; mm_synchronize() waits for the handle's stream.
+ *  - Every function returns MM_OK (0) or a negative mm_status; no exception
+ *    crosses the ABI.  mm_last_error() gives the message of the calling
+ *    thread's last failure.
+ *  - form MM_FP64: state, fields and FFTs in FP64.  MM_FP32: state and
+ *    fields in FP32 with the integrator state kept compensated
+ *    (hi + lo), FP64 for the Newell tensor assembly, the Dormand-Prince
+ *    error norm and the energy reductions.
+ */
+#ifndef MMCUDA_H
+#define MMCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MMCUDA_ABI_VERSION 1
+
+typedef struct mm_handle mm_handle;
+
+enum mm_status {
+  MM_OK = 0,
+  MM_ERR_ARG = -1,         /* bad argument / size */
+  MM_ERR_CUDA = -2,        /* CUDA runtime failure */
+  MM_ERR_NAN = -3,         /* NaN in inputs or in the integration */
+  MM_ERR_NOCONVERGE = -4,  /* > 50 rejected attempts in one adaptive step */
+  MM_ERR_TIMEOUT = -5,     /* bounded device wait ran out */
+  MM_ERR_STATE = -6,       /* call out of order (e.g. no Ms set) */
+  MM_ERR_UNSUPPORTED = -7  /* valid in the reference, not on this path */
+};
+
+enum mm_form { MM_FP64 = 0, MM_FP32 = 1 };
+
+/* interaction terms; bit i of a term mask selects term i */
+enum mm_term {
+  MM_TERM_ZEEMAN = 0,
+  MM_TERM_EXCH = 1,
+  MM_TERM_DMI_BULK = 2,
+  MM_TERM_DMI_INTERFACIAL = 3,
+  MM_TERM_ANIS = 4,
+  MM_TERM_DEMAG = 5,
+  MM_NTERMS = 6
+};
+
+enum mm_driver { MM_DRIVER_SD = 0, MM_DRIVER_LLG = 1 };
+
+/* FDMesh(; dx, dy, dz, nx, ny, nz, pbc)  src/micro/mesh.jl:69-98 */
+typedef struct {
+  int32_t nx, ny, nz;
+  double dx, dy, dz;
+  int32_t pbc; /* bit0 x, bit1 y, bit2 z periodic */
+} mm_mesh_desc;
+
+/* Adaptive integrator statistics, cf. get_statistics
+ * src/integrator/adaptive_rk.jl:188-192 */
+typedef struct {
+  double t, step, step_next;
+  int64_t nsteps, nfevals, attempts, rejected;
+  int32_t status; /* 0 ok, 1 NaN, 2 too many attempts */
+} mm_stats;
+
+int mm_abi_version(void);
+/* Message of the calling thread's last failing call (always NUL-terminated). */
+int mm_last_error(char* buf, size_t n);
+
+/* Sim(mesh)  src/sim.jl:48-107 (state + driver storage on `device`) */
+int mm_create(const mm_mesh_desc* mesh, int form, int device, mm_handle** out);
+int mm_destroy(mm_handle* h);
+/* CUDA stream (cudaStream_t) the handle launches on. */
+int mm_get_stream(mm_handle* h, void** stream);
+int mm_synchronize(mm_handle* h);
+/* Bytes of device memory held by the handle. */
+int mm_device_bytes(mm_handle* h, size_t* bytes);
+
+/* set_Ms(sim, Ms)  src/sim.jl:129-143 -- A/m; Ms == NULL uses Ms_uniform */
+int mm_set_Ms(mm_handle* h, const double* Ms, double Ms_uniform);
+/* init_m0 copy-in  src/sim.jl:278-309 (the caller normalises / zeroes) */
+int mm_set_m(mm_handle* h, const double* m_aos);
+/* sim.spin copy-out */
+int mm_get_m(mm_handle* h, double* m_aos);
+/* set_pinning  src/sim.jl (sim.pins): NULL clears */
+int mm_set_pins(mm_handle* h, const uint8_t* pins);
+/* LLG driver parameters  src/driver.jl:15-21 (alpha, gamma, precession) */
+int mm_set_llg(mm_handle* h, double alpha, double gamma, int precession);
+
+/* add_zeeman / update_zeeman  src/micro/add_field.jl:11-48: H in A/m,
+ * AoS 3N or NULL for the uniform (Hx, Hy, Hz).  add accumulates, update replaces. */
+int mm_add_zeeman(mm_handle* h, const double* H_aos, double Hx, double Hy, double Hz);
+int mm_update_zeeman(mm_handle* h, const double* H_aos, double Hx, double Hy, double Hz);
+/* add_exch  src/micro/add_field.jl:233-263: A (J/m) per cell, or NULL for the
+ * uniform / per-axis (Ax, Ay, Az) of UniformExchange */
+int mm_add_exch(mm_handle* h, const double* A, double Ax, double Ay, double Az);
+/* add_dmi(type="bulk")  src/micro/add_field.jl:299-326 (uniform Dx, Dy, Dz, J/m^2) */
+int mm_add_dmi_bulk(mm_handle* h, double Dx, double Dy, double Dz);
+/* add_dmi(type="interfacial")  src/micro/add_field.jl:327-335 */
+int mm_add_dmi_interfacial(mm_handle* h, const double* D, double D_uniform);
+/* add_anis  src/micro/add_field.jl:430-465: Ku (J/m^3) per cell or uniform; axis normalised */
+int mm_add_anis(mm_handle* h, const double* Ku, double Ku_uniform, double ax, double ay, double az);
+/* add_demag(sim; Nx, Ny, Nz)  src/micro/add_field.jl:403-419 -> init_demag
+ * src/micro/demag.jl:30-100 (FP64 Newell tensor assembled on the device) */
+int mm_add_demag(mm_handle* h, int Nx, int Ny, int Nz);
+/* Same, with a caller-supplied real-space tensor (6 x N, order xx yy zz xy
+ * xz yz, dimensionless) in place of the Newell assembly. */
+int mm_add_demag_tensor(mm_handle* h, const double* tensor_6N);
+
+/* effective_field(sim, spin, t)  src/micro/field.jl:496-505 -> H_aos (3N, A/m) */
+int mm_effective_field(mm_handle* h, double* H_aos);
+/* Field (3N) and per-cell energy (N) of one term (term.field / term.energy
+ * after effective_field(term, sim, spin, t), src/micro/field.jl:1-242);
+ * either output may be NULL. */
+int mm_term_field(mm_handle* h, int term, double* field_aos, double* energy_cells);
+/* compute_system_energy  src/micro/field.jl:520-536: per-term sums (J) in
+ * FP64, indexed by mm_term; either output may be NULL. */
+int mm_energy(mm_handle* h, double* per_term, double* total);
+/* llg_call_back(sim, dm_dt, spin, t)  src/llg/llg.jl:45-59 -> dm/dt AoS */
+int mm_llg_rhs(mm_handle* h, double* dmdt_aos);
+/* average_m(sim) */
+int mm_average_m(mm_handle* h, double* m3);
+
+/* advance_step(sim, ::RungeKutta) x nsteps  src/integrator/rk.jl:23-52 */
+int mm_rk4_run(mm_handle* h, double dt, int64_t nsteps);
+/* RungeKutta t and nsteps (t = nsteps * dt) */
+int mm_rk4_state(mm_handle* h, double* t, int64_t* nsteps);
+
+/* Dormand-Prince (DOPRI54) tolerance, default 1e-6  src/driver.jl:126,134 */
+int mm_dopri_set_tol(mm_handle* h, double tol);
+/* run_until(sim, t_end)  src/sim.jl:547-574 with integrate_to_time
+ * src/integrator/adaptive_rk.jl:168-186 (step control on the device) */
+int mm_run_until(mm_handle* h, double t_end, mm_stats* stats);
+/* advance_step(sim, ::AdaptiveRK)  src/integrator/adaptive_rk.jl:93-148 */
+int mm_advance_step(mm_handle* h, mm_stats* stats);
+/* Reset the adaptive integrator (t = 0, step sizes and counters cleared). */
+int mm_dopri_reset(mm_handle* h);
+
+/* relax(sim; max_steps, stopping_dmdt)  src/sim.jl:392-490 with the SD
+ * driver (src/sd.jl:9-98) or the LLG driver with Dormand-Prince */
+int mm_relax(mm_handle* h, int driver, int64_t max_steps, double stopping_dmdt, int64_t* steps_done,
+             double* max_dmdt);
+
+/* ---- measurement hooks (the reference times host sections with TimerOutputs,
+ * src/MicroMagnetic.jl:7-13; these time device kernels with CUDA events) ---- */
+enum mm_kernel {
+  MM_K_DEMAG_FWD_X = 0,  /* r2c x pass (m*mu0*Ms -> X) */
+  MM_K_DEMAG_FWD_Y = 1,  /* forward y pass (3-D meshes) */
+  MM_K_DEMAG_CONV = 2,   /* z (3-D) or y (films) pass with the tensor product */
+  MM_K_DEMAG_INV_Y = 3,  /* inverse y pass (3-D meshes) */
+  MM_K_DEMAG_INV_X = 4,  /* c2r x pass (-> H_demag) */
+  MM_K_RK4_STAGE = 5,    /* fused H_eff + LLG + RK4 stage-2 update */
+  MM_K_RK4_STEP = 6,     /* one whole RK4 step (graph) */
+  MM_NKERNELS = 7
+};
+/* Launches `kernel` `reps` times on the handle's stream after one warm-up and
+ * reports the mean CUDA-event duration per launch (ms) and the algorithmic
+ * HBM bytes one launch must move (compulsory reads + writes).  Kernels that
+ * a handle does not use report 0. */
+int mm_kernel_time(mm_handle* h, int kernel, int reps, double* ms_per_launch, double* alg_bytes);
+/* Number of kernel launches in one RK4 step. */
+int mm_rk4_launches_per_step(mm_handle* h, int* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MMCUDA_H */

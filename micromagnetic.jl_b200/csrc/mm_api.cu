@@ -1,0 +1,1023 @@
+// mm_api.cu -- handle/engine and the extern "C" ABI of libmmcuda.so.
+//
+// A handle (mm_handle) owns an Engine<R> (R = double for MM_FP64, float for
+// MM_FP32): the device state, the term parameters, the demag plan and the
+// integrator state.  Integration loops are captured once into CUDA graphs
+// (one RK4 step; one Dormand-Prince attempt with a device-side step-size
+// controller) and replayed; the host only synchronises between batches.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mmcuda.h"
+#include "mm_demag.cuh"
+#include "mm_field.cuh"
+#include "mm_integ.cuh"
+
+namespace mm {
+
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define MM_CUDA(call)                                                                          \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return fail(MM_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename R>
+__global__ void k_zeeman_accumulate(const double* __restrict__ aos, R* __restrict__ Hz, int64_t N, int replace) {
+  const int64_t I = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (I >= N) return;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const R v = static_cast<R>(aos[3 * I + c]);
+    Hz[c * N + I] = replace ? v : Hz[c * N + I] + v;
+  }
+}
+
+template <typename R>
+__global__ void k_to_double(const R* __restrict__ a, double* __restrict__ b, int64_t n) {
+  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (i < n) b[i] = static_cast<double>(a[i]);
+}
+
+class EngineBase {
+ public:
+  virtual ~EngineBase() = default;
+  virtual int set_Ms(const double* Ms, double uni) = 0;
+  virtual int set_m(const double* m) = 0;
+  virtual int get_m(double* m) = 0;
+  virtual int set_pins(const uint8_t* p) = 0;
+  virtual int set_llg(double alpha, double gamma, int prec) = 0;
+  virtual int zeeman(const double* H, double hx, double hy, double hz, bool replace) = 0;
+  virtual int add_exch(const double* A, double ax, double ay, double az) = 0;
+  virtual int add_dmi_bulk(double dx, double dy, double dz) = 0;
+  virtual int add_dmi_interfacial(const double* D, double uni) = 0;
+  virtual int add_anis(const double* Ku, double uni, double ax, double ay, double az) = 0;
+  virtual int add_demag(int Nx, int Ny, int Nz, const double* T6N_host) = 0;
+  virtual int effective_field(double* H) = 0;
+  virtual int term_field(int term, double* f, double* e) = 0;
+  virtual int energy(double* per, double* total) = 0;
+  virtual int llg_rhs(double* out) = 0;
+  virtual int average_m(double* m3) = 0;
+  virtual int rk4_run(double dt, int64_t n) = 0;
+  virtual int rk4_state(double* t, int64_t* n) = 0;
+  virtual int dopri_tol(double tol) = 0;
+  virtual int run_until(double t_end, mm_stats* st) = 0;
+  virtual int advance_step(mm_stats* st) = 0;
+  virtual int dopri_reset() = 0;
+  virtual int relax(int driver, int64_t max_steps, double stop, int64_t* steps, double* max_dmdt) = 0;
+  virtual int kernel_time(int kernel, int reps, double* ms, double* bytes) = 0;
+  virtual int rk4_launches() const = 0;
+  virtual cudaStream_t stream() const = 0;
+  virtual size_t device_bytes() const = 0;
+  int device = 0;
+};
+
+template <typename R>
+class Engine : public EngineBase {
+ public:
+  static constexpr bool kF32 = sizeof(R) == 4;
+
+  ~Engine() override {
+    cudaSetDevice(device);
+    if (rk_graph) cudaGraphExecDestroy(rk_graph);
+    if (dp_graph) cudaGraphExecDestroy(dp_graph);
+    demag.reset();
+    for (void* p : allocs_) cudaFree(p);
+    if (st_) cudaStreamDestroy(st_);
+  }
+
+  int init(const mm_mesh_desc& d, int dev) {
+    device = dev;
+    nx = d.nx; ny = d.ny; nz = d.nz; pbc = d.pbc;
+    dx = d.dx; dy = d.dy; dz = d.dz;
+    N = static_cast<int64_t>(nx) * ny * nz;
+    MM_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    const int nb = stage_blocks(N);
+    int rc = 0;
+    if ((rc = alloc(m, 3 * N)) || (kF32 && (rc = alloc(m_lo, 3 * N))) || (rc = alloc(Ms, N)) ||
+        (rc = alloc(nbm, N)) || (rc = alloc(yA, 3 * N)) || (rc = alloc(work, 3 * N)) ||
+        (rc = alloc(stage64, 3 * N)) || (rc = alloc(partials, static_cast<int64_t>(nb) * kNTerms + 1024)) ||
+        (rc = alloc(scal, 64)))
+      return rc;
+    return MM_OK;
+  }
+
+  cudaStream_t stream() const override { return st_; }
+  size_t device_bytes() const override { return bytes_ + (demag ? demag->device_bytes() : 0); }
+
+  // ------------------------------------------------------------ setup --
+  int set_Ms(const double* Msh, double uni) override {
+    if (Msh) {
+      for (int64_t i = 0; i < N; ++i)
+        if (std::isnan(Msh[i])) return fail(MM_ERR_NAN, "NaN is given by the input Ms!");
+      MM_CUDA(cudaMemcpyAsync(stage64, Msh, sizeof(double) * N, cudaMemcpyHostToDevice, st_));
+    } else {
+      if (std::isnan(uni)) return fail(MM_ERR_NAN, "NaN is given by the input Ms!");
+      std::vector<double> tmp(N, uni);
+      MM_CUDA(cudaMemcpyAsync(stage64, tmp.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st_));
+      MM_CUDA(cudaStreamSynchronize(st_));
+    }
+    // stored as mu0*Ms in Tesla (src/sim.jl:138): Ms .*= mu_0 in FP64 then cast
+    launch_scalar_to_R<R>(stage64, Ms, N, kMu0, st_);
+    launch_nbmask<R>(nx, ny, nz, pbc, Ms, nbm, st_);
+    MM_CUDA(cudaStreamSynchronize(st_));
+    ms_set = true;
+    ++version;
+    return MM_OK;
+  }
+
+  int set_m(const double* mh) override {
+    // NaN check of init_m0 (src/sim.jl:295-297), done by the conversion kernel
+    int* flag = reinterpret_cast<int*>(scal + 63);
+    MM_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st_));
+    MM_CUDA(cudaMemcpyAsync(stage64, mh, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st_));
+    launch_aos_to_soa<R>(stage64, m, m_lo, N, flag, st_);
+    int hflag = 0;
+    MM_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    MM_CUDA(cudaStreamSynchronize(st_));
+    if (hflag) return fail(MM_ERR_NAN, "NaN is given by the input m0!");
+    return MM_OK;
+  }
+
+  int get_m(double* mh) override {
+    launch_soa_to_aos<R>(m, m_lo, stage64, N, st_);
+    MM_CUDA(cudaMemcpyAsync(mh, stage64, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st_));
+    MM_CUDA(cudaStreamSynchronize(st_));
+    return MM_OK;
+  }
+
+  int set_pins(const uint8_t* p) override {
+    if (!p) {
+      pins_on = false;
+      ++version;
+      return MM_OK;
+    }
+    int rc;
+    if (!pins && (rc = alloc(pins, N))) return rc;
+    MM_CUDA(cudaMemcpyAsync(pins, p, N, cudaMemcpyHostToDevice, st_));
+    MM_CUDA(cudaStreamSynchronize(st_));
+    pins_on = true;
+    ++version;
+    return MM_OK;
+  }
+
+  int set_llg(double a, double g, int prec) override {
+    alpha = a;
+    gamma = g;
+    precession = prec;
+    ++version;
+    return MM_OK;
+  }
+
+  int upload_R(const double* h, R*& dst, int64_t n) {
+    int rc;
+    if (!dst && (rc = alloc(dst, n))) return rc;
+    MM_CUDA(cudaMemcpyAsync(stage64, h, sizeof(double) * n, cudaMemcpyHostToDevice, st_));
+    launch_scalar_to_R<R>(stage64, dst, n, 1.0, st_);
+    MM_CUDA(cudaStreamSynchronize(st_));
+    return MM_OK;
+  }
+
+  // an array whose entries are all equal is kept as a scalar
+  static bool uniform(const double* a, int64_t n, double& v) {
+    v = a[0];
+    for (int64_t i = 1; i < n; ++i)
+      if (a[i] != v) return false;
+    return true;
+  }
+
+  int zeeman(const double* H, double hx, double hy, double hz, bool replace) override {
+    if (replace) {
+      hz_uni[0] = hz_uni[1] = hz_uni[2] = 0.0;
+      hz_arr = false;
+    }
+    if (H) {
+      int rc;
+      if (!Hz && (rc = alloc(Hz, 3 * N))) return rc;
+      MM_CUDA(cudaMemcpyAsync(stage64, H, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st_));
+      k_zeeman_accumulate<R><<<stage_blocks(N), 256, 0, st_>>>(stage64, Hz, N, hz_arr ? 0 : 1);
+      MM_CUDA(cudaStreamSynchronize(st_));
+      hz_arr = true;
+    } else {
+      hz_uni[0] += hx;
+      hz_uni[1] += hy;
+      hz_uni[2] += hz;
+    }
+    mask |= TB_ZEEMAN;
+    ++version;
+    return MM_OK;
+  }
+
+  int add_exch(const double* Ah, double ax, double ay, double az) override {
+    if (mask & TB_EXCH) return fail(MM_ERR_UNSUPPORTED, "one exchange term per handle");
+    double v;
+    if (Ah && !uniform(Ah, N, v)) {
+      int rc;
+      if ((rc = upload_R(Ah, A, N))) return rc;
+      ex_spatial = true;
+    } else {
+      if (Ah) ax = ay = az = v;
+      ex_A[0] = ax; ex_A[1] = ay; ex_A[2] = az;
+      ex_spatial = false;
+    }
+    mask |= TB_EXCH;
+    ++version;
+    return MM_OK;
+  }
+
+  int add_dmi_bulk(double Dx, double Dy, double Dz) override {
+    if (mask & TB_DMI_BULK) return fail(MM_ERR_UNSUPPORTED, "one bulk DMI term per handle");
+    bd[0] = Dx; bd[1] = Dy; bd[2] = Dz;
+    mask |= TB_DMI_BULK;
+    ++version;
+    return MM_OK;
+  }
+
+  int add_dmi_interfacial(const double* Dh, double uni) override {
+    if (mask & TB_DMI_INTERFACIAL) return fail(MM_ERR_UNSUPPORTED, "one interfacial DMI term per handle");
+    double v;
+    if (Dh && !uniform(Dh, N, v)) {
+      int rc;
+      if ((rc = upload_R(Dh, D, N))) return rc;
+      id_spatial = true;
+    } else {
+      id_D = Dh ? v : uni;
+      id_spatial = false;
+    }
+    mask |= TB_DMI_INTERFACIAL;
+    ++version;
+    return MM_OK;
+  }
+
+  int add_anis(const double* Kh, double uni, double ax, double ay, double az) override {
+    if (mask & TB_ANIS) return fail(MM_ERR_UNSUPPORTED, "one uniaxial anisotropy term per handle");
+    const double lt = std::sqrt(ax * ax + ay * ay + az * az);
+    if (!(lt > 0)) return fail(MM_ERR_ARG, "anisotropy axis has zero length");
+    // axis normalised at add time (src/micro/add_field.jl:441-444)
+    an_u[0] = ax / lt; an_u[1] = ay / lt; an_u[2] = az / lt;
+    double v;
+    if (Kh && !uniform(Kh, N, v)) {
+      int rc;
+      if ((rc = upload_R(Kh, Ku, N))) return rc;
+      an_spatial = true;
+    } else {
+      an_K = Kh ? v : uni;
+      an_spatial = false;
+    }
+    mask |= TB_ANIS;
+    ++version;
+    return MM_OK;
+  }
+
+  int add_demag(int Nx, int Ny, int Nz, const double* T6N_host) override {
+    if (mask & TB_DEMAG) return fail(MM_ERR_UNSUPPORTED, "one demag term per handle");
+    if (Nx < 0 || Ny < 0 || Nz < 0) return fail(MM_ERR_ARG, "macro-PBC image counts must be >= 0");
+    auto plan = std::make_unique<DemagPlan<R>>();
+    char msg[256] = {0};
+    int rc = plan->init(nx, ny, nz, st_, msg, sizeof(msg));
+    if (rc == -1) return fail(MM_ERR_ARG, "%s", msg);
+    if (rc) return fail(MM_ERR_CUDA, "demag plan allocation failed (%d)", rc);
+    double* T = nullptr;
+    MM_CUDA(cudaMalloc(&T, sizeof(double) * 6 * N));
+    if (T6N_host) {
+      cudaMemcpyAsync(T, T6N_host, sizeof(double) * 6 * N, cudaMemcpyHostToDevice, st_);
+    } else {
+      newell_tensor_device(nx, ny, nz, dx, dy, dz, Nx, Ny, Nz, T, st_);
+    }
+    rc = plan->set_tensor(T, st_);
+    cudaStreamSynchronize(st_);
+    cudaFree(T);
+    if (rc) return fail(MM_ERR_CUDA, "demag tensor assembly failed: %s", cudaGetErrorString(static_cast<cudaError_t>(rc)));
+    if (!Hd && (rc = alloc(Hd, 3 * N))) return rc;
+    demag = std::move(plan);
+    mask |= TB_DEMAG;
+    ++version;
+    MM_CUDA(cudaGetLastError());
+    return MM_OK;
+  }
+
+  FieldArgs<R> fargs(unsigned msk) const {
+    FieldArgs<R> a{};
+    a.nx = nx; a.ny = ny; a.nz = nz; a.pbc = pbc; a.N = N;
+    a.V = static_cast<R>(dx * dy * dz);
+    a.Ms = Ms; a.nbm = nbm;
+    a.mask = msk & mask;
+    if (ex_spatial) {
+      a.ex_x = static_cast<R>(2.0 / (dx * dx)); a.ex_y = static_cast<R>(2.0 / (dy * dy)); a.ex_z = static_cast<R>(2.0 / (dz * dz));
+      a.A = A;
+    } else {
+      a.ex_x = static_cast<R>(2 * ex_A[0] / (dx * dx));
+      a.ex_y = static_cast<R>(2 * ex_A[1] / (dy * dy));
+      a.ex_z = static_cast<R>(2 * ex_A[2] / (dz * dz));
+      a.A = nullptr;
+    }
+    a.bd_x = static_cast<R>(bd[0] / dx); a.bd_y = static_cast<R>(bd[1] / dy); a.bd_z = static_cast<R>(bd[2] / dz);
+    a.D_uni = static_cast<R>(id_D);
+    a.D = id_spatial ? D : nullptr;
+    a.id_x = static_cast<R>(1.0 / dx); a.id_y = static_cast<R>(1.0 / dy);
+    a.Ku_uni = static_cast<R>(an_K);
+    a.Ku = an_spatial ? Ku : nullptr;
+    a.ux = static_cast<R>(an_u[0]); a.uy = static_cast<R>(an_u[1]); a.uz = static_cast<R>(an_u[2]);
+    a.hz_x = static_cast<R>(hz_uni[0]); a.hz_y = static_cast<R>(hz_uni[1]); a.hz_z = static_cast<R>(hz_uni[2]);
+    a.Hz = hz_arr ? Hz : nullptr;
+    a.Hd = Hd;
+    a.alpha = static_cast<R>(alpha);
+    a.gamma = static_cast<R>(gamma);
+    a.precession = precession;
+    a.pins = pins_on ? pins : nullptr;
+    return a;
+  }
+
+  // ------------------------------------------------------ evaluation --
+  void enqueue_field(const R* y, R* out, unsigned msk, R* ecell) {
+    if ((msk & mask & TB_DEMAG) && demag) demag->apply(y, Ms, Hd, st_);
+    StageArgs<R> s{};
+    s.out = out;
+    s.ecell = ecell;
+    launch_stage<R>(SM_FIELD, fargs(msk), y, s, st_);
+  }
+
+  void enqueue_rhs(const R* y, R* out) {
+    if ((mask & TB_DEMAG) && demag) demag->apply(y, Ms, Hd, st_);
+    StageArgs<R> s{};
+    s.out = out;
+    launch_stage<R>(SM_RHS, fargs(~0u), y, s, st_);
+  }
+
+  int need_ms() const { return ms_set ? MM_OK : fail(MM_ERR_STATE, "set_Ms must be called first"); }
+
+  int download_aos(const R* soa, double* out) {
+    launch_soa_to_aos<R>(soa, nullptr, stage64, N, st_);
+    MM_CUDA(cudaMemcpyAsync(out, stage64, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st_));
+    MM_CUDA(cudaStreamSynchronize(st_));
+    return MM_OK;
+  }
+
+  int effective_field(double* H) override {
+    if (int rc = need_ms()) return rc;
+    enqueue_field(m, work, ~0u, nullptr);
+    MM_CUDA(cudaGetLastError());
+    if (!H) return MM_OK;
+    return download_aos(work, H);
+  }
+
+  int term_field(int term, double* f, double* e) override {
+    if (int rc = need_ms()) return rc;
+    if (term < 0 || term >= kNTerms) return fail(MM_ERR_ARG, "bad term index %d", term);
+    if (!(mask & (1u << term))) return fail(MM_ERR_ARG, "term %d was not added", term);
+    int rc;
+    if (!ecell && (rc = alloc(ecell, N))) return rc;
+    enqueue_field(m, work, 1u << term, ecell);
+    MM_CUDA(cudaGetLastError());
+    if (e) {
+      k_to_double<R><<<stage_blocks(N), 256, 0, st_>>>(ecell, stage64, N);
+      MM_CUDA(cudaMemcpyAsync(e, stage64, sizeof(double) * N, cudaMemcpyDeviceToHost, st_));
+      MM_CUDA(cudaStreamSynchronize(st_));
+    }
+    if (f) return download_aos(work, f);
+    return MM_OK;
+  }
+
+  int energy(double* per, double* total) override {
+    if (int rc = need_ms()) return rc;
+    if ((mask & TB_DEMAG) && demag) demag->apply(m, Ms, Hd, st_);
+    StageArgs<R> s{};
+    s.partials = partials;
+    launch_stage<R>(SM_ENERGY, fargs(~0u), m, s, st_);
+    launch_reduce_sum(partials, stage_blocks(N), kNTerms, scal, st_);
+    double e[kNTerms];
+    MM_CUDA(cudaMemcpyAsync(e, scal, sizeof(e), cudaMemcpyDeviceToHost, st_));
+    MM_CUDA(cudaStreamSynchronize(st_));
+    double t = 0.0;
+    for (int i = 0; i < kNTerms; ++i) {
+      if (!(mask & (1u << i))) e[i] = 0.0;
+      t += e[i];
+      if (per) per[i] = e[i];
+    }
+    if (total) *total = t;
+    return MM_OK;
+  }
+
+  int llg_rhs(double* out) override {
+    if (int rc = need_ms()) return rc;
+    enqueue_rhs(m, work);
+    MM_CUDA(cudaGetLastError());
+    return download_aos(work, out);
+  }
+
+  int average_m(double* m3) override {
+    launch_average_m<R>(m, m_lo, N, partials, scal, st_);
+    double s[3];
+    MM_CUDA(cudaMemcpyAsync(s, scal, sizeof(s), cudaMemcpyDeviceToHost, st_));
+    MM_CUDA(cudaStreamSynchronize(st_));
+    for (int c = 0; c < 3; ++c) m3[c] = s[c] / static_cast<double>(N);
+    return MM_OK;
+  }
+
+  // -------------------------------------------------------------- RK4 --
+  void enqueue_rk4_step(double h) {
+    const FieldArgs<R> fa = fargs(~0u);
+    for (int s = 1; s <= 4; ++s) {
+      // stage inputs ping-pong so that no kernel overwrites a field it reads
+      const R* yin = s == 1 ? m : (s == 3 ? yB : yA);
+      R* ynext = (s == 2) ? yB : yA;
+      if ((mask & TB_DEMAG) && demag) demag->apply(yin, Ms, Hd, st_);
+      StageArgs<R> sa{};
+      sa.m = m;
+      sa.m_lo = m_lo;
+      sa.acc = acc;
+      sa.ynext = ynext;
+      sa.h = h;
+      sa.stage = s;
+      launch_stage<R>(SM_RK4, fa, yin, sa, st_);
+    }
+  }
+
+  int rk4_run(double dt, int64_t n) override {
+    if (int rc = need_ms()) return rc;
+    if (n < 0 || !(dt > 0)) return fail(MM_ERR_ARG, "rk4: need dt > 0 and nsteps >= 0");
+    int rc;
+    if (!acc && (rc = alloc(acc, 3 * N))) return rc;
+    if (!yB && (rc = alloc(yB, 3 * N))) return rc;
+    if (!rk_graph || rk_dt != dt || rk_version != version) {
+      if (rk_graph) cudaGraphExecDestroy(rk_graph);
+      rk_graph = nullptr;
+      cudaGraph_t g;
+      MM_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+      enqueue_rk4_step(dt);
+      MM_CUDA(cudaStreamEndCapture(st_, &g));
+      MM_CUDA(cudaGraphInstantiate(&rk_graph, g, 0));
+      cudaGraphDestroy(g);
+      rk_dt = dt;
+      rk_version = version;
+    }
+    for (int64_t i = 0; i < n; ++i) MM_CUDA(cudaGraphLaunch(rk_graph, st_));
+    rk_n += n;
+    rk_t = static_cast<double>(rk_n) * dt;  // integrator.t = nsteps * h (rk.jl:50)
+    MM_CUDA(cudaGetLastError());
+    return MM_OK;
+  }
+
+  int rk4_state(double* t, int64_t* n) override {
+    if (t) *t = rk_t;
+    if (n) *n = rk_n;
+    return MM_OK;
+  }
+
+  int rk4_launches() const override {
+    const int passes = ((mask & TB_DEMAG) && demag) ? demag->launches_per_apply() : 0;
+    return 4 * (passes + 1);
+  }
+
+  // Compulsory bytes of one fused RK4 stage-2 kernel: y, Ms, [H_demag], m_n, acc
+  // read; acc and the next stage input written (the canonical schedule), plus
+  // one word per spatially varying parameter array and the Zeeman array.
+  double stage_bytes() const {
+    double words = 16.0 + (((mask & TB_DEMAG) && demag) ? 3.0 : 0.0);
+    if ((mask & TB_EXCH) && ex_spatial) words += 1.0;
+    if ((mask & TB_DMI_INTERFACIAL) && id_spatial) words += 1.0;
+    if ((mask & TB_ANIS) && an_spatial) words += 1.0;
+    if ((mask & TB_ZEEMAN) && hz_arr) words += 3.0;
+    return words * sizeof(R) * static_cast<double>(N);
+  }
+
+  int kernel_time(int kernel, int reps, double* ms, double* bytes) override {
+    if (int rc = need_ms()) return rc;
+    if (kernel < 0 || kernel >= MM_NKERNELS || reps < 1) return fail(MM_ERR_ARG, "bad kernel id or reps");
+    int rc;
+    if (!acc && (rc = alloc(acc, 3 * N))) return rc;
+    if (!yB && (rc = alloc(yB, 3 * N))) return rc;
+    const bool dm = (mask & TB_DEMAG) && demag;
+    double b = 0.0;
+    if (kernel <= MM_K_DEMAG_INV_X) {
+      b = dm ? demag->pass_bytes(kernel) : 0.0;
+    } else if (kernel == MM_K_RK4_STAGE) {
+      b = stage_bytes();
+    } else {
+      b = 4.0 * stage_bytes() - 4.0 * 3.0 * sizeof(R) * N;  // stage 1 reads no m_n/acc, stage 4 writes no y
+      if (dm)
+        for (int p = 0; p < 5; ++p) b += 4.0 * demag->pass_bytes(p);
+    }
+    if (bytes) *bytes = b;
+    if (ms) *ms = 0.0;
+    if (b == 0.0) return MM_OK;
+    // the whole-step timing runs on the live state: save and restore it
+    R* save = nullptr;
+    R* save_lo = nullptr;
+    const int64_t n0 = rk_n;
+    const double t0 = rk_t;
+    if (kernel == MM_K_RK4_STEP) {
+      if ((rc = scratch(save, save_lo))) return rc;
+      MM_CUDA(cudaMemcpyAsync(save, m, sizeof(R) * 3 * N, cudaMemcpyDeviceToDevice, st_));
+      if (m_lo) MM_CUDA(cudaMemcpyAsync(save_lo, m_lo, sizeof(R) * 3 * N, cudaMemcpyDeviceToDevice, st_));
+      if ((rc = rk4_run(rk_dt > 0 ? rk_dt : 1e-15, 0))) return rc;  // make sure the step graph exists
+    }
+    auto launch = [&]() {
+      if (kernel <= MM_K_DEMAG_INV_X) {
+        demag->launch_pass(kernel, yA, Ms, Hd, st_);
+      } else if (kernel == MM_K_RK4_STAGE) {
+        StageArgs<R> sa{};
+        sa.m = m; sa.m_lo = m_lo; sa.acc = acc; sa.ynext = yB; sa.h = 1e-15; sa.stage = 2;
+        launch_stage<R>(SM_RK4, fargs(~0u), yA, sa, st_);
+      } else {
+        cudaGraphLaunch(rk_graph, st_);
+      }
+    };
+    launch();  // warm-up
+    cudaEvent_t e0, e1;
+    MM_CUDA(cudaEventCreate(&e0));
+    MM_CUDA(cudaEventCreate(&e1));
+    MM_CUDA(cudaEventRecord(e0, st_));
+    for (int r = 0; r < reps; ++r) launch();
+    MM_CUDA(cudaEventRecord(e1, st_));
+    MM_CUDA(cudaEventSynchronize(e1));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (kernel == MM_K_RK4_STEP) {
+      MM_CUDA(cudaMemcpyAsync(m, save, sizeof(R) * 3 * N, cudaMemcpyDeviceToDevice, st_));
+      if (m_lo) MM_CUDA(cudaMemcpyAsync(m_lo, save_lo, sizeof(R) * 3 * N, cudaMemcpyDeviceToDevice, st_));
+      MM_CUDA(cudaStreamSynchronize(st_));
+      rk_n = n0;
+      rk_t = t0;
+    }
+    MM_CUDA(cudaGetLastError());
+    if (ms) *ms = static_cast<double>(t) / reps;
+    return MM_OK;
+  }
+
+  int scratch(R*& a, R*& b) {
+    int rc;
+    if (!save_ && (rc = alloc(save_, 3 * N))) return rc;
+    if (kF32 && !save_lo_ && (rc = alloc(save_lo_, 3 * N))) return rc;
+    a = save_;
+    b = save_lo_;
+    return MM_OK;
+  }
+  R* save_ = nullptr;
+  R* save_lo_ = nullptr;
+
+  // ---------------------------------------------------- Dormand-Prince --
+  int dopri_alloc() {
+    int rc;
+    if (ctrl) return MM_OK;
+    for (int i = 0; i < 7; ++i)
+      if ((rc = alloc(ks[i], 3 * N))) return rc;
+    if ((rc = alloc(yB, 3 * N)) || (rc = alloc(yn, 3 * N)) || (kF32 && (rc = alloc(yn_lo, 3 * N))) ||
+        (rc = alloc(ctrl, 1)))
+      return rc;
+    hctrl = DopriCtrl{};
+    hctrl.tol = tol;
+    hctrl.inner = 1;
+    MM_CUDA(cudaMemcpyAsync(ctrl, &hctrl, sizeof(DopriCtrl), cudaMemcpyHostToDevice, st_));
+    MM_CUDA(cudaStreamSynchronize(st_));
+    return MM_OK;
+  }
+
+  void enqueue_dopri_attempt() {
+    const FieldArgs<R> fa = fargs(~0u);
+    for (int s = 1; s <= 7; ++s) {
+      const R* yin = s == 1 ? m : (s == 7 ? yn : (s % 2 == 0 ? yA : yB));
+      R* target = s == 6 ? yn : (s % 2 == 1 ? yA : yB);
+      if ((mask & TB_DEMAG) && demag) demag->apply(yin, Ms, Hd, st_, &ctrl->active);
+      StageArgs<R> sa{};
+      sa.m = m;
+      sa.m_lo = m_lo;
+      sa.ynext = target;
+      sa.ynext_lo = yn_lo;
+      for (int i = 0; i < 7; ++i) sa.k[i] = ks[i];
+      sa.stage = s;
+      sa.ctrl = ctrl;
+      sa.partials = partials;
+      launch_stage<R>(SM_DOPRI, fa, yin, sa, st_);
+    }
+    launch_dopri_control(ctrl, partials, stage_blocks(N), st_);
+    launch_dopri_accept<R>(ctrl, m, m_lo, yn, yn_lo, 3 * N, st_);
+  }
+
+  int pull_ctrl() {
+    MM_CUDA(cudaMemcpyAsync(&hctrl, ctrl, sizeof(DopriCtrl), cudaMemcpyDeviceToHost, st_));
+    MM_CUDA(cudaStreamSynchronize(st_));
+    return MM_OK;
+  }
+  int push_ctrl() {
+    MM_CUDA(cudaMemcpyAsync(ctrl, &hctrl, sizeof(DopriCtrl), cudaMemcpyHostToDevice, st_));
+    return MM_OK;
+  }
+
+  // compute_initial_step(sim, integrator, 1e-12)  adaptive_rk.jl:151-165
+  int initial_step(double& out) {
+    enqueue_rhs(m, work);
+    launch_absmax<R>(work, 3 * N, partials, scal, st_);
+    double mx = 0.0;
+    MM_CUDA(cudaMemcpyAsync(&mx, scal, sizeof(double), cudaMemcpyDeviceToHost, st_));
+    MM_CUDA(cudaStreamSynchronize(st_));
+    const double order_main = 5.0;
+    const double r_step = mx / (0.824 * std::pow(hctrl.tol, 1.0 / order_main));
+    double abs_step = 1e-12, tmp = 1e-12;
+    if (abs_step * r_step > 0.001) tmp = 0.001 / r_step;
+    hctrl.nfevals += 1;
+    out = std::min(abs_step, tmp);
+    return MM_OK;
+  }
+
+  int run_attempts() {
+    if (!dp_graph || dp_version != version) {
+      if (dp_graph) cudaGraphExecDestroy(dp_graph);
+      dp_graph = nullptr;
+      cudaGraph_t g;
+      MM_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+      enqueue_dopri_attempt();
+      MM_CUDA(cudaStreamEndCapture(st_, &g));
+      MM_CUDA(cudaGraphInstantiate(&dp_graph, g, 0));
+      cudaGraphDestroy(g);
+      dp_version = version;
+    }
+    int batch = 1;
+    const long long a0 = hctrl.attempts;
+    for (int guard = 0; guard < 1 << 24; ++guard) {
+      for (int b = 0; b < batch; ++b) MM_CUDA(cudaGraphLaunch(dp_graph, st_));
+      if (int rc = pull_ctrl()) return rc;
+      if (!hctrl.active) break;
+      batch = std::min(batch * 2, 64);
+      (void)a0;
+    }
+    MM_CUDA(cudaGetLastError());
+    return MM_OK;
+  }
+
+  static void fill_stats(const DopriCtrl& c, mm_stats* s) {
+    if (!s) return;
+    s->t = c.t;
+    s->step = c.step;
+    s->step_next = c.step_next;
+    s->nsteps = c.nsteps;
+    s->nfevals = c.nfevals;
+    s->attempts = c.attempts;
+    s->rejected = c.rejected;
+    s->status = c.status;
+  }
+
+  int dopri_tol(double t) override {
+    if (!(t > 0)) return fail(MM_ERR_ARG, "tolerance must be > 0");
+    tol = t;
+    if (ctrl) {
+      if (int rc = pull_ctrl()) return rc;
+      hctrl.tol = t;
+      return push_ctrl();
+    }
+    return MM_OK;
+  }
+
+  int dopri_reset() override {
+    if (!ctrl) return MM_OK;
+    hctrl = DopriCtrl{};
+    hctrl.tol = tol;
+    hctrl.inner = 1;
+    return push_ctrl();
+  }
+
+  int finish_status() {
+    if (hctrl.status == 1) return fail(MM_ERR_NAN, "NaN error detected in the adaptive step (t = %g)", hctrl.t);
+    if (hctrl.status == 2) return fail(MM_ERR_NOCONVERGE, "Too many inner steps, system may not converge (t = %g)", hctrl.t);
+    return MM_OK;
+  }
+
+  int run_until(double t_end, mm_stats* st) override {
+    if (int rc = need_ms()) return rc;
+    if (int rc = dopri_alloc()) return rc;
+    if (int rc = pull_ctrl()) return rc;
+    hctrl.status = 0;
+    if (t_end < hctrl.t - hctrl.step || t_end == hctrl.t || !(hctrl.t < t_end)) {
+      fill_stats(hctrl, st);
+      return MM_OK;
+    }
+    // integrate_to_time: clip to the end time, then advance_step's init
+    if (hctrl.step_next + hctrl.t > t_end) hctrl.step_next = t_end - hctrl.t;
+    if (hctrl.step_next <= 0) {
+      double s0;
+      if (int rc = initial_step(s0)) return rc;
+      hctrl.step_next = s0;
+    }
+    hctrl.step = hctrl.step_next;
+    hctrl.t_final = t_end;
+    hctrl.inner = 1;
+    hctrl.single = 0;
+    hctrl.active = 1;
+    if (int rc = push_ctrl()) return rc;
+    if (int rc = run_attempts()) return rc;
+    fill_stats(hctrl, st);
+    return finish_status();
+  }
+
+  int advance_step(mm_stats* st) override {
+    if (int rc = need_ms()) return rc;
+    if (int rc = dopri_alloc()) return rc;
+    if (int rc = pull_ctrl()) return rc;
+    hctrl.status = 0;
+    if (hctrl.step_next <= 0) {
+      double s0;
+      if (int rc = initial_step(s0)) return rc;
+      hctrl.step_next = s0;
+    }
+    hctrl.step = hctrl.step_next;
+    hctrl.t_final = INFINITY;
+    hctrl.inner = 1;
+    hctrl.single = 1;
+    hctrl.active = 1;
+    if (int rc = push_ctrl()) return rc;
+    if (int rc = run_attempts()) return rc;
+    fill_stats(hctrl, st);
+    return finish_status();
+  }
+
+  // ------------------------------------------------------------ relax --
+  int relax(int driver, int64_t max_steps, double stop, int64_t* steps, double* max_dmdt_out) override {
+    if (int rc = need_ms()) return rc;
+    int rc;
+    if (!pre && (rc = alloc(pre, 3 * N))) return rc;
+    const double time_factor = 2.21e5 / 2;
+    const double dmdt_factor = (2 * kPi / 360) * 1e9;
+    double max_dmdt = 0.0;
+    int64_t i = 1;
+    if (driver == MM_DRIVER_SD) {
+      if (!gk && (rc = alloc(gk, 3 * N))) return rc;
+      if (!sd && (rc = alloc(sd, 1))) return rc;
+      if (kF32) MM_CUDA(cudaMemsetAsync(m_lo, 0, sizeof(R) * 3 * N, st_));
+      SdState hs{0.0, 1.0, 1e-10, sd_steps};
+      MM_CUDA(cudaMemcpyAsync(sd, &hs, sizeof(hs), cudaMemcpyHostToDevice, st_));
+      const int nb = stage_blocks(N);
+      for (; i <= max_steps; ++i) {
+        enqueue_field(m, work, ~0u, nullptr);
+        launch_sd_gk<R>(m, pre, work, gk, N, sd_steps == 0 ? 1 : 0, partials, st_);
+        launch_sd_tau(sd, partials, nb, st_);
+        launch_sd_update<R>(m, pre, work, gk, pins_on ? pins : nullptr, sd, N, st_);
+        launch_sd_count(sd, st_);
+        ++sd_steps;
+        if (sd_steps % 10 == 0) launch_normalise<R>(m, N, st_);
+        launch_max_dm<R>(m, nullptr, pre, nullptr, N, partials + 3 * nb, scal, st_);
+        double out[2];
+        MM_CUDA(cudaMemcpyAsync(&out[0], scal, sizeof(double), cudaMemcpyDeviceToHost, st_));
+        MM_CUDA(cudaMemcpyAsync(&out[1], &sd->tau, sizeof(double), cudaMemcpyDeviceToHost, st_));
+        MM_CUDA(cudaStreamSynchronize(st_));
+        const double step_size = out[1] / time_factor;
+        max_dmdt = out[0] / step_size;
+        if (max_dmdt < stop * dmdt_factor) break;
+      }
+    } else {
+      if ((rc = dopri_alloc())) return rc;
+      for (; i <= max_steps; ++i) {
+        MM_CUDA(cudaMemcpyAsync(pre, m, sizeof(R) * 3 * N, cudaMemcpyDeviceToDevice, st_));
+        if (kF32) {
+          if (!pre_lo && (rc = alloc(pre_lo, 3 * N))) return rc;
+          MM_CUDA(cudaMemcpyAsync(pre_lo, m_lo, sizeof(R) * 3 * N, cudaMemcpyDeviceToDevice, st_));
+        }
+        mm_stats s;
+        rc = advance_step(&s);
+        if (rc && rc != MM_ERR_NOCONVERGE && rc != MM_ERR_NAN) return rc;
+        launch_max_dm<R>(m, m_lo, pre, pre_lo, N, partials, scal, st_);
+        double dm = 0.0;
+        MM_CUDA(cudaMemcpyAsync(&dm, scal, sizeof(double), cudaMemcpyDeviceToHost, st_));
+        MM_CUDA(cudaStreamSynchronize(st_));
+        max_dmdt = dm / hctrl.step;
+        if (max_dmdt < stop * dmdt_factor) break;
+      }
+    }
+    if (steps) *steps = i > max_steps ? max_steps : i;
+    if (max_dmdt_out) *max_dmdt_out = max_dmdt / dmdt_factor;
+    MM_CUDA(cudaGetLastError());
+    return MM_OK;
+  }
+
+  // ------------------------------------------------------------ state --
+  int nx = 1, ny = 1, nz = 1, pbc = 0;
+  int64_t N = 1;
+  double dx = 1e-9, dy = 1e-9, dz = 1e-9;
+  R *m = nullptr, *m_lo = nullptr, *Ms = nullptr, *yA = nullptr, *yB = nullptr, *acc = nullptr, *work = nullptr;
+  R *Hd = nullptr, *ecell = nullptr, *A = nullptr, *D = nullptr, *Ku = nullptr, *Hz = nullptr;
+  R *ks[7] = {}, *yn = nullptr, *yn_lo = nullptr, *pre = nullptr, *pre_lo = nullptr, *gk = nullptr;
+  uint8_t *nbm = nullptr, *pins = nullptr;
+  double *stage64 = nullptr, *partials = nullptr, *scal = nullptr;
+  DopriCtrl* ctrl = nullptr;
+  DopriCtrl hctrl{};
+  SdState* sd = nullptr;
+  long long sd_steps = 0;
+  std::unique_ptr<DemagPlan<R>> demag;
+  unsigned mask = 0;
+  bool ms_set = false, pins_on = false, ex_spatial = false, id_spatial = false, an_spatial = false, hz_arr = false;
+  double ex_A[3] = {0, 0, 0}, bd[3] = {0, 0, 0}, id_D = 0, an_K = 0, an_u[3] = {0, 0, 1}, hz_uni[3] = {0, 0, 0};
+  double alpha = 0.1, gamma = 2.21e5, tol = 1e-6;  // src/driver.jl:126,148
+  int precession = 1;
+  uint64_t version = 1;
+  double rk_t = 0.0, rk_dt = 0.0;
+  int64_t rk_n = 0;
+  cudaGraphExec_t rk_graph = nullptr, dp_graph = nullptr;
+  uint64_t rk_version = 0, dp_version = 0;
+
+ private:
+  template <typename T>
+  int alloc(T*& p, int64_t n) {
+    void* q = nullptr;
+    const size_t b = sizeof(T) * static_cast<size_t>(n);
+    cudaError_t e = cudaMalloc(&q, b);
+    if (e != cudaSuccess) return fail(MM_ERR_CUDA, "cudaMalloc(%zu): %s", b, cudaGetErrorString(e));
+    e = cudaMemsetAsync(q, 0, b, st_);
+    if (e != cudaSuccess) return fail(MM_ERR_CUDA, "cudaMemset: %s", cudaGetErrorString(e));
+    allocs_.push_back(q);
+    bytes_ += b;
+    p = static_cast<T*>(q);
+    return MM_OK;
+  }
+  cudaStream_t st_ = nullptr;
+  std::vector<void*> allocs_;
+  size_t bytes_ = 0;
+};
+
+}  // namespace mm
+
+struct mm_handle {
+  std::unique_ptr<mm::EngineBase> eng;
+};
+
+using mm::fail;
+
+#define MM_HANDLE(h)                                                          \
+  do {                                                                        \
+    if (!(h) || !(h)->eng) return fail(MM_ERR_ARG, "null handle");            \
+    if (cudaSetDevice((h)->eng->device) != cudaSuccess)                       \
+      return fail(MM_ERR_CUDA, "cudaSetDevice(%d) failed", (h)->eng->device); \
+  } while (0)
+
+#define MM_GUARD(expr)                                          \
+  try {                                                         \
+    return (expr);                                              \
+  } catch (const std::exception& ex) {                          \
+    return fail(MM_ERR_CUDA, "exception: %s", ex.what());       \
+  } catch (...) {                                               \
+    return fail(MM_ERR_CUDA, "unknown exception");              \
+  }
+
+extern "C" {
+
+int mm_abi_version(void) { return MMCUDA_ABI_VERSION; }
+
+int mm_last_error(char* buf, size_t n) {
+  if (!buf || n == 0) return MM_ERR_ARG;
+  snprintf(buf, n, "%s", mm::g_err.c_str());
+  return MM_OK;
+}
+
+int mm_create(const mm_mesh_desc* d, int form, int device, mm_handle** out) {
+  if (!d || !out) return fail(MM_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (d->nx < 1 || d->ny < 1 || d->nz < 1) return fail(MM_ERR_ARG, "mesh sizes must be >= 1");
+  if (!(d->dx > 0) || !(d->dy > 0) || !(d->dz > 0)) return fail(MM_ERR_ARG, "cell sizes must be > 0");
+  if (static_cast<int64_t>(d->nx) * d->ny * d->nz >= (1LL << 31))
+    return fail(MM_ERR_ARG, "mesh has 2^31 or more cells");
+  if (form != MM_FP64 && form != MM_FP32) return fail(MM_ERR_ARG, "form must be MM_FP64 or MM_FP32");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(MM_ERR_CUDA, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(MM_ERR_ARG, "bad device %d", device);
+  if (cudaSetDevice(device) != cudaSuccess) return fail(MM_ERR_CUDA, "cudaSetDevice failed");
+  try {
+    auto h = std::make_unique<mm_handle>();
+    int rc;
+    if (form == MM_FP64) {
+      auto e = std::make_unique<mm::Engine<double>>();
+      rc = e->init(*d, device);
+      h->eng = std::move(e);
+    } else {
+      auto e = std::make_unique<mm::Engine<float>>();
+      rc = e->init(*d, device);
+      h->eng = std::move(e);
+    }
+    if (rc) return rc;
+    *out = h.release();
+    return MM_OK;
+  } catch (...) {
+    return fail(MM_ERR_CUDA, "allocation failed");
+  }
+}
+
+int mm_destroy(mm_handle* h) {
+  if (!h) return MM_OK;
+  delete h;
+  return MM_OK;
+}
+
+int mm_get_stream(mm_handle* h, void** s) {
+  MM_HANDLE(h);
+  if (!s) return fail(MM_ERR_ARG, "null argument");
+  *s = static_cast<void*>(h->eng->stream());
+  return MM_OK;
+}
+
+int mm_synchronize(mm_handle* h) {
+  MM_HANDLE(h);
+  cudaError_t e = cudaStreamSynchronize(h->eng->stream());
+  if (e != cudaSuccess) return fail(MM_ERR_CUDA, "%s", cudaGetErrorString(e));
+  return MM_OK;
+}
+
+int mm_device_bytes(mm_handle* h, size_t* b) {
+  MM_HANDLE(h);
+  if (!b) return fail(MM_ERR_ARG, "null argument");
+  *b = h->eng->device_bytes();
+  return MM_OK;
+}
+
+int mm_set_Ms(mm_handle* h, const double* Ms, double uni) { MM_HANDLE(h); MM_GUARD(h->eng->set_Ms(Ms, uni)); }
+int mm_set_m(mm_handle* h, const double* m) {
+  MM_HANDLE(h);
+  if (!m) return fail(MM_ERR_ARG, "null m");
+  MM_GUARD(h->eng->set_m(m));
+}
+int mm_get_m(mm_handle* h, double* m) {
+  MM_HANDLE(h);
+  if (!m) return fail(MM_ERR_ARG, "null m");
+  MM_GUARD(h->eng->get_m(m));
+}
+int mm_set_pins(mm_handle* h, const uint8_t* p) { MM_HANDLE(h); MM_GUARD(h->eng->set_pins(p)); }
+int mm_set_llg(mm_handle* h, double a, double g, int p) { MM_HANDLE(h); MM_GUARD(h->eng->set_llg(a, g, p)); }
+int mm_add_zeeman(mm_handle* h, const double* H, double x, double y, double z) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->zeeman(H, x, y, z, false));
+}
+int mm_update_zeeman(mm_handle* h, const double* H, double x, double y, double z) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->zeeman(H, x, y, z, true));
+}
+int mm_add_exch(mm_handle* h, const double* A, double ax, double ay, double az) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->add_exch(A, ax, ay, az));
+}
+int mm_add_dmi_bulk(mm_handle* h, double x, double y, double z) { MM_HANDLE(h); MM_GUARD(h->eng->add_dmi_bulk(x, y, z)); }
+int mm_add_dmi_interfacial(mm_handle* h, const double* D, double u) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->add_dmi_interfacial(D, u));
+}
+int mm_add_anis(mm_handle* h, const double* K, double u, double ax, double ay, double az) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->add_anis(K, u, ax, ay, az));
+}
+int mm_add_demag(mm_handle* h, int Nx, int Ny, int Nz) { MM_HANDLE(h); MM_GUARD(h->eng->add_demag(Nx, Ny, Nz, nullptr)); }
+int mm_add_demag_tensor(mm_handle* h, const double* T) {
+  MM_HANDLE(h);
+  if (!T) return fail(MM_ERR_ARG, "null tensor");
+  MM_GUARD(h->eng->add_demag(0, 0, 0, T));
+}
+int mm_effective_field(mm_handle* h, double* H) { MM_HANDLE(h); MM_GUARD(h->eng->effective_field(H)); }
+int mm_term_field(mm_handle* h, int term, double* f, double* e) { MM_HANDLE(h); MM_GUARD(h->eng->term_field(term, f, e)); }
+int mm_energy(mm_handle* h, double* per, double* tot) { MM_HANDLE(h); MM_GUARD(h->eng->energy(per, tot)); }
+int mm_llg_rhs(mm_handle* h, double* out) {
+  MM_HANDLE(h);
+  if (!out) return fail(MM_ERR_ARG, "null output");
+  MM_GUARD(h->eng->llg_rhs(out));
+}
+int mm_average_m(mm_handle* h, double* m3) {
+  MM_HANDLE(h);
+  if (!m3) return fail(MM_ERR_ARG, "null output");
+  MM_GUARD(h->eng->average_m(m3));
+}
+int mm_rk4_run(mm_handle* h, double dt, int64_t n) { MM_HANDLE(h); MM_GUARD(h->eng->rk4_run(dt, n)); }
+int mm_rk4_state(mm_handle* h, double* t, int64_t* n) { MM_HANDLE(h); MM_GUARD(h->eng->rk4_state(t, n)); }
+int mm_dopri_set_tol(mm_handle* h, double tol) { MM_HANDLE(h); MM_GUARD(h->eng->dopri_tol(tol)); }
+int mm_run_until(mm_handle* h, double t, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h->eng->run_until(t, s)); }
+int mm_advance_step(mm_handle* h, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h->eng->advance_step(s)); }
+int mm_dopri_reset(mm_handle* h) { MM_HANDLE(h); MM_GUARD(h->eng->dopri_reset()); }
+int mm_relax(mm_handle* h, int driver, int64_t max_steps, double stop, int64_t* steps, double* mx) {
+  MM_HANDLE(h);
+  if (driver != MM_DRIVER_SD && driver != MM_DRIVER_LLG) return fail(MM_ERR_ARG, "driver must be SD or LLG");
+  MM_GUARD(h->eng->relax(driver, max_steps, stop, steps, mx));
+}
+
+int mm_kernel_time(mm_handle* h, int kernel, int reps, double* ms, double* bytes) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->kernel_time(kernel, reps, ms, bytes));
+}
+int mm_rk4_launches_per_step(mm_handle* h, int* n) {
+  MM_HANDLE(h);
+  if (!n) return fail(MM_ERR_ARG, "null output");
+  *n = h->eng->rk4_launches();
+  return MM_OK;
+}
+
+}  // extern "C"

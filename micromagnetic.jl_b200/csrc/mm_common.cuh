@@ -1,0 +1,87 @@
+// mm_common.cuh -- shared types and helpers of libmmcuda (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+namespace mm {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kMu0 = 4.0 * kPi * 1e-7;  // vacuum permeability (MicroMagnetic.jl src/const.jl:1)
+
+// ---------------------------------------------------------------- complex ---
+template <typename R> struct Cplx;
+template <> struct Cplx<float> { using T = float2; };
+template <> struct Cplx<double> { using T = double2; };
+template <typename R> using cplx_t = typename Cplx<R>::T;
+
+template <typename C> __host__ __device__ __forceinline__ C cmk(decltype(C::x) a, decltype(C::x) b) {
+  C c; c.x = a; c.y = b; return c;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return cmk<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return cmk<C>(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  return cmk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C> __device__ __forceinline__ C cconj(C a) { return cmk<C>(a.x, -a.y); }
+template <typename C, typename R> __device__ __forceinline__ C cscale(C a, R s) { return cmk<C>(a.x * s, a.y * s); }
+// multiply by (sgn * i): sgn = -1 for the forward transform, +1 for the inverse
+template <bool INV, typename C> __device__ __forceinline__ C crot(C a) {
+  return INV ? cmk<C>(-a.y, a.x) : cmk<C>(a.y, -a.x);
+}
+
+// ------------------------------------------------------------ FFT plans -----
+constexpr int kMaxStages = 16;
+// Radix sequence of a 1-D transform, 4 bits per stage (stage s in bits
+// 4s..4s+3), so that device code decodes it without an indexed array.
+struct FftPlan1 {
+  int L;                    // complex transform length (1 = identity)
+  int nst;                  // number of radix stages
+  unsigned long long code;  // radices
+};
+__host__ __device__ __forceinline__ int plan_radix(const FftPlan1& p, int s) {
+  return static_cast<int>((p.code >> (4 * s)) & 0xfull);
+}
+
+// Stage radices for a 7-smooth length, largest first (8, 7, 5, 4, 3, 2).
+inline bool make_fft_plan(int L, FftPlan1& p) {
+  p.L = L;
+  p.nst = 0;
+  p.code = 0;
+  int m = L;
+  while (m > 1) {
+    int r = 0;
+    if (m % 8 == 0) r = 8;
+    else if (m % 7 == 0) r = 7;
+    else if (m % 5 == 0) r = 5;
+    else if (m % 4 == 0) r = 4;
+    else if (m % 3 == 0) r = 3;
+    else if (m % 2 == 0) r = 2;
+    else return false;
+    if (p.nst >= kMaxStages) return false;
+    p.code |= static_cast<unsigned long long>(r) << (4 * p.nst);
+    ++p.nst;
+    m /= r;
+  }
+  return true;
+}
+
+inline bool is_7smooth(int n) {
+  if (n < 1) return false;
+  for (int p : {2, 3, 5, 7})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+// Padded FFT length for the zero-padded linear convolution of n cells: any
+// P >= 2n-1 gives the same physical-cell result (the reference uses 2n, or
+// 2n-1 for n <= 3, src/micro/demag.jl:41-44); the smallest 7-smooth length is
+// used, even where the real-to-complex x transform needs it.
+inline int padded_fft_len(int n, bool even) {
+  if (n <= 1) return 1;
+  int P = 2 * n - 1;
+  while (!is_7smooth(P) || (even && (P % 2))) ++P;
+  return P;
+}
+
+}  // namespace mm

@@ -1,0 +1,73 @@
+// mm_demag.cuh -- zero-padded FFT demagnetising-field convolution (internal).
+//
+// Follows MicroMagnetic.jl src/micro/demag.jl:30-131: H = -(1/mu0) * N (*) M,
+// M = mu0*Ms*m, with the Newell tensor N assembled in FP64
+// (demag.jl:133-417, far field atomistic/demag.jl:106-138).
+//
+// Layout in HBM (x fastest everywhere):
+//   X    [3][nz][ny][Hx] complex   x half-spectrum of the physical rows only
+//   Y    [3][nz][Py][Hx] complex   after the forward y pass (3-D meshes)
+//   Nhat [6][Pz/2+1][Py/2+1][Hx]   real tensor spectrum, one quadrant
+//        (xx yy zz xy xz yz), pre-scaled by -1/(mu0 Px Py Pz); the other
+//        quadrants follow from the even/odd symmetry of each component.
+// Passes per evaluation: fwd-x (r2c, pruned to ny*nz rows), fwd-y,
+// z-conv (fwd-z * Nhat * inv-z), inv-y, inv-x (c2r).  For nz == 1 the
+// y passes and the product fuse into one y-conv pass.
+#pragma once
+#include "mm_common.cuh"
+
+namespace mm {
+
+struct DemagGeom {
+  int nx, ny, nz;
+  int Px, Py, Pz;  // padded lengths
+  int Lc, Hx;      // Lc = Px/2 (0 when Px == 1), Hx = Lc + 1 (1 when Px == 1)
+  int Tyq, Tzq;    // Py/2 + 1, Pz/2 + 1
+  FftPlan1 plx, ply, plz;
+  const int* gate;  // device flag: kernels return at once when *gate == 0 (null: always run)
+};
+
+template <typename R>
+class DemagPlan {
+ public:
+  using C = cplx_t<R>;
+  DemagPlan() = default;
+  ~DemagPlan();
+  DemagPlan(const DemagPlan&) = delete;
+  DemagPlan& operator=(const DemagPlan&) = delete;
+
+  // Geometry, buffers and twiddle tables.  Returns 0 or a cudaError/-1 (size).
+  int init(int nx, int ny, int nz, cudaStream_t st, char* err, size_t nerr);
+  // Tensor spectrum from a real-space FP64 tensor on the device (6 x N,
+  // order xx yy zz xy xz yz).
+  int set_tensor(const double* T6N_dev, cudaStream_t st);
+  // H_demag (SoA 3N) of the magnetisation m (SoA 3N) with mu0*Ms (N).
+  void apply(const R* m, const R* mu0Ms, R* Hd, cudaStream_t st, const int* gate = nullptr);
+  // Number of kernel launches of one apply().
+  int launches_per_apply() const;
+  // One pass alone (0 fwd-x, 1 fwd-y, 2 conv, 3 inv-y, 4 inv-x), for timing;
+  // false when this geometry does not use it.
+  bool launch_pass(int which, const R* m, const R* mu0Ms, R* Hd, cudaStream_t st);
+  // Compulsory HBM bytes of one launch of that pass.
+  double pass_bytes(int which) const;
+  size_t device_bytes() const { return bytes_; }
+
+  DemagGeom g{};
+  bool fused2d = false;
+  C* X = nullptr;
+  C* Y = nullptr;
+  R* Nhat = nullptr;
+  C* twx = nullptr;
+  C* twy = nullptr;
+  C* twz = nullptr;
+
+ private:
+  size_t bytes_ = 0;
+};
+
+// FP64 Newell tensor (real space) with macro-PBC images, on the device:
+// out[c*N + I], c = xx yy zz xy xz yz.  dx,dy,dz are the raw cell sizes.
+int newell_tensor_device(int nx, int ny, int nz, double dx, double dy, double dz, int Nx, int Ny,
+                         int Nz, double* out_dev, cudaStream_t st);
+
+}  // namespace mm

@@ -1,0 +1,595 @@
+// mm_field.cu -- fused effective field + LLG + integrator stage kernels.
+#include <cmath>
+
+#include "mm_field.cuh"
+
+namespace mm {
+
+constexpr int kStageThreads = 256;
+
+int stage_blocks(int64_t N) { return static_cast<int>((N + kStageThreads - 1) / kStageThreads); }
+
+// ------------------------------------------------- compensated FP32 math ---
+// Error-free transforms (Knuth two-sum, FMA two-product) used to keep the FP32
+// form's integrator state m = hi + lo at well beyond FP32 precision.
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+  s = a + b;
+  const float bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+// hi + lo + d  ->  (hi', lo')
+__device__ __forceinline__ void df_add(float& hi, float& lo, float d) {
+  float s, e;
+  two_sum(hi, lo + d, s, e);
+  hi = s;
+  lo = e;
+}
+
+// Normalise (hi + lo) per cell to unit length in double-float arithmetic
+// (normalise, src/helper.jl:255-271: unchanged when |m|^2 == 0).
+__device__ __forceinline__ void df_normalise(float* hi, float* lo) {
+  float n2h = 0.f, n2l = 0.f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float p = hi[c] * hi[c];
+    const float pe = fmaf(hi[c], hi[c], -p);
+    float s, e;
+    two_sum(n2h, p, s, e);
+    n2h = s;
+    n2l += e + pe + 2.f * hi[c] * lo[c];
+  }
+  if (!(n2h + n2l > 0.f)) return;
+  const float d = (n2h - 1.f) + n2l;  // |m|^2 - 1
+  if (fabsf(d) < 1e-2f) {
+    // 1/sqrt(1+d) - 1 = -d/2 + 3d^2/8 - 5d^3/16 + 35d^4/128
+    const float eps = d * (-0.5f + d * (0.375f + d * (-0.3125f + d * 0.2734375f)));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float s, e;
+      two_sum(hi[c], fmaf(hi[c], eps, lo[c] * (1.f + eps)), s, e);
+      hi[c] = s;
+      lo[c] = e;
+    }
+  } else {
+    const float r = 1.f / sqrtf(n2h + n2l);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float v = hi[c] * r;
+      lo[c] = fmaf(hi[c], r, -v) + lo[c] * r;
+      float s, e;
+      two_sum(v, lo[c], s, e);
+      hi[c] = s;
+      lo[c] = e;
+    }
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void plain_normalise(R* a) {
+  const R m2 = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
+  if (m2 > 0) {
+    const R len = R(1) / sqrt(m2);
+    a[0] *= len;
+    a[1] *= len;
+    a[2] *= len;
+  }
+}
+
+// --------------------------------------------------------------- masks ---
+template <typename R>
+__global__ void k_nbmask(int nx, int ny, int nz, int pbc, const R* __restrict__ Ms, uint8_t* __restrict__ nbm) {
+  const int64_t N = static_cast<int64_t>(nx) * ny * nz;
+  const int64_t I = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (I >= N) return;
+  const int64_t nxy = static_cast<int64_t>(nx) * ny;
+  const int i = static_cast<int>(I % nx), j = static_cast<int>((I / nx) % ny), k = static_cast<int>(I / nxy);
+  const bool px = pbc & 1, py = pbc & 2, pz = pbc & 4;
+  int64_t nb[6];
+  nb[0] = i > 0 ? I - 1 : (px ? I + nx - 1 : -1);
+  nb[1] = i < nx - 1 ? I + 1 : (px ? I - (nx - 1) : -1);
+  nb[2] = j > 0 ? I - nx : (py ? I + static_cast<int64_t>(ny - 1) * nx : -1);
+  nb[3] = j < ny - 1 ? I + nx : (py ? I - static_cast<int64_t>(ny - 1) * nx : -1);
+  nb[4] = k > 0 ? I - nxy : (pz ? I + (nz - 1) * nxy : -1);
+  nb[5] = k < nz - 1 ? I + nxy : (pz ? I - (nz - 1) * nxy : -1);
+  uint8_t b = 0;
+#pragma unroll
+  for (int d = 0; d < 6; ++d)
+    if (nb[d] >= 0 && Ms[nb[d]] > R(0)) b |= static_cast<uint8_t>(1u << d);
+  nbm[I] = b;
+}
+
+template <typename R>
+void launch_nbmask(int nx, int ny, int nz, int pbc, const R* Ms, uint8_t* nbm, cudaStream_t st) {
+  const int64_t N = static_cast<int64_t>(nx) * ny * nz;
+  k_nbmask<R><<<stage_blocks(N), kStageThreads, 0, st>>>(nx, ny, nz, pbc, Ms, nbm);
+}
+
+// --------------------------------------------------------- cell H_eff ---
+// Field (A/m) of the masked terms at cell I from stage state y; optional
+// per-term energies (J) of the cell.  Restates the KernelAbstractions
+// kernels of src/micro/kernels.jl (zeeman 14-20, anisotropy 54-75, exchange
+// 226-304, bulk DMI 306-344, interfacial DMI 426-466) and the demag energy of
+// src/micro/demag.jl:435-456; terms with Ms == 0 contribute nothing.
+template <typename R, bool ENERGY>
+__device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __restrict__ y, int64_t I,
+                                          R m[3], R h[3], double* e) {
+  const int64_t N = a.N;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int64_t nxy = static_cast<int64_t>(nx) * ny;
+  m[0] = y[I];
+  m[1] = y[N + I];
+  m[2] = y[2 * N + I];
+  h[0] = h[1] = h[2] = R(0);
+  const R Ms = a.Ms[I];
+  const unsigned mask = a.mask;
+  if (ENERGY) {
+#pragma unroll
+    for (int t = 0; t < kNTerms; ++t) e[t] = 0.0;
+  }
+  if (Ms != R(0) && (mask & (TB_EXCH | TB_DMI_BULK | TB_DMI_INTERFACIAL | TB_ANIS))) {
+    const int i = static_cast<int>(I % nx), j = static_cast<int>((I / nx) % ny), k = static_cast<int>(I / nxy);
+    const bool px = a.pbc & 1, py = a.pbc & 2, pz = a.pbc & 4;
+    const unsigned nbm = a.nbm[I];
+    int64_t nb[6];
+    nb[0] = i > 0 ? I - 1 : (px ? I + nx - 1 : -1);
+    nb[1] = i < nx - 1 ? I + 1 : (px ? I - (nx - 1) : -1);
+    nb[2] = j > 0 ? I - nx : (py ? I + static_cast<int64_t>(ny - 1) * nx : -1);
+    nb[3] = j < ny - 1 ? I + nx : (py ? I - static_cast<int64_t>(ny - 1) * nx : -1);
+    nb[4] = k > 0 ? I - nxy : (pz ? I + (nz - 1) * nxy : -1);
+    nb[5] = k < nz - 1 ? I + nxy : (pz ? I - (nz - 1) * nxy : -1);
+    const R Ms_inv = R(1) / Ms;
+    R mn[6][3];
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+      if ((nbm >> d) & 1u) {
+        const int64_t q = nb[d];
+        mn[d][0] = __ldg(y + q);
+        mn[d][1] = __ldg(y + N + q);
+        mn[d][2] = __ldg(y + 2 * N + q);
+      } else {
+        mn[d][0] = mn[d][1] = mn[d][2] = R(0);
+      }
+    }
+    // exchange
+    if (mask & TB_EXCH) {
+      R fx = 0, fy = 0, fz = 0;
+      const R coef[6] = {a.ex_x, a.ex_x, a.ex_y, a.ex_y, a.ex_z, a.ex_z};
+      bool on = true;
+      R AI = R(0);
+      if (a.A) {
+        AI = a.A[I];
+        on = AI != R(0);
+      }
+      if (on) {
+#pragma unroll
+        for (int d = 0; d < 6; ++d) {
+          if ((nbm >> d) & 1u) {
+            R c = coef[d];
+            if (a.A) {
+              const R An = __ldg(a.A + nb[d]);
+              if (An == R(0)) continue;
+              const R Aeff = 2 * AI * An / (AI + An);
+              c = Aeff * coef[d];
+            }
+            fx += c * (mn[d][0] - m[0]);
+            fy += c * (mn[d][1] - m[1]);
+            fz += c * (mn[d][2] - m[2]);
+          }
+        }
+        if (ENERGY) e[1] = -0.5 * (double(fx) * m[0] + double(fy) * m[1] + double(fz) * m[2]) * double(a.V);
+        h[0] += fx * Ms_inv;
+        h[1] += fy * Ms_inv;
+        h[2] += fz * Ms_inv;
+      }
+    }
+    // bulk DMI: sum_d (D/d) a_d x m_d, a = +x,-x,+y,-y,+z,-z for d = -x,+x,-y,+y,-z,+z
+    if (mask & TB_DMI_BULK) {
+      R fx = 0, fy = 0, fz = 0;
+      if (nbm & 1u) { fy += a.bd_x * (-mn[0][2]); fz += a.bd_x * mn[0][1]; }
+      if (nbm & 2u) { fy += a.bd_x * mn[1][2]; fz += a.bd_x * (-mn[1][1]); }
+      if (nbm & 4u) { fx += a.bd_y * mn[2][2]; fz += a.bd_y * (-mn[2][0]); }
+      if (nbm & 8u) { fx += a.bd_y * (-mn[3][2]); fz += a.bd_y * mn[3][0]; }
+      if (nbm & 16u) { fx += a.bd_z * (-mn[4][1]); fy += a.bd_z * mn[4][0]; }
+      if (nbm & 32u) { fx += a.bd_z * mn[5][1]; fy += a.bd_z * (-mn[5][0]); }
+      if (ENERGY) e[2] = -0.5 * (double(fx) * m[0] + double(fy) * m[1] + double(fz) * m[2]) * double(a.V);
+      h[0] += fx * Ms_inv;
+      h[1] += fy * Ms_inv;
+      h[2] += fz * Ms_inv;
+    }
+    // interfacial DMI: r = +y,-y,-x,+x for d = -x,+x,-y,+y; harmonic mean of D
+    if (mask & TB_DMI_INTERFACIAL) {
+      const R DI = a.D ? a.D[I] : a.D_uni;
+      if (DI != R(0)) {
+        R fx = 0, fy = 0, fz = 0;
+        const R dd[4] = {a.id_x, a.id_x, a.id_y, a.id_y};
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+          if (!((nbm >> d) & 1u)) continue;
+          R c;
+          if (a.D) {
+            const R Dn = __ldg(a.D + nb[d]);
+            if (Dn == R(0)) continue;
+            c = (2 * DI * Dn / (DI + Dn)) * dd[d];
+          } else {
+            c = DI * dd[d];
+          }
+          // r x m_nb
+          if (d == 0) { fx += c * mn[0][2]; fz += c * (-mn[0][0]); }
+          else if (d == 1) { fx += c * (-mn[1][2]); fz += c * mn[1][0]; }
+          else if (d == 2) { fy += c * mn[2][2]; fz += c * (-mn[2][1]); }
+          else { fy += c * (-mn[3][2]); fz += c * mn[3][1]; }
+        }
+        if (ENERGY) e[3] = -0.5 * (double(fx) * m[0] + double(fy) * m[1] + double(fz) * m[2]) * double(a.V);
+        h[0] += fx * Ms_inv;
+        h[1] += fy * Ms_inv;
+        h[2] += fz * Ms_inv;
+      }
+    }
+    // uniaxial anisotropy
+    if (mask & TB_ANIS) {
+      const R Ku = a.Ku ? a.Ku[I] : a.Ku_uni;
+      const R inv2 = R(2) / Ms;
+      const R sa = m[0] * a.ux + m[1] * a.uy + m[2] * a.uz;
+      h[0] += Ku * sa * a.ux * inv2;
+      h[1] += Ku * sa * a.uy * inv2;
+      h[2] += Ku * sa * a.uz * inv2;
+      if (ENERGY) e[4] = double(Ku) * (1.0 - double(sa) * sa) * double(a.V);
+    }
+  }
+  if (mask & TB_DEMAG) {
+    const R dx = a.Hd[I], dy = a.Hd[N + I], dz = a.Hd[2 * N + I];
+    h[0] += dx;
+    h[1] += dy;
+    h[2] += dz;
+    if (ENERGY) e[5] = -0.5 * double(Ms) * double(a.V) * (double(m[0]) * dx + double(m[1]) * dy + double(m[2]) * dz);
+  }
+  if (mask & TB_ZEEMAN) {
+    // uniform part plus the per-cell part (accumulated add_zeeman fields)
+    R zx = a.hz_x, zy = a.hz_y, zz = a.hz_z;
+    if (a.Hz) {
+      zx += a.Hz[I];
+      zy += a.Hz[N + I];
+      zz += a.Hz[2 * N + I];
+    }
+    h[0] += zx;
+    h[1] += zy;
+    h[2] += zz;
+    if (ENERGY) e[0] = -double(a.V) * double(Ms) * (double(m[0]) * zx + double(m[1]) * zy + double(m[2]) * zz);
+  }
+}
+
+// llg_rhs_kernel!  src/llg/llg.jl:6-40
+template <typename R>
+__device__ __forceinline__ void llg_rhs(const FieldArgs<R>& a, int64_t I, const R m[3], const R h[3], R f[3]) {
+  if (a.pins && a.pins[I]) {
+    f[0] = f[1] = f[2] = R(0);
+    return;
+  }
+  const R alpha = a.alpha;
+  const R c = -a.gamma / (1 + alpha * alpha);
+  const R mm = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+  const R mh = m[0] * h[0] + m[1] * h[1] + m[2] * h[2];
+  const R h1 = mm * h[0] - mh * m[0];
+  const R h2 = mm * h[1] - mh * m[1];
+  const R h3 = mm * h[2] - mh * m[2];
+  R f1 = 0, f2 = 0, f3 = 0;
+  if (a.precession) {
+    f1 = -m[2] * h2 + m[1] * h3;
+    f2 = m[2] * h1 - m[0] * h3;
+    f3 = -m[1] * h1 + m[0] * h2;
+  }
+  f[0] = c * (f1 - h1 * alpha);
+  f[1] = c * (f2 - h2 * alpha);
+  f[2] = c * (f3 - h3 * alpha);
+}
+
+// Dormand-Prince 5(4) tableau (src/integrator/adaptive_rk_steps.jl:49-57)
+__constant__ double c_dp_a[6][6] = {
+    {1.0 / 5, 0, 0, 0, 0, 0},
+    {3.0 / 40, 9.0 / 40, 0, 0, 0, 0},
+    {44.0 / 45, -56.0 / 15, 32.0 / 9, 0, 0, 0},
+    {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729, 0, 0},
+    {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656, 0},
+    {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}};
+__constant__ double c_dp_w[7] = {71.0 / 57600, 0, -71.0 / 16695, 71.0 / 1920, -17253.0 / 339200, 22.0 / 525, -1.0 / 40};
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(kStageThreads) k_stage(FieldArgs<R> a, const R* __restrict__ y, StageArgs<R> s) {
+  constexpr bool kF32 = sizeof(R) == 4;
+  if (MODE == SM_DOPRI && !s.ctrl->active) return;
+  const int64_t N = a.N;
+  const int64_t I = blockIdx.x * static_cast<int64_t>(kStageThreads) + threadIdx.x;
+  const bool live = I < N;
+  double e[kNTerms];
+  R m[3], h[3];
+  double red = 0.0;  // SM_DOPRI stage 7: error max
+  if (live) {
+    cell_heff<R, MODE == SM_ENERGY || MODE == SM_FIELD>(a, y, I, m, h, e);
+    if (MODE == SM_FIELD) {
+      s.out[I] = h[0];
+      s.out[N + I] = h[1];
+      s.out[2 * N + I] = h[2];
+      if (s.ecell) {
+        double et = 0.0;
+#pragma unroll
+        for (int t = 0; t < kNTerms; ++t) et += e[t];
+        s.ecell[I] = static_cast<R>(et);
+      }
+    } else if (MODE == SM_RHS) {
+      R f[3];
+      llg_rhs(a, I, m, h, f);
+      s.out[I] = f[0];
+      s.out[N + I] = f[1];
+      s.out[2 * N + I] = f[2];
+    } else if (MODE == SM_RK4) {
+      // advance_step(::RungeKutta)  src/integrator/rk.jl:23-52
+      R f[3];
+      llg_rhs(a, I, m, h, f);
+      const int st = s.stage;
+      if (st < 4) {
+        R acc[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const R kc = f[c];
+          acc[c] = st == 1 ? kc : s.acc[c * N + I] + 2 * kc;
+          s.acc[c * N + I] = acc[c];
+        }
+        const R cf = static_cast<R>(st == 3 ? s.h : 0.5 * s.h);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const R m0 = s.m[c * N + I];
+          R v;
+          if (kF32) v = m0 + (s.m_lo[c * N + I] + cf * f[c]);
+          else v = m0 + cf * f[c];
+          s.ynext[c * N + I] = v;
+        }
+      } else {
+        const R c6 = static_cast<R>(1.0 / 6 * s.h);
+        R mv[3];
+        if constexpr (kF32) {
+          float lo[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            mv[c] = s.m[c * N + I];
+            lo[c] = s.m_lo[c * N + I];
+            df_add(mv[c], lo[c], c6 * (s.acc[c * N + I] + f[c]));
+          }
+          df_normalise(mv, lo);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s.m_lo[c * N + I] = lo[c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) mv[c] = s.m[c * N + I] + c6 * (s.acc[c * N + I] + f[c]);
+          plain_normalise(mv);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s.m[c * N + I] = mv[c];
+      }
+    } else if (MODE == SM_DOPRI) {
+      // rk_step_dopri54!  src/integrator/adaptive_rk_steps.jl:49-107
+      R f[3];
+      llg_rhs(a, I, m, h, f);
+      const int st = s.stage;
+      const double hstep = s.ctrl->step;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s.k[st - 1][c * N + I] = f[c];
+      if (st <= 6) {
+        const double* arow = c_dp_a[st - 1];
+        R v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if constexpr (kF32) {
+            float sum = 0.f;
+            for (int j = 0; j < st; ++j) {
+              if (arow[j] == 0.0) continue;
+              const float kj = j == st - 1 ? f[c] : s.k[j][c * N + I];
+              sum += static_cast<float>(arow[j] * hstep) * kj;
+            }
+            v[c] = sum;
+          } else {
+            double acc = s.m[c * N + I];
+            for (int j = 0; j < st; ++j) {
+              if (arow[j] == 0.0) continue;
+              const double kj = j == st - 1 ? f[c] : s.k[j][c * N + I];
+              acc = acc + (arow[j] * hstep) * kj;
+            }
+            v[c] = static_cast<R>(acc);
+          }
+        }
+        if (st < 6) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            if constexpr (kF32) v[c] = s.m[c * N + I] + (s.m_lo[c * N + I] + v[c]);
+            s.ynext[c * N + I] = v[c];
+          }
+        } else {
+          // 5th-order solution, normalised before k7 (adaptive_rk_steps.jl:92-96)
+          if constexpr (kF32) {
+            float hi[3], lo[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              hi[c] = s.m[c * N + I];
+              lo[c] = s.m_lo[c * N + I];
+              df_add(hi[c], lo[c], v[c]);
+            }
+            df_normalise(hi, lo);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              s.ynext[c * N + I] = hi[c];
+              s.ynext_lo[c * N + I] = lo[c];
+            }
+          } else {
+            plain_normalise(v);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) s.ynext[c * N + I] = v[c];
+          }
+        }
+      } else {
+        // error estimate: max |sum_j w_j k_j| / (1 + |y_next|)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          double et = 0.0;
+          et = c_dp_w[0] * double(s.k[0][c * N + I]);
+          et += c_dp_w[2] * double(s.k[2][c * N + I]);
+          et += c_dp_w[3] * double(s.k[3][c * N + I]);
+          et += c_dp_w[4] * double(s.k[4][c * N + I]);
+          et += c_dp_w[5] * double(s.k[5][c * N + I]);
+          et += c_dp_w[6] * double(f[c]);
+          const double v = fabs(et / (1.0 + fabs(double(m[c]))));
+          red = (v > red || isnan(v)) ? v : red;
+        }
+      }
+    }
+  }
+  if (MODE == SM_ENERGY || (MODE == SM_DOPRI && s.stage == 7)) {
+    // deterministic block reduction in FP64
+    __shared__ double sh[kStageThreads / 32][kNTerms];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int W = MODE == SM_ENERGY ? kNTerms : 1;
+    double v[W];
+#pragma unroll
+    for (int t = 0; t < W; ++t) v[t] = live ? (MODE == SM_ENERGY ? e[t] : red) : 0.0;
+#pragma unroll
+    for (int t = 0; t < W; ++t) {
+      for (int o = 16; o > 0; o >>= 1) {
+        const double u = __shfl_down_sync(0xffffffffu, v[t], o);
+        if (MODE == SM_ENERGY) v[t] += u;
+        else v[t] = (u > v[t] || isnan(u)) ? u : v[t];
+      }
+      if (lane == 0) sh[warp][t] = v[t];
+    }
+    __syncthreads();
+    if (threadIdx.x < W) {
+      double acc = MODE == SM_ENERGY ? 0.0 : 0.0;
+      for (int w = 0; w < kStageThreads / 32; ++w) {
+        const double u = sh[w][threadIdx.x];
+        if (MODE == SM_ENERGY) acc += u;
+        else acc = (u > acc || isnan(u)) ? u : acc;
+      }
+      s.partials[blockIdx.x * W + threadIdx.x] = acc;
+    }
+  }
+}
+
+template <typename R>
+void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<R>& sa, cudaStream_t st) {
+  const int nb = stage_blocks(fa.N);
+  switch (mode) {
+    case SM_FIELD: k_stage<R, SM_FIELD><<<nb, kStageThreads, 0, st>>>(fa, y, sa); break;
+    case SM_RHS: k_stage<R, SM_RHS><<<nb, kStageThreads, 0, st>>>(fa, y, sa); break;
+    case SM_RK4: k_stage<R, SM_RK4><<<nb, kStageThreads, 0, st>>>(fa, y, sa); break;
+    case SM_ENERGY: k_stage<R, SM_ENERGY><<<nb, kStageThreads, 0, st>>>(fa, y, sa); break;
+    default: k_stage<R, SM_DOPRI><<<nb, kStageThreads, 0, st>>>(fa, y, sa); break;
+  }
+}
+
+// --------------------------------------------------------- conversions ---
+template <typename R>
+__global__ void k_aos_to_soa(const double* __restrict__ aos, R* __restrict__ hi, R* __restrict__ lo, int64_t N,
+                             int* __restrict__ nanflag) {
+  const int64_t I = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (I >= N) return;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double v = aos[3 * I + c];
+    if (nanflag && isnan(v)) *nanflag = 1;
+    const R h = static_cast<R>(v);
+    hi[c * N + I] = h;
+    if (lo) lo[c * N + I] = static_cast<R>(v - static_cast<double>(h));
+  }
+}
+
+template <typename R>
+__global__ void k_soa_to_aos(const R* __restrict__ hi, const R* __restrict__ lo, double* __restrict__ aos, int64_t N) {
+  const int64_t I = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (I >= N) return;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double v = static_cast<double>(hi[c * N + I]);
+    if (lo) v += static_cast<double>(lo[c * N + I]);
+    aos[3 * I + c] = v;
+  }
+}
+
+template <typename R>
+__global__ void k_scalar_to_R(const double* __restrict__ a, R* __restrict__ b, int64_t n, double scale) {
+  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (i < n) b[i] = static_cast<R>(a[i] * scale);
+}
+
+template <typename R>
+void launch_aos_to_soa(const double* aos, R* hi, R* lo, int64_t N, int* nanflag, cudaStream_t st) {
+  k_aos_to_soa<R><<<stage_blocks(N), kStageThreads, 0, st>>>(aos, hi, lo, N, nanflag);
+}
+template <typename R>
+void launch_soa_to_aos(const R* hi, const R* lo, double* aos, int64_t N, cudaStream_t st) {
+  k_soa_to_aos<R><<<stage_blocks(N), kStageThreads, 0, st>>>(hi, lo, aos, N);
+}
+template <typename R>
+void launch_scalar_to_R(const double* a, R* b, int64_t n, double scale, cudaStream_t st) {
+  k_scalar_to_R<R><<<stage_blocks(n), kStageThreads, 0, st>>>(a, b, n, scale);
+}
+
+// ---------------------------------------------------------- reductions ---
+// out[t] = sum_b partials[b*width + t], fixed order (one block).
+__global__ void k_reduce_sum(const double* __restrict__ partials, int nblocks, int width, double* __restrict__ out) {
+  __shared__ double sh[256];
+  for (int t = 0; t < width; ++t) {
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) acc += partials[static_cast<int64_t>(b) * width + t];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[t] = sh[0];
+    __syncthreads();
+  }
+}
+
+void launch_reduce_sum(const double* partials, int nblocks, int width, double* out, cudaStream_t st) {
+  k_reduce_sum<<<1, 256, 0, st>>>(partials, nblocks, width, out);
+}
+
+template <typename R>
+__global__ void k_sum_m(const R* __restrict__ m, const R* __restrict__ lo, int64_t N, double* __restrict__ partials) {
+  __shared__ double sh[3][kStageThreads];
+  const int64_t I = blockIdx.x * static_cast<int64_t>(kStageThreads) + threadIdx.x;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double v = 0.0;
+    if (I < N) {
+      v = m[c * N + I];
+      if (lo) v += lo[c * N + I];
+    }
+    sh[c][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int o = kStageThreads / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) partials[blockIdx.x * 3 + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+template <typename R>
+void launch_average_m(const R* m, const R* m_lo, int64_t N, double* partials, double* out, cudaStream_t st) {
+  const int nb = stage_blocks(N);
+  k_sum_m<R><<<nb, kStageThreads, 0, st>>>(m, m_lo, N, partials);
+  k_reduce_sum<<<1, 256, 0, st>>>(partials, nb, 3, out);
+}
+
+#define MM_INST(R)                                                                                       \
+  template void launch_stage<R>(int, const FieldArgs<R>&, const R*, const StageArgs<R>&, cudaStream_t); \
+  template void launch_nbmask<R>(int, int, int, int, const R*, uint8_t*, cudaStream_t);                 \
+  template void launch_aos_to_soa<R>(const double*, R*, R*, int64_t, int*, cudaStream_t);                     \
+  template void launch_soa_to_aos<R>(const R*, const R*, double*, int64_t, cudaStream_t);               \
+  template void launch_scalar_to_R<R>(const double*, R*, int64_t, double, cudaStream_t);                \
+  template void launch_average_m<R>(const R*, const R*, int64_t, double*, double*, cudaStream_t);
+MM_INST(float)
+MM_INST(double)
+
+}  // namespace mm

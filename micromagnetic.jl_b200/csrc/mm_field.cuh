@@ -1,0 +1,109 @@
+// mm_field.cuh -- fused effective-field / LLG / integrator-stage kernels
+// (internal interface of libmmcuda).
+//
+// One thread per cell, SoA state y[c*N + cell] (x fastest).  The local terms
+// (exchange, bulk and interfacial DMI, uniaxial anisotropy, Zeeman) are
+// evaluated from the cell and its six neighbours, the demag field is read
+// from the buffer written by the FFT passes, and the LLG right-hand side and
+// the integrator-stage update are applied in the same kernel.
+#pragma once
+#include "mm_common.cuh"
+
+namespace mm {
+
+enum TermBit : unsigned {
+  TB_ZEEMAN = 1u << 0,
+  TB_EXCH = 1u << 1,
+  TB_DMI_BULK = 1u << 2,
+  TB_DMI_INTERFACIAL = 1u << 3,
+  TB_ANIS = 1u << 4,
+  TB_DEMAG = 1u << 5,
+};
+constexpr int kNTerms = 6;
+
+template <typename R> struct FieldArgs {
+  int nx, ny, nz, pbc;
+  int64_t N;
+  R V;                    // cell volume
+  const R* Ms;            // mu0*Ms (T), N
+  const uint8_t* nbm;     // bit d: neighbour d exists and has Ms > 0
+  unsigned mask;          // TermBit set
+  // exchange: uniform coefficients 2A/d^2, or 2/d^2 with the A array
+  R ex_x, ex_y, ex_z;
+  const R* A;             // null: uniform
+  // bulk DMI: D/d per axis
+  R bd_x, bd_y, bd_z;
+  // interfacial DMI: D (uniform) or D array, and 1/dx, 1/dy
+  R D_uni;
+  const R* D;
+  R id_x, id_y;
+  // uniaxial anisotropy
+  R Ku_uni;
+  const R* Ku;
+  R ux, uy, uz;
+  // Zeeman (A/m), uniform or SoA array
+  R hz_x, hz_y, hz_z;
+  const R* Hz;
+  // demag field (SoA, written by the FFT passes)
+  const R* Hd;
+  // LLG
+  R alpha, gamma;
+  int precession;
+  const uint8_t* pins;
+};
+
+enum StageMode { SM_FIELD = 0, SM_RHS = 1, SM_RK4 = 2, SM_ENERGY = 3, SM_DOPRI = 4 };
+
+// Dormand-Prince device-side controller state (src/integrator/adaptive_rk.jl:93-186)
+struct DopriCtrl {
+  double t, step, step_next, t_final, tol;
+  double err;               // last scaled error norm
+  long long nsteps, nfevals, attempts, rejected;
+  int inner;                // attempts of the current advance_step (nstep)
+  int active;               // 1 while integrating
+  int status;               // 0 ok, 1 NaN, 2 too many attempts
+  int accepted_last;        // last attempt accepted
+  int need_init;            // compute_initial_step pending
+  int single;               // stop after one accepted step (advance_step)
+  double init_rmax;         // max |f| for the initial step
+};
+
+template <typename R> struct StageArgs {
+  R* out;                   // SM_FIELD: H (SoA); SM_RHS: dm/dt (SoA)
+  R* ecell;                 // SM_FIELD: per-cell energy of the masked terms (may be null)
+  double* partials;         // SM_ENERGY: [blocks][kNTerms]; SM_DOPRI stage 7: [blocks] max
+  // integrator state m_n = m + m_lo (m_lo null in the FP64 form)
+  R* m;
+  R* m_lo;
+  R* acc;                   // RK4 accumulator
+  R* ynext;                 // next stage input
+  R* ynext_lo;              // DOPRI stage 7: low part of y_next
+  R* k[7];                  // DOPRI stage derivatives
+  double h;                 // RK4 step
+  int stage;                // 1-based
+  const DopriCtrl* ctrl;    // DOPRI: step size and active flag
+};
+
+template <typename R>
+void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<R>& sa, cudaStream_t st);
+
+int stage_blocks(int64_t N);
+
+template <typename R>
+void launch_nbmask(int nx, int ny, int nz, int pbc, const R* Ms, uint8_t* nbm, cudaStream_t st);
+
+// AoS double <-> SoA R (+ compensated low part)
+template <typename R>
+void launch_aos_to_soa(const double* aos, R* hi, R* lo, int64_t N, int* nanflag, cudaStream_t st);
+template <typename R>
+void launch_soa_to_aos(const R* hi, const R* lo, double* aos, int64_t N, cudaStream_t st);
+template <typename R>
+void launch_scalar_to_R(const double* a, R* b, int64_t n, double scale, cudaStream_t st);
+
+// deterministic final reductions
+void launch_reduce_sum(const double* partials, int nblocks, int width, double* out, cudaStream_t st);
+
+template <typename R>
+void launch_average_m(const R* m, const R* m_lo, int64_t N, double* partials, double* out, cudaStream_t st);
+
+}  // namespace mm

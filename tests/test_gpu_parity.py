@@ -1,0 +1,270 @@
+"""GPU parity: libmmcuda (through its C ABI) against the CPU oracle and the
+reference's golden vectors.
+
+Tolerances (relative max-norm ||gpu - ref||_inf / ||ref||_inf):
+  * FP64 form, local terms, LLG right-hand side, RK4 / DOPRI steps: 1e-12
+  * FP64 form, demag with the oracle's tensor uploaded (pure convolution): 1e-12
+  * FP64 form, demag with the tensor assembled on the GPU: 1e-9 (the Newell
+    sums cancel catastrophically at R ~ 60 cells, so libm vs CUDA atan/asinh
+    differences of 1 ulp show up at this level; see TENSOR_TOL)
+  * FP32 form against the FP64 form: 1e-5
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from helpers import GpuSim, build_oracle, random_config, rel_maxnorm
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL64 = 1e-12
+TENSOR_TOL = 1e-9
+TOL32 = 1e-5
+
+def _seed(mesh):
+    return mesh[0] * 10000 + mesh[1] * 100 + mesh[2]
+
+
+LOCAL = ("exch", "dmi_bulk", "dmi_int", "anis", "zeeman")
+
+MESHES = [
+    (7, 5, 3, ""), (20, 5, 3, ""), (16, 16, 1, "xy"), (12, 1, 1, ""), (1, 1, 1, ""), (3, 2, 1, ""),
+    (5, 4, 6, "xyz"), (33, 7, 2, "x"), (2, 1, 1, ""), (9, 11, 4, "z"), (64, 48, 1, ""), (1, 6, 5, "y"),
+]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+@pytest.mark.parametrize("mesh", MESHES)
+def test_local_terms_fp64(mesh):
+    nx, ny, nz, pbc = mesh
+    cfg = random_config(_seed(mesh), nx, ny, nz, pbc, terms=LOCAL)
+    o, idx = build_oracle(cfg)
+    g = GpuSim(cfg, form=0)
+    for t in LOCAL:
+        fo, eo = o.term_field(idx[t])
+        fg, eg = g.term_field(t)
+        assert rel_maxnorm(fg, fo) <= TOL64, (t, rel_maxnorm(fg, fo))
+        assert rel_maxnorm(eg, eo) <= TOL64, (t, "energy", rel_maxnorm(eg, eo))
+    assert rel_maxnorm(g.field(), o.effective_field()) <= TOL64
+    assert rel_maxnorm(g.rhs(), o.llg_rhs()) <= TOL64
+
+
+@pytest.mark.parametrize("mesh", MESHES)
+def test_demag_convolution_fp64(mesh):
+    """FFT convolution alone: the oracle's real-space tensor is uploaded."""
+    from oracle.oracle import demag_tensor
+
+    nx, ny, nz, pbc = mesh
+    cfg = random_config(7 + _seed(mesh), nx, ny, nz, "", terms=("demag",))
+    T = demag_tensor(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, idx = build_oracle(cfg, tensor=T)
+    g = GpuSim(cfg, form=0, tensor=T)
+    fo, eo = o.term_field(idx["demag"])
+    fg, eg = g.term_field("demag")
+    assert rel_maxnorm(fg, fo) <= TOL64, rel_maxnorm(fg, fo)
+    assert rel_maxnorm(eg, eo) <= TOL64
+
+
+@pytest.mark.parametrize("mesh", MESHES)
+def test_demag_newell_fp64(mesh):
+    nx, ny, nz, pbc = mesh
+    cfg = random_config(11 + _seed(mesh), nx, ny, nz, "", terms=("demag",))
+    o, idx = build_oracle(cfg)
+    g = GpuSim(cfg, form=0)
+    fo, _ = o.term_field(idx["demag"])
+    fg, _ = g.term_field("demag")
+    assert rel_maxnorm(fg, fo) <= TENSOR_TOL, rel_maxnorm(fg, fo)
+
+
+def test_demag_macro_pbc_fp64():
+    cfg = random_config(5, 6, 5, 1, "", terms=("demag",))
+    cfg["macro"] = (3, 2, 0)
+    o, idx = build_oracle(cfg)
+    g = GpuSim(cfg, form=0)
+    assert rel_maxnorm(g.term_field("demag")[0], o.term_field(idx["demag"])[0]) <= TENSOR_TOL
+
+
+def test_golden_fields_gpu():
+    """test/test_fields.jl:25-59 at the reference tolerances, on the GPU."""
+    gd = dict(np.load(os.path.join(GOLD, "fields_20x5x3.npz")))
+    n = 300
+    m = gd["m0"].reshape(-1, 3).copy()
+    m[gd["Ms"] == 0] = 0
+    cfg = dict(nx=20, ny=5, nz=3, dx=2.5e-9, dy=2.5e-9, dz=3e-9, pbc="", Ms=gd["Ms"], m=m.reshape(-1),
+               terms=["exch", "demag", "dmi_bulk", "dmi_int", "anis"], A=1.3e-11, Dbulk=(4e-3, 4e-3, 4e-3),
+               Dint=np.full(n, 2e-3), Ku=np.full(n, -3e4), axis=(0, 0, 1), H=np.zeros(3 * n), alpha=0.1,
+               gamma=2.21e5)
+    g = GpuSim(cfg, form=0)
+    keys = {"exch": "exch", "demag": "demag", "dmi_bulk": "dmi", "dmi_int": "dmi_interfacial", "anis": "anis"}
+    energies = {}
+    for t, k in keys.items():
+        f, e = g.term_field(t)
+        assert np.max(np.abs(f - gd[k])) < 1e-5, (t, np.max(np.abs(f - gd[k])))
+        energies[k] = e.sum()
+    E = gd["energy"]
+    assert abs((energies["demag"] - E[0]) / E[0]) < 1e-11
+    for i, k in enumerate(["exch", "dmi", "dmi_interfacial", "anis"], start=1):
+        assert abs((energies[k] - E[i]) / E[i]) < 1e-13, k
+
+
+def test_demag_known_answers_gpu():
+    cases = json.load(open(os.path.join(GOLD, "demag_known.json")))["cases"]
+    for c in cases:
+        n = c["nx"] * c["ny"] * c["nz"]
+        mm = np.array(c["m"], float)
+        mm /= np.linalg.norm(mm)
+        cfg = dict(nx=c["nx"], ny=c["ny"], nz=c["nz"], dx=c["dx"], dy=c["dy"], dz=c["dz"], pbc="",
+                   Ms=np.full(n, c["Ms"]), m=np.tile(mm, n), terms=["demag"], alpha=0.1, gamma=2.21e5)
+        f = GpuSim(cfg, form=0).field()
+        exp = np.array(c["field"])
+        assert np.linalg.norm(f - exp) <= math.sqrt(np.finfo(float).eps) * np.linalg.norm(exp)
+
+
+@pytest.mark.parametrize("mesh", [(20, 5, 3, ""), (16, 16, 1, "xy"), (9, 11, 4, "z")])
+def test_rk4_steps_fp64(mesh):
+    """One and ten RK4 steps (src/integrator/rk.jl:23-52) with all terms."""
+    nx, ny, nz, pbc = mesh
+    cfg = random_config(3, nx, ny, nz, pbc)
+    from oracle.oracle import demag_tensor
+
+    T = demag_tensor(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, _ = build_oracle(cfg, tensor=T)
+    g = GpuSim(cfg, form=0, tensor=T)
+    dt = 2e-14
+    o.rk4(dt, 1)
+    g.rk4(dt, 1)
+    assert rel_maxnorm(g.m(), o.get_m()) <= TOL64
+    o.rk4(dt, 9)
+    g.rk4(dt, 9)
+    assert rel_maxnorm(g.m(), o.get_m()) <= 1e-11
+
+
+def test_dopri_run_until_fp64():
+    """run_until with Dormand-Prince: same accepted steps and state as the oracle."""
+    from oracle.oracle import demag_tensor
+
+    cfg = random_config(4, 12, 10, 2, "")
+    T = demag_tensor(12, 10, 2, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, _ = build_oracle(cfg, tensor=T)
+    g = GpuSim(cfg, form=0, tensor=T)
+    o.set_tol(1e-6)
+    g.set_tol(1e-6)
+    for t in (2e-13, 5e-13):
+        ok, so = o.run_until(t)
+        rc, sg = g.run_until(t)
+        assert ok and rc == 0
+        assert sg["nsteps"] == so["nsteps"] and sg["attempts"] - sg["rejected"] == so["nsteps"]
+        assert abs(sg["t"] - so["t"]) <= 1e-15 * t
+        assert rel_maxnorm(g.m(), o.get_m()) <= 1e-11
+
+
+def analytical(alpha, gamma, H0, t):
+    p = gamma / (1 + alpha * alpha)
+    beta = p * H0 * t
+    return np.cos(beta) / np.cosh(alpha * beta), np.sin(beta) / np.cosh(alpha * beta), np.tanh(alpha * beta)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_macrospin_rk4_and_dopri(form):
+    """test/test_llg.jl:23-104 on the GPU: analytic damped precession."""
+    cfg = dict(nx=1, ny=1, nz=1, dx=1e-9, dy=1e-9, dz=1e-9, pbc="", Ms=np.array([8e5]), m=np.array([1.0, 0, 0]),
+               terms=["exch", "zeeman"], A=1.3e-11, H=np.array([0, 0, 1e5]), alpha=0.05, gamma=2.21e5)
+    g = GpuSim(cfg, form=form)
+    g.rk4(1e-13, 500)
+    exp = analytical(0.05, 2.21e5, 1e5, 5e-11)
+    m = g.m()
+    assert all(abs(m[i] - exp[i]) < 8e-6 for i in range(3))
+    cfg["terms"] = ["zeeman"]
+    g = GpuSim(cfg, form=form)
+    g.set_tol(1e-8)
+    for i in range(1, 11):
+        rc, _ = g.run_until(1e-10 * i)
+        assert rc == 0
+    exp = analytical(0.05, 2.21e5, 1e5, 1e-9)
+    m = g.m()
+    assert all(abs(m[i] - exp[i]) < 8e-7 for i in range(3))
+
+
+def test_energies_fp64():
+    from oracle.oracle import demag_tensor
+
+    cfg = random_config(8, 10, 6, 3, "")
+    T = demag_tensor(10, 6, 3, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, idx = build_oracle(cfg, tensor=T)
+    g = GpuSim(cfg, form=0, tensor=T)
+    tot, per = g.energy()
+    for t, i in idx.items():
+        eo = o.term_field(i)[1].sum()
+        assert abs(per[{"zeeman": 0, "exch": 1, "dmi_bulk": 2, "dmi_int": 3, "anis": 4, "demag": 5}[t]] - eo) <= 1e-12 * abs(eo) + 1e-40
+
+
+@pytest.mark.parametrize("driver", ["SD", "LLG"])
+def test_relax_domain_wall_gpu(driver):
+    """test/test_relax.jl:8-40 on the GPU, plus the step count of the oracle."""
+    nx, ny, nz = 500, 1, 11
+    n = nx * ny * nz
+    m = np.zeros((nz, ny, nx, 3))
+    i = np.arange(1, nx + 1)
+    m[..., :] = np.where((i < 240)[:, None], [1, 0.1, 0], np.where((i < 260)[:, None], [0, 1, 0.1], [-1, 0.1, 0]))
+    m /= np.linalg.norm(m, axis=-1, keepdims=True)
+    cfg = dict(nx=nx, ny=ny, nz=nz, dx=2e-9, dy=2e-9, dz=1e-9, pbc="", Ms=np.full(n, 8.6e5), m=m.reshape(-1),
+               terms=["exch", "anis"], A=1.3e-11, Ku=np.full(n, 1e5), axis=(1, 0, 0), alpha=0.5, gamma=2.21e5)
+    g = GpuSim(cfg, form=0)
+    o, _ = build_oracle(cfg)
+    import ctypes
+
+    if driver == "LLG":
+        g.h.call("mm_set_llg", 0.5, 2.21e5, 0)
+        o.set_llg(0.5, 2.21e5, precession=False)
+    steps = ctypes.c_int64()
+    mx = ctypes.c_double()
+    g.h.call("mm_relax", 0 if driver == "SD" else 1, 2000, 0.1, ctypes.byref(steps), ctypes.byref(mx))
+    so, _ = o.relax(driver, 2000, 0.1)
+    mg = g.m().reshape(-1, 3).mean(0)
+    assert abs(mg[0]) < 0.01 and abs(mg[1]) < 0.04 and abs(mg[2]) < 0.01
+    assert abs(steps.value - so) <= max(2, so // 50), (steps.value, so)
+
+
+@pytest.mark.parametrize("mesh", [(20, 5, 3, ""), (16, 16, 1, "xy"), (9, 11, 4, "z")])
+def test_fp32_form_fields(mesh):
+    nx, ny, nz, pbc = mesh
+    cfg = random_config(9, nx, ny, nz, pbc)
+    g64 = GpuSim(cfg, form=0)
+    g32 = GpuSim(cfg, form=1)
+    assert rel_maxnorm(g32.field(), g64.field()) <= TOL32
+    assert rel_maxnorm(g32.rhs(), g64.rhs()) <= TOL32
+    t64, p64 = g64.energy()
+    t32, p32 = g32.energy()
+    assert abs(t32 - t64) <= TOL32 * np.abs(p64).sum()
+
+
+def test_fp32_form_rk4_1000_steps():
+    """FP32 form vs FP64 form after 1000 RK4 steps (dt = 1e-13) on a film with
+    exchange, Zeeman and demag (the 200x50x1 workload, reduced to 64x32x1)."""
+    rng = np.random.default_rng(101)
+    nx, ny, nz = 64, 32, 1
+    n = nx * ny
+    m = rng.normal(size=(n, 3))
+    m /= np.linalg.norm(m, axis=1, keepdims=True)
+    B = rng.uniform(0, 0.03)
+    phi = rng.uniform(0, 2 * np.pi)
+    H = np.tile([B / (4e-7 * np.pi) * np.cos(phi), B / (4e-7 * np.pi) * np.sin(phi), 0.0], n)
+    cfg = dict(nx=nx, ny=ny, nz=nz, dx=2.5e-9, dy=2.5e-9, dz=3e-9, pbc="", Ms=np.full(n, 8e5), m=m.reshape(-1),
+               terms=["exch", "zeeman", "demag"], A=1.3e-11, H=H, alpha=0.02, gamma=2.211e5)
+    g64 = GpuSim(cfg, form=0)
+    g32 = GpuSim(cfg, form=1)
+    g64.rk4(1e-13, 1000)
+    g32.rk4(1e-13, 1000)
+    err = rel_maxnorm(g32.m(), g64.m())
+    print("fp32 vs fp64 after 1000 RK4 steps:", err)
+    assert err <= TOL32

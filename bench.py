@@ -237,7 +237,7 @@ def run_native(args):
     dt = w["dt"]
     forms = {"fp32": _lib.MM_FP32, "fp64": _lib.MM_FP64}
     results = {}
-    for fname in ("fp32", "fp64"):
+    for fname in ((args.only,) if args.only else ("fp32", "fp64")):
         h, m0 = setup_native(w, forms[fname], device)
         stream = torch.cuda.ExternalStream(h.stream(), device=device)
         for _ in range(args.warmup):
@@ -268,6 +268,10 @@ def run_native(args):
                "launches_per_step": h.rk4_launches(), "device_bytes": h.device_bytes()}
         if sampler:
             res["clocks"] = sampler.summary()
+        if args.quick:
+            h.close()
+            del stream
+            continue
         # per-kernel CUDA-event timing on the handle's stream (same kernels as the step)
         kern = {}
         for kid, kname in enumerate(_lib.KERNELS):
@@ -305,6 +309,12 @@ def run_native(args):
         results[fname] = res
         h.close()
         del stream
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({k: {"ms_per_step": v["ms_per_step"], "value": v["value"]} for k, v in results.items()}))
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     if rank == 0:
         r = results["fp32"]
         peak, peak_kind = measured_peak()
@@ -351,6 +361,8 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", choices=["fp32", "fp64"], help="time one form only (profiling runs)")
+    ap.add_argument("--quick", action="store_true", help="timed steps only: no e2e, kernel timing or CPU leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

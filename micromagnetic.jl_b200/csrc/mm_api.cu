@@ -109,7 +109,7 @@ class Engine : public EngineBase {
     dx = d.dx; dy = d.dy; dz = d.dz;
     N = static_cast<int64_t>(nx) * ny * nz;
     MM_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
-    const int nb = stage_blocks(N);
+    const int nb = std::max(stage_blocks(N), stage_grid(nx, ny, nz).nblocks);
     int rc = 0;
     if ((rc = alloc(m, 3 * N)) || (kF32 && (rc = alloc(m_lo, 3 * N))) || (rc = alloc(Ms, N)) ||
         (rc = alloc(nbm, N)) || (rc = alloc(yA, 3 * N)) || (rc = alloc(work, 3 * N)) ||
@@ -339,7 +339,9 @@ class Engine : public EngineBase {
     a.Hz = hz_arr ? Hz : nullptr;
     a.Hd = Hd;
     a.alpha = static_cast<R>(alpha);
-    a.gamma = static_cast<R>(gamma);
+    const double c = -gamma / (1 + alpha * alpha);  // llg.jl:24
+    a.llg_c = static_cast<R>(c);
+    a.llg_c_lo = static_cast<R>(c - static_cast<double>(a.llg_c));
     a.precession = precession;
     a.pins = pins_on ? pins : nullptr;
     return a;
@@ -401,7 +403,7 @@ class Engine : public EngineBase {
     StageArgs<R> s{};
     s.partials = partials;
     launch_stage<R>(SM_ENERGY, fargs(~0u), m, s, st_);
-    launch_reduce_sum(partials, stage_blocks(N), kNTerms, scal, st_);
+    launch_reduce_sum(partials, stage_grid(nx, ny, nz).nblocks, kNTerms, scal, st_);
     double e[kNTerms];
     MM_CUDA(cudaMemcpyAsync(e, scal, sizeof(e), cudaMemcpyDeviceToHost, st_));
     MM_CUDA(cudaStreamSynchronize(st_));
@@ -609,7 +611,7 @@ class Engine : public EngineBase {
       sa.partials = partials;
       launch_stage<R>(SM_DOPRI, fa, yin, sa, st_);
     }
-    launch_dopri_control(ctrl, partials, stage_blocks(N), st_);
+    launch_dopri_control(ctrl, partials, stage_grid(nx, ny, nz).nblocks, st_);
     launch_dopri_accept<R>(ctrl, m, m_lo, yn, yn_lo, 3 * N, st_);
   }
 

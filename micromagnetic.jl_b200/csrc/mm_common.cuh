@@ -32,22 +32,59 @@ template <bool INV, typename C> __device__ __forceinline__ C crot(C a) {
 
 // ------------------------------------------------------------ FFT plans -----
 constexpr int kMaxStages = 16;
-// Radix sequence of a 1-D transform, 4 bits per stage (stage s in bits
-// 4s..4s+3), so that device code decodes it without an indexed array.
+// Radix sequence of a 1-D transform, 3 bits per stage (stage s in bits
+// 3s..3s+2: 1=2 2=3 3=4 4=5 5=7 6=8 7=16), so that device code decodes it
+// without an indexed array.
 struct FftPlan1 {
   int L;                    // complex transform length (1 = identity)
   int nst;                  // number of radix stages
+  int pow2;                 // L is a power of two
   unsigned long long code;  // radices
 };
 __host__ __device__ __forceinline__ int plan_radix(const FftPlan1& p, int s) {
-  return static_cast<int>((p.code >> (4 * s)) & 0xfull);
+  const int c = static_cast<int>((p.code >> (3 * s)) & 7ull);
+  return c == 1 ? 2 : c == 2 ? 3 : c == 3 ? 4 : c == 4 ? 5 : c == 5 ? 7 : c == 6 ? 8 : 16;
 }
 
-// Stage radices for a 7-smooth length, largest first (8, 7, 5, 4, 3, 2).
-inline bool make_fft_plan(int L, FftPlan1& p) {
+inline int radix_code(int r) {
+  switch (r) {
+    case 2: return 1;
+    case 3: return 2;
+    case 4: return 3;
+    case 5: return 4;
+    case 7: return 5;
+    case 8: return 6;
+    default: return 7;
+  }
+}
+
+// Stage radices for a 7-smooth length.  Powers of two are split into the
+// fewest stages of radix <= max_pow2_radix with balanced exponents (2^11 with
+// 16 -> 16,16,8); other lengths take 8, 7, 5, 4, 3, 2 greedily.
+inline bool make_fft_plan(int L, FftPlan1& p, int max_pow2_radix = 8) {
   p.L = L;
   p.nst = 0;
   p.code = 0;
+  p.pow2 = (L & (L - 1)) == 0;
+  auto push = [&](int r) {
+    if (p.nst >= kMaxStages) return false;
+    p.code |= static_cast<unsigned long long>(radix_code(r)) << (3 * p.nst);
+    ++p.nst;
+    return true;
+  };
+  if (p.pow2) {
+    int lg = 0;
+    while ((1 << lg) < L) ++lg;
+    int lmax = 0;
+    while ((1 << lmax) < max_pow2_radix) ++lmax;
+    if (lg == 0) return true;
+    const int ns = (lg + lmax - 1) / lmax;
+    for (int s = 0; s < ns; ++s) {
+      const int e = lg / ns + (s < lg % ns ? 1 : 0);
+      if (!push(1 << e)) return false;
+    }
+    return true;
+  }
   int m = L;
   while (m > 1) {
     int r = 0;
@@ -58,12 +95,29 @@ inline bool make_fft_plan(int L, FftPlan1& p) {
     else if (m % 3 == 0) r = 3;
     else if (m % 2 == 0) r = 2;
     else return false;
-    if (p.nst >= kMaxStages) return false;
-    p.code |= static_cast<unsigned long long>(r) << (4 * p.nst);
-    ++p.nst;
+    if (!push(r)) return false;
     m /= r;
   }
   return true;
+}
+
+// Division by a run-time invariant d for 0 <= x < 2^31 with one multiply-high
+// (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994): q = (umulhi(x, m) + x) >> l.
+struct FastDiv {
+  unsigned d, m, l;
+};
+inline FastDiv make_fastdiv(unsigned d) {
+  FastDiv f;
+  f.d = d;
+  f.l = 0;
+  while ((1ull << f.l) < d) ++f.l;
+  f.m = static_cast<unsigned>(((1ull << (32 + f.l)) / d) - (1ull << 32) + 1);
+  return f;
+}
+__device__ __forceinline__ int fdiv(int x, const FastDiv f) {
+  const unsigned t = __umulhi(static_cast<unsigned>(x), f.m);
+  return static_cast<int>((t + static_cast<unsigned>(x)) >> f.l);
 }
 
 inline bool is_7smooth(int n) {

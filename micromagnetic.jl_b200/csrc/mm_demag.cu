@@ -9,12 +9,20 @@
 
 namespace mm {
 
-// Threads per block and register elements per thread of the FFT passes; one
-// block transforms at most E*T complex values (64 KB of shared memory).
-template <typename R> struct FftCfg;
-template <> struct FftCfg<float> { static constexpr int T = 512, E = 16; };
-template <> struct FftCfg<double> { static constexpr int T = 512, E = 8; };
-template <typename R> constexpr int fft_cap() { return FftCfg<R>::T * FftCfg<R>::E; }
+// Pass configuration: NT threads per block and the number of complex values
+// a block transforms.  The hot passes run 256-thread blocks (three per SM
+// overlap their loads with the transforms of the others); the one-time FP64
+// tensor passes run 512.
+template <typename R, int NT> struct PassCfg {
+  // complex values per block (each of the two ping-pong buffers): 32 KB
+  // (64 KB of shared memory per block for the hot passes)
+  static constexpr int cap = (sizeof(R) == 4 || NT == 512) ? 4096 : 2048;
+  static constexpr int minb = NT == 256 ? 3 : 1;
+};
+constexpr int kHotNT = 256;
+constexpr int kTensorNT = 512;
+template <typename R> constexpr int hot_cap() { return PassCfg<R, kHotNT>::cap; }
+constexpr int tensor_cap() { return PassCfg<double, kTensorNT>::cap; }
 
 // Symmetry of the six tensor components under x -> -x, y -> -y, z -> -z
 // (fill_tensors calls, src/micro/demag.jl:56-83): xx yy zz even; xy odd in x,y;
@@ -24,30 +32,41 @@ __host__ __device__ inline int odd_axis(int c, int ax) {
   return (tbl[c] >> ax) & 1;
 }
 
+static int floor_pow2(int v) {
+  int p = 1;
+  while (p * 2 <= v) p *= 2;
+  return p;
+}
+static int ilog2(int v) {
+  int l = 0;
+  while ((1 << l) < v) ++l;
+  return l;
+}
+
 // ============================================================== kernels ====
 enum XMode { XM_MAGN = 0, XM_TENSOR = 1 };
 
 // Forward x pass: real rows (zero padded / mirrored to Px) -> half spectrum.
 // line = c*rows + row;  X[line*Hx + k].
-template <typename R, int MODE>
-__global__ void __launch_bounds__(512, 1) k_fwd_x(const R* __restrict__ m, const R* __restrict__ Ms,
-                                               const double* __restrict__ Tr, int tsign,
-                                               cplx_t<R>* __restrict__ X, DemagGeom g,
-                                               int lines_total, int nl,
-                                               const cplx_t<R>* __restrict__ twx) {
+template <typename R, int MODE, int NT>
+__global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_fwd_x(
+    const R* __restrict__ m, const R* __restrict__ Ms, const double* __restrict__ Tr, int tsign,
+    cplx_t<R>* __restrict__ X, DemagGeom g, int lines_total, int nl, const cplx_t<R>* __restrict__ twx,
+    int half) {
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
+  C* buf2 = buf + half;
   if (g.gate && !*g.gate) return;
   const int Lc = g.Lc, LS = Lc | 1, nx = g.nx, Px = g.Px;
   const int rows = g.ny * g.nz;
   const int64_t N = static_cast<int64_t>(rows) * nx;
   const int line0 = blockIdx.x * nl;
   const int nlh = min(nl, lines_total - line0);
-  for (int e = threadIdx.x; e < nlh * Lc; e += blockDim.x) {
-    const int l = e / Lc, t = e - l * Lc;
+  for (int e = threadIdx.x; e < nlh * Lc; e += NT) {
+    const int l = fdiv(e, g.fLc), t = e - l * Lc;
     const int line = line0 + l;
-    const int c = line / rows, row = line - c * rows;
+    const int c = fdiv(line, g.frows), row = line - c * rows;
     R v[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -68,15 +87,15 @@ __global__ void __launch_bounds__(512, 1) k_fwd_x(const R* __restrict__ m, const
     buf[l * LS + t] = cmk<C>(v[0], v[1]);
   }
   __syncthreads();
-  fft_lines<false, FftCfg<R>::E>(buf, LS, nlh, g.plx, twx, 2);
+  buf = fft_lines<false, NT>(buf, buf2, LS, nlh, g.plx, twx, 2);
   const int Hx = g.Hx;
-  const R half = R(0.5);
-  for (int e = threadIdx.x; e < nlh * Hx; e += blockDim.x) {
-    const int l = e / Hx, k = e - l * Hx;
+  const R one_half = R(0.5);
+  for (int e = threadIdx.x; e < nlh * Hx; e += NT) {
+    const int l = fdiv(e, g.fHx), k = e - l * Hx;
     const C zk = buf[l * LS + (k == Lc ? 0 : k)];
     const C zc = cconj(buf[l * LS + (k == 0 ? 0 : Lc - k)]);
-    const C ev = cscale(cadd(zk, zc), half);
-    const C od = crot<false>(cscale(csub(zk, zc), half));  // (zk - zc)/(2i)
+    const C ev = cscale(cadd(zk, zc), one_half);
+    const C od = crot<false>(cscale(csub(zk, zc), one_half));  // (zk - zc)/(2i)
     const C w = __ldg(twx + k);
     X[static_cast<int64_t>(line0 + l) * Hx + k] = cadd(ev, cmul(w, od));
   }
@@ -84,9 +103,8 @@ __global__ void __launch_bounds__(512, 1) k_fwd_x(const R* __restrict__ m, const
 
 // Px == 1 (nx == 1): the x "transform" is the identity.
 template <typename R, int MODE>
-__global__ void k_fwd_x1(const R* __restrict__ m, const R* __restrict__ Ms,
-                         const double* __restrict__ Tr, cplx_t<R>* __restrict__ X, int rows,
-                         int lines_total, const int* __restrict__ gate) {
+__global__ void k_fwd_x1(const R* __restrict__ m, const R* __restrict__ Ms, const double* __restrict__ Tr,
+                         cplx_t<R>* __restrict__ X, int rows, int lines_total, const int* __restrict__ gate) {
   using C = cplx_t<R>;
   if (gate && !*gate) return;
   const int line = blockIdx.x * blockDim.x + threadIdx.x;
@@ -99,21 +117,22 @@ __global__ void k_fwd_x1(const R* __restrict__ m, const R* __restrict__ Ms,
 }
 
 // Inverse x pass: half spectrum -> real rows (unnormalised c2r), keeps nx.
-template <typename R>
-__global__ void __launch_bounds__(512, 1) k_inv_x(const cplx_t<R>* __restrict__ X, R* __restrict__ H,
-                                               DemagGeom g, int lines_total, int nl,
-                                               const cplx_t<R>* __restrict__ twx) {
+template <typename R, int NT>
+__global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_inv_x(
+    const cplx_t<R>* __restrict__ X, R* __restrict__ H, DemagGeom g, int lines_total, int nl,
+    const cplx_t<R>* __restrict__ twx, int half) {
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
+  C* buf2 = buf + half;
   if (g.gate && !*g.gate) return;
   const int Lc = g.Lc, LS = Lc | 1, nx = g.nx, Hx = g.Hx;
   const int rows = g.ny * g.nz;
   const int64_t N = static_cast<int64_t>(rows) * nx;
   const int line0 = blockIdx.x * nl;
   const int nlh = min(nl, lines_total - line0);
-  for (int e = threadIdx.x; e < nlh * Lc; e += blockDim.x) {
-    const int l = e / Lc, k = e - l * Lc;
+  for (int e = threadIdx.x; e < nlh * Lc; e += NT) {
+    const int l = fdiv(e, g.fLc), k = e - l * Lc;
     const C* xr = X + static_cast<int64_t>(line0 + l) * Hx;
     const C a = xr[k];
     const C b = cconj(xr[Lc - k]);
@@ -122,11 +141,11 @@ __global__ void __launch_bounds__(512, 1) k_inv_x(const cplx_t<R>* __restrict__ 
     buf[l * LS + k] = cadd(cadd(a, b), crot<true>(cmul(csub(a, b), w)));
   }
   __syncthreads();
-  fft_lines<true, FftCfg<R>::E>(buf, LS, nlh, g.plx, twx, 2);
-  for (int e = threadIdx.x; e < nlh * Lc; e += blockDim.x) {
-    const int l = e / Lc, t = e - l * Lc;
+  buf = fft_lines<true, NT>(buf, buf2, LS, nlh, g.plx, twx, 2);
+  for (int e = threadIdx.x; e < nlh * Lc; e += NT) {
+    const int l = fdiv(e, g.fLc), t = e - l * Lc;
     const int line = line0 + l;
-    const int c = line / rows, row = line - c * rows;
+    const int c = fdiv(line, g.frows), row = line - c * rows;
     const C z = buf[l * LS + t];
     const int u = 2 * t;
     R* out = H + c * N + static_cast<int64_t>(row) * nx;
@@ -145,17 +164,19 @@ __global__ void k_inv_x1(const cplx_t<R>* __restrict__ X, R* __restrict__ H, int
 }
 
 // Product with the tensor spectrum, in shared memory: lines (c*W + w) of
-// length L hold the 3 components; along y (kz = kz_fixed) or along z
-// (ky = ky_fixed).
-template <typename R, bool ALONG_Y>
-__device__ __forceinline__ void tensor_product(cplx_t<R>* buf, int LS, int W, int L, int kx0,
-                                               int ky_fixed, const R* __restrict__ Nhat,
-                                               const int Hx, const int Py, const int Pz) {
+// length L hold the 3 components at (kx0 + w, ky, kz); along y (kz = 0) or
+// along z (ky fixed).  The stored quadrant is unfolded with the component
+// parities (odd in y: xy, yz; odd in z: xz, yz).
+template <typename R, bool ALONG_Y, int NT>
+__device__ __forceinline__ void tensor_product(cplx_t<R>* buf, int LS, int lgW, int L, const FastDiv fL,
+                                               int kx0, int ky_fixed, const R* __restrict__ Nhat, int Hx, int Py,
+                                               int Pz) {
   using C = cplx_t<R>;
+  const int W = 1 << lgW;
   const int Tyq = Py / 2 + 1, Tzq = Pz / 2 + 1;
   const int64_t Ts = static_cast<int64_t>(Tzq) * Tyq * Hx;
-  for (int e = threadIdx.x; e < W * L; e += blockDim.x) {
-    const int w = e / L, t = e - w * L;
+  for (int e = threadIdx.x; e < W * L; e += NT) {
+    const int w = e & (W - 1), t = e >> lgW;  // w fastest: coalesced tensor reads
     const int kx = kx0 + w;
     if (kx >= Hx) continue;
     const int ky = ALONG_Y ? t : ky_fixed;
@@ -175,70 +196,86 @@ __device__ __forceinline__ void tensor_product(cplx_t<R>* buf, int LS, int W, in
     *p1 = cmk<C>(xy * a.x + yy * bb.x + yz * c.x, xy * a.y + yy * bb.y + yz * c.y);
     *p2 = cmk<C>(xz * a.x + yz * bb.x + zz * c.x, xz * a.y + yz * bb.y + zz * c.y);
   }
+  (void)fL;
   __syncthreads();
 }
 
 enum YMode { YM_FWD = 0, YM_INV = 1, YM_CONV2D = 2, YM_TENSOR = 3, YM_TENSOR_Q = 4 };
 
-// y pass over column tiles [kx0, kx0+W) of one z plane for ncompc components.
-// grid: (tiles, nz, 3/ncompc)
-template <typename R, int MODE>
-__global__ void __launch_bounds__(512, 1) k_ypass(const cplx_t<R>* in, cplx_t<R>* out,
-                                               const R* __restrict__ Nhat, double* __restrict__ Tq,
-                                               DemagGeom g, int W, int ncompc,
-                                               const cplx_t<R>* __restrict__ twy, int tsign,
-                                               double tscale) {
+// y pass over column tiles [kx0, kx0 + 2^lgW) of one z plane for ncompc
+// components.  grid: (tiles, nz, 3/ncompc).  Shared layout: line (cl*W + w),
+// position j (LS = Py | 1 keeps the transposed stores free of bank conflicts).
+template <typename R, int MODE, int NT>
+__global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_ypass(
+    const cplx_t<R>* in, cplx_t<R>* out, const R* __restrict__ Nhat, double* __restrict__ Tq, DemagGeom g,
+    int lgW, int ncompc, const cplx_t<R>* __restrict__ twy, int tsign, double tscale, int half) {
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
+  C* buf2 = buf + half;
   if (g.gate && !*g.gate) return;
   const int Py = g.Py, LS = Py | 1, Hx = g.Hx, ny = g.ny, nz = g.nz;
+  const int W = 1 << lgW;
   const int kx0 = blockIdx.x * W;
   const int z = blockIdx.y;
   const int c0 = blockIdx.z * ncompc;
   const int rows_in = (MODE == YM_INV) ? Py : ny;
-  // load
-  for (int e = threadIdx.x; e < ncompc * Py * W; e += blockDim.x) {
-    const int w = e % W;
-    const int r = e / W;
-    const int j = r % Py;
-    const int cl = r / Py;
+  // zero the padded rows, then load the rows that hold data
+  if (MODE != YM_INV) {
+    const int pad = (MODE == YM_TENSOR || MODE == YM_TENSOR_Q) ? 0 : Py - ny;
+    for (int e = threadIdx.x; e < ncompc * W * pad; e += NT) {
+      const int l = fdiv(e, g.fpady), j = ny + (e - l * pad);
+      buf[l * LS + j] = cmk<C>(R(0), R(0));
+    }
+  }
+  const int nload = (MODE == YM_TENSOR || MODE == YM_TENSOR_Q) ? Py : rows_in;
+  const FastDiv fr = (MODE == YM_INV || MODE == YM_TENSOR || MODE == YM_TENSOR_Q) ? g.fPy : g.fny;
+  for (int e = threadIdx.x; e < ncompc * nload * W; e += NT) {
+    const int w = e & (W - 1);
+    const int r = e >> lgW;
+    const int cl = fdiv(r, fr);
+    const int j = r - cl * nload;
     const int kx = kx0 + w;
     C v = cmk<C>(R(0), R(0));
     if (kx < Hx) {
       const int64_t base = static_cast<int64_t>((c0 + cl) * nz + z) * rows_in;
       if (j < rows_in) {
         v = in[(base + j) * Hx + kx];
-      } else if (MODE == YM_TENSOR || MODE == YM_TENSOR_Q) {
-        if (j >= Py - ny + 1) {
-          v = in[(base + (Py - j)) * Hx + kx];
-          if (tsign < 0) v = cmk<C>(-v.x, -v.y);
-        }
+      } else if (j >= Py - ny + 1) {  // tensor modes: mirrored rows
+        v = in[(base + (Py - j)) * Hx + kx];
+        if (tsign < 0) v = cmk<C>(-v.x, -v.y);
       }
     }
     buf[(cl * W + w) * LS + j] = v;
   }
   __syncthreads();
-  fft_lines<MODE == YM_INV, FftCfg<R>::E>(buf, LS, ncompc * W, g.ply, twy, 1);
+  {
+    C* res = fft_lines<MODE == YM_INV, NT>(buf, buf2, LS, ncompc * W, g.ply, twy, 1);
+    if (res != buf) {
+      buf2 = buf;
+      buf = res;
+    }
+  }
   if (MODE == YM_CONV2D) {
-    tensor_product<R, true>(buf, LS, W, Py, kx0, 0, Nhat, Hx, Py, g.Pz);
-    fft_lines<true, FftCfg<R>::E>(buf, LS, ncompc * W, g.ply, twy, 1);
+    tensor_product<R, true, NT>(buf, LS, lgW, Py, g.fPy, kx0, 0, Nhat, Hx, Py, g.Pz);
+    buf = fft_lines<true, NT>(buf, buf2, LS, ncompc * W, g.ply, twy, 1);
   }
   // store
   if (MODE == YM_TENSOR_Q) {
-    for (int e = threadIdx.x; e < g.Tyq * W; e += blockDim.x) {
-      const int w = e % W, j = e / W;
+    for (int e = threadIdx.x; e < g.Tyq * W; e += NT) {
+      const int w = e & (W - 1), j = e >> lgW;
       const int kx = kx0 + w;
       if (kx < Hx) Tq[static_cast<int64_t>(j) * Hx + kx] = static_cast<double>(buf[w * LS + j].x) * tscale;
     }
     return;
   }
   const int rows_out = (MODE == YM_FWD || MODE == YM_TENSOR) ? Py : ny;
-  for (int e = threadIdx.x; e < ncompc * rows_out * W; e += blockDim.x) {
-    const int w = e % W;
-    const int r = e / W;
-    const int j = r % rows_out;
-    const int cl = r / rows_out;
+  const FastDiv fo = (MODE == YM_FWD || MODE == YM_TENSOR) ? g.fPy : g.fny;
+  for (int e = threadIdx.x; e < ncompc * rows_out * W; e += NT) {
+    const int w = e & (W - 1);
+    const int r = e >> lgW;
+    const int cl = fdiv(r, fo);
+    const int j = r - cl * rows_out;
     const int kx = kx0 + w;
     if (kx < Hx) {
       const int64_t base = static_cast<int64_t>((c0 + cl) * nz + z) * rows_out;
@@ -249,56 +286,82 @@ __global__ void __launch_bounds__(512, 1) k_ypass(const cplx_t<R>* in, cplx_t<R>
 
 enum ZMode { ZM_CONV = 0, ZM_TENSOR_Q = 1 };
 
-// z pass over column tiles of one ky row.  grid: (tiles, Py or Tyq)
-template <typename R, int MODE>
-__global__ void __launch_bounds__(512, 1) k_zpass(cplx_t<R>* __restrict__ Y, const R* __restrict__ Nhat,
-                                               double* __restrict__ Tq, DemagGeom g, int W,
-                                               int ncompc, const cplx_t<R>* __restrict__ twz,
-                                               int tsign, double tscale) {
+// z pass over column tiles of one ky row (and, in ZM_CONV, of its mirror row
+// Py - ky in the same block, so each tensor entry is fetched once).
+// grid: (tiles, Py/2 + 1 or Tyq)
+template <typename R, int MODE, int NT>
+__global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_zpass(
+    cplx_t<R>* __restrict__ Y, const R* __restrict__ Nhat, double* __restrict__ Tq, DemagGeom g, int lgW,
+    int ncompc, const cplx_t<R>* __restrict__ twz, int tsign, double tscale, int half) {
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
+  C* buf2 = buf + half;
   if (g.gate && !*g.gate) return;
   const int Pz = g.Pz, LS = Pz | 1, Hx = g.Hx, Py = g.Py, nz = g.nz;
+  const int W = 1 << lgW;
   const int kx0 = blockIdx.x * W;
-  const int ky = blockIdx.y;
-  for (int e = threadIdx.x; e < ncompc * Pz * W; e += blockDim.x) {
-    const int w = e % W;
-    const int r = e / W;
-    const int kz = r % Pz;
-    const int cl = r / Pz;
+  const int kyA = blockIdx.y;
+  // rows handled: ky and (for the product) its mirror, when distinct
+  const int kyB = (MODE == ZM_CONV && kyA > 0 && 2 * kyA != Py) ? Py - kyA : -1;
+  const int nrow = kyB >= 0 ? 2 : 1;
+  const int ncl = ncompc * nrow;  // line groups of W lines
+  const int pad = (MODE == ZM_TENSOR_Q) ? 0 : Pz - nz;
+  for (int e = threadIdx.x; e < ncl * W * pad; e += NT) {
+    const int l = fdiv(e, g.fpadz), kz = nz + (e - l * pad);
+    buf[l * LS + kz] = cmk<C>(R(0), R(0));
+  }
+  const int nload = (MODE == ZM_TENSOR_Q) ? Pz : nz;
+  const FastDiv fr = (MODE == ZM_TENSOR_Q) ? g.fPz : g.fnz;
+  for (int e = threadIdx.x; e < ncl * nload * W; e += NT) {
+    const int w = e & (W - 1);
+    const int r = e >> lgW;
+    const int q = fdiv(r, fr);  // line group = row * ncompc + cl
+    const int kz = r - q * nload;
+    const int row = q / ncompc, cl = q - row * ncompc;
+    const int ky = row == 0 ? kyA : kyB;
     const int kx = kx0 + w;
     C v = cmk<C>(R(0), R(0));
     if (kx < Hx) {
       if (kz < nz) {
         v = Y[(static_cast<int64_t>(cl * nz + kz) * Py + ky) * Hx + kx];
-      } else if (MODE == ZM_TENSOR_Q && kz >= Pz - nz + 1) {
+      } else if (kz >= Pz - nz + 1) {  // tensor mode: mirrored rows
         v = Y[(static_cast<int64_t>(cl * nz + (Pz - kz)) * Py + ky) * Hx + kx];
         if (tsign < 0) v = cmk<C>(-v.x, -v.y);
       }
     }
-    buf[(cl * W + w) * LS + kz] = v;
+    buf[(q * W + w) * LS + kz] = v;
   }
   __syncthreads();
-  fft_lines<false, FftCfg<R>::E>(buf, LS, ncompc * W, g.plz, twz, 1);
+  {
+    C* res = fft_lines<false, NT>(buf, buf2, LS, ncl * W, g.plz, twz, 1);
+    if (res != buf) {
+      buf2 = buf;
+      buf = res;
+    }
+  }
   if (MODE == ZM_TENSOR_Q) {
-    for (int e = threadIdx.x; e < g.Tzq * W; e += blockDim.x) {
-      const int w = e % W, kz = e / W;
+    for (int e = threadIdx.x; e < g.Tzq * W; e += NT) {
+      const int w = e & (W - 1), kz = e >> lgW;
       const int kx = kx0 + w;
       if (kx < Hx)
-        Tq[(static_cast<int64_t>(kz) * g.Tyq + ky) * Hx + kx] = static_cast<double>(buf[w * LS + kz].x) * tscale;
+        Tq[(static_cast<int64_t>(kz) * g.Tyq + kyA) * Hx + kx] = static_cast<double>(buf[w * LS + kz].x) * tscale;
     }
     return;
   }
-  tensor_product<R, false>(buf, LS, W, Pz, kx0, ky, Nhat, Hx, Py, Pz);
-  fft_lines<true, FftCfg<R>::E>(buf, LS, ncompc * W, g.plz, twz, 1);
-  for (int e = threadIdx.x; e < ncompc * nz * W; e += blockDim.x) {
-    const int w = e % W;
-    const int r = e / W;
-    const int kz = r % nz;
-    const int cl = r / nz;
+  tensor_product<R, false, NT>(buf, LS, lgW, Pz, g.fPz, kx0, kyA, Nhat, Hx, Py, Pz);
+  if (kyB >= 0)
+    tensor_product<R, false, NT>(buf + 3 * W * LS, LS, lgW, Pz, g.fPz, kx0, kyB, Nhat, Hx, Py, Pz);
+  buf = fft_lines<true, NT>(buf, buf2, LS, ncl * W, g.plz, twz, 1);
+  for (int e = threadIdx.x; e < ncl * nz * W; e += NT) {
+    const int w = e & (W - 1);
+    const int r = e >> lgW;
+    const int q = fdiv(r, g.fnz);
+    const int kz = r - q * nz;
+    const int row = q / ncompc, cl = q - row * ncompc;
+    const int ky = row == 0 ? kyA : kyB;
     const int kx = kx0 + w;
-    if (kx < Hx) Y[(static_cast<int64_t>(cl * nz + kz) * Py + ky) * Hx + kx] = buf[(cl * W + w) * LS + kz];
+    if (kx < Hx) Y[(static_cast<int64_t>(cl * nz + kz) * Py + ky) * Hx + kx] = buf[(q * W + w) * LS + kz];
   }
 }
 
@@ -402,6 +465,7 @@ int newell_tensor_device(int nx, int ny, int nz, double dx, double dy, double dz
   return static_cast<int>(cudaGetLastError());
 }
 
+
 // ============================================================ host side ====
 template <typename C>
 static C* upload_twiddles(int L, size_t& bytes, cudaStream_t st) {
@@ -419,6 +483,21 @@ static C* upload_twiddles(int L, size_t& bytes, cudaStream_t st) {
   return d;
 }
 
+template <typename R, int NT>
+static void set_smem_attrs_nt() {
+  const int mx = 200 * 1024;
+  cudaFuncSetAttribute(k_fwd_x<R, XM_MAGN, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_fwd_x<R, XM_TENSOR, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_inv_x<R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ypass<R, YM_FWD, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ypass<R, YM_INV, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ypass<R, YM_CONV2D, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ypass<R, YM_TENSOR, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ypass<R, YM_TENSOR_Q, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_zpass<R, ZM_CONV, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_zpass<R, ZM_TENSOR_Q, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+}
+
 template <typename R>
 static void set_smem_attrs() {
   static uint64_t done_mask = 0;  // one bit per device
@@ -426,17 +505,8 @@ static void set_smem_attrs() {
   cudaGetDevice(&dev);
   if (dev < 64 && ((done_mask >> dev) & 1ull)) return;
   if (dev < 64) done_mask |= 1ull << dev;
-  const int mx = 200 * 1024;
-  cudaFuncSetAttribute(k_fwd_x<R, XM_MAGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_fwd_x<R, XM_TENSOR>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_inv_x<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ypass<R, YM_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ypass<R, YM_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ypass<R, YM_CONV2D>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ypass<R, YM_TENSOR>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ypass<R, YM_TENSOR_Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_zpass<R, ZM_CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_zpass<R, ZM_TENSOR_Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  set_smem_attrs_nt<R, kHotNT>();
+  if (sizeof(R) == 8) set_smem_attrs_nt<double, kTensorNT>();
 }
 
 template <typename R>
@@ -460,19 +530,30 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
   g.Hx = g.Px > 1 ? g.Lc + 1 : 1;
   g.Tyq = g.Py / 2 + 1;
   g.Tzq = g.Pz / 2 + 1;
-  // every pass (including the FP64 tensor passes) must fit one block
-  const int cap64 = fft_cap<double>();
-  if (g.Lc > cap64 || g.Py > cap64 || 3 * g.Pz > cap64) {
-    snprintf(err, nerr, "demag: mesh %dx%dx%d exceeds the FFT pass limits (nx<=%d, ny<=%d, nz<=%d)", nx, ny,
-             nz, cap64, cap64 / 2, cap64 / 6);
+  // every hot pass (single-component lines; 3-component z lines) and every
+  // FP64 tensor pass must fit one block
+  const int cap = std::min(hot_cap<R>(), tensor_cap());
+  if (g.Lc > cap || g.Py > cap || 3 * g.Pz > cap) {
+    snprintf(err, nerr, "demag: mesh %dx%dx%d exceeds the FFT pass limits (padded x/2 <= %d, padded y <= %d, padded z <= %d)",
+             nx, ny, nz, cap, cap, cap / 3);
     return -1;
   }
-  if (!make_fft_plan(g.Lc > 0 ? g.Lc : 1, g.plx) || !make_fft_plan(g.Py, g.ply) ||
-      !make_fft_plan(g.Pz, g.plz)) {
+  const int maxr = sizeof(R) == 4 ? 16 : 8;
+  if (!make_fft_plan(g.Lc > 0 ? g.Lc : 1, g.plx, maxr) || !make_fft_plan(g.Py, g.ply, maxr) ||
+      !make_fft_plan(g.Pz, g.plz, maxr)) {
     snprintf(err, nerr, "demag: no radix plan");
     return -1;
   }
-  fused2d = (g.Pz == 1) && (3 * g.Py <= fft_cap<R>());
+  g.fLc = make_fastdiv(std::max(1, g.Lc));
+  g.fHx = make_fastdiv(g.Hx);
+  g.fPy = make_fastdiv(g.Py);
+  g.fPz = make_fastdiv(g.Pz);
+  g.fny = make_fastdiv(ny);
+  g.fnz = make_fastdiv(nz);
+  g.frows = make_fastdiv(ny * nz);
+  g.fpady = make_fastdiv(std::max(1, g.Py - ny));
+  g.fpadz = make_fastdiv(std::max(1, g.Pz - nz));
+  fused2d = (g.Pz == 1) && (3 * g.Py <= hot_cap<R>());
   set_smem_attrs<R>();
   set_smem_attrs<double>();
   const int64_t nX = 3LL * nz * ny * g.Hx;
@@ -494,9 +575,9 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
 }
 
 // ---- launch helpers shared by apply() and the tensor assembly ------------
-template <typename R, int MODE>
-static void launch_fwd_x(const DemagGeom& g, const R* m, const R* Ms, const double* Tr, int tsign,
-                         cplx_t<R>* X, int ncomp, const cplx_t<R>* twx, cudaStream_t st) {
+template <typename R, int MODE, int NT>
+static void launch_fwd_x(const DemagGeom& g, const R* m, const R* Ms, const double* Tr, int tsign, cplx_t<R>* X,
+                         int ncomp, const cplx_t<R>* twx, cudaStream_t st) {
   using C = cplx_t<R>;
   const int rows = g.ny * g.nz;
   const int lines = ncomp * rows;
@@ -504,61 +585,66 @@ static void launch_fwd_x(const DemagGeom& g, const R* m, const R* Ms, const doub
     k_fwd_x1<R, MODE><<<(lines + 255) / 256, 256, 0, st>>>(m, Ms, Tr, X, rows, lines, g.gate);
     return;
   }
-  const int nl = std::max(1, fft_cap<R>() / g.Lc);
+  const int nl = std::max(1, PassCfg<R, NT>::cap / g.Lc);
   const int blocks = (lines + nl - 1) / nl;
-  const size_t sm = sizeof(C) * nl * (g.Lc | 1);
-  k_fwd_x<R, MODE><<<blocks, FftCfg<R>::T, sm, st>>>(m, Ms, Tr, tsign, X, g, lines, nl, twx);
+  const int half = nl * (g.Lc | 1);
+  const size_t sm = 2 * sizeof(C) * half;
+  k_fwd_x<R, MODE, NT><<<blocks, NT, sm, st>>>(m, Ms, Tr, tsign, X, g, lines, nl, twx, half);
 }
 
-template <typename R, int MODE>
-static void launch_ypass(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* out, const R* Nhat,
-                         double* Tq, int ncompc, int ncomp, const cplx_t<R>* twy, int tsign,
-                         double tscale, cudaStream_t st) {
+template <typename R, int MODE, int NT>
+static void launch_ypass(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* out, const R* Nhat, double* Tq,
+                         int ncompc, int ncomp, const cplx_t<R>* twy, int tsign, double tscale, cudaStream_t st) {
   using C = cplx_t<R>;
-  const int W = std::max(1, std::min(g.Hx, fft_cap<R>() / (ncompc * g.Py)));
+  const int W = floor_pow2(std::max(1, std::min(g.Hx, PassCfg<R, NT>::cap / (ncompc * g.Py))));
   dim3 grid((g.Hx + W - 1) / W, g.nz, ncomp / ncompc);
-  const size_t sm = sizeof(C) * ncompc * W * (g.Py | 1);
-  k_ypass<R, MODE><<<grid, FftCfg<R>::T, sm, st>>>(in, out, Nhat, Tq, g, W, ncompc, twy, tsign, tscale);
+  const int half = ncompc * W * (g.Py | 1);
+  const size_t sm = 2 * sizeof(C) * half;
+  k_ypass<R, MODE, NT><<<grid, NT, sm, st>>>(in, out, Nhat, Tq, g, ilog2(W), ncompc, twy, tsign, tscale, half);
 }
 
-template <typename R, int MODE>
-static void launch_zpass(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, double* Tq, int ncompc,
-                         int kyrows, const cplx_t<R>* twz, int tsign, double tscale, cudaStream_t st) {
+template <typename R, int MODE, int NT>
+static void launch_zpass(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, double* Tq, int ncompc, int kyrows,
+                         const cplx_t<R>* twz, int tsign, double tscale, cudaStream_t st) {
   using C = cplx_t<R>;
-  const int W = std::max(1, std::min(g.Hx, fft_cap<R>() / (ncompc * g.Pz)));
+  const int nrow = (MODE == ZM_CONV && g.Py > 2) ? 2 : 1;  // ky and its mirror row
+  const int W = floor_pow2(std::max(1, std::min(g.Hx, PassCfg<R, NT>::cap / (nrow * ncompc * g.Pz))));
   dim3 grid((g.Hx + W - 1) / W, kyrows, 1);
-  const size_t sm = sizeof(C) * ncompc * W * (g.Pz | 1);
-  k_zpass<R, MODE><<<grid, FftCfg<R>::T, sm, st>>>(Y, Nhat, Tq, g, W, ncompc, twz, tsign, tscale);
+  const int half = nrow * ncompc * W * (g.Pz | 1);
+  const size_t sm = 2 * sizeof(C) * half;
+  k_zpass<R, MODE, NT><<<grid, NT, sm, st>>>(Y, Nhat, Tq, g, ilog2(W), ncompc, twz, tsign, tscale, half);
 }
 
 template <typename R>
 static bool run_pass(const DemagPlan<R>& p, DemagGeom g, int which, const R* m, const R* mu0Ms, R* Hd,
                      cudaStream_t st) {
   using C = cplx_t<R>;
+  constexpr int NT = kHotNT;
   switch (which) {
     case 0:
-      launch_fwd_x<R, XM_MAGN>(g, m, mu0Ms, nullptr, 1, p.X, 3, p.twx, st);
+      launch_fwd_x<R, XM_MAGN, NT>(g, m, mu0Ms, nullptr, 1, p.X, 3, p.twx, st);
       return true;
     case 1:
       if (p.fused2d) return false;
-      launch_ypass<R, YM_FWD>(g, p.X, p.Y, p.Nhat, nullptr, 1, 3, p.twy, 1, 0.0, st);
+      launch_ypass<R, YM_FWD, NT>(g, p.X, p.Y, p.Nhat, nullptr, 1, 3, p.twy, 1, 0.0, st);
       return true;
     case 2:
-      if (p.fused2d) launch_ypass<R, YM_CONV2D>(g, p.X, p.X, p.Nhat, nullptr, 3, 3, p.twy, 1, 0.0, st);
-      else launch_zpass<R, ZM_CONV>(g, p.Y, p.Nhat, nullptr, 3, g.Py, p.twz, 1, 0.0, st);
+      if (p.fused2d) launch_ypass<R, YM_CONV2D, NT>(g, p.X, p.X, p.Nhat, nullptr, 3, 3, p.twy, 1, 0.0, st);
+      else launch_zpass<R, ZM_CONV, NT>(g, p.Y, p.Nhat, nullptr, 3, g.Py / 2 + 1, p.twz, 1, 0.0, st);
       return true;
     case 3:
       if (p.fused2d) return false;
-      launch_ypass<R, YM_INV>(g, p.Y, p.X, p.Nhat, nullptr, 1, 3, p.twy, 1, 0.0, st);
+      launch_ypass<R, YM_INV, NT>(g, p.Y, p.X, p.Nhat, nullptr, 1, 3, p.twy, 1, 0.0, st);
       return true;
     case 4: {
       const int lines = 3 * g.ny * g.nz;
       if (g.Px == 1) {
         k_inv_x1<R><<<(lines + 255) / 256, 256, 0, st>>>(p.X, Hd, lines, g.gate);
       } else {
-        const int nl = std::max(1, fft_cap<R>() / g.Lc);
-        const size_t sm = sizeof(C) * nl * (g.Lc | 1);
-        k_inv_x<R><<<(lines + nl - 1) / nl, FftCfg<R>::T, sm, st>>>(p.X, Hd, g, lines, nl, p.twx);
+        const int nl = std::max(1, PassCfg<R, NT>::cap / g.Lc);
+        const int half = nl * (g.Lc | 1);
+        const size_t sm = 2 * sizeof(C) * half;
+        k_inv_x<R, NT><<<(lines + nl - 1) / nl, NT, sm, st>>>(p.X, Hd, g, lines, nl, p.twx, half);
       }
       return true;
     }
@@ -606,6 +692,7 @@ int DemagPlan<R>::launches_per_apply() const {
 template <typename R>
 int DemagPlan<R>::set_tensor(const double* T6N, cudaStream_t st) {
   using C64 = double2;
+  constexpr int NT = kTensorNT;
   size_t b64 = 0;
   C64 *tx = nullptr, *ty = nullptr, *tz = nullptr, *X64 = nullptr, *Y64 = nullptr;
   double* Tq = nullptr;
@@ -613,6 +700,11 @@ int DemagPlan<R>::set_tensor(const double* T6N, cudaStream_t st) {
   const int64_t nX = static_cast<int64_t>(g.nz) * g.ny * g.Hx;
   const int64_t nY = static_cast<int64_t>(g.nz) * g.Py * g.Hx;
   const int64_t Ts = static_cast<int64_t>(g.Tzq) * g.Tyq * g.Hx;
+  // FP64 plans (radix <= 8) for the same lengths
+  DemagGeom g64 = g;
+  make_fft_plan(g.Lc > 0 ? g.Lc : 1, g64.plx, 8);
+  make_fft_plan(g.Py, g64.ply, 8);
+  make_fft_plan(g.Pz, g64.plz, 8);
   int rc = 0;
   if (g.Px > 1 && !(tx = upload_twiddles<C64>(g.Px, b64, st))) rc = 2;
   if (!rc && !(ty = upload_twiddles<C64>(g.Py, b64, st))) rc = 2;
@@ -624,12 +716,12 @@ int DemagPlan<R>::set_tensor(const double* T6N, cudaStream_t st) {
     const double scale = -1.0 / (kMu0 * static_cast<double>(g.Px) * g.Py * g.Pz);
     for (int c = 0; c < 6; ++c) {
       const int sx = odd_axis(c, 0) ? -1 : 1, sy = odd_axis(c, 1) ? -1 : 1, sz = odd_axis(c, 2) ? -1 : 1;
-      launch_fwd_x<double, XM_TENSOR>(g, nullptr, nullptr, T6N + c * N, sx, X64, 1, tx, st);
+      launch_fwd_x<double, XM_TENSOR, NT>(g64, nullptr, nullptr, T6N + c * N, sx, X64, 1, tx, st);
       if (g.Pz == 1) {
-        launch_ypass<double, YM_TENSOR_Q>(g, X64, nullptr, nullptr, Tq + c * Ts, 1, 1, ty, sy, scale, st);
+        launch_ypass<double, YM_TENSOR_Q, NT>(g64, X64, nullptr, nullptr, Tq + c * Ts, 1, 1, ty, sy, scale, st);
       } else {
-        launch_ypass<double, YM_TENSOR>(g, X64, Y64, nullptr, nullptr, 1, 1, ty, sy, 0.0, st);
-        launch_zpass<double, ZM_TENSOR_Q>(g, Y64, nullptr, Tq + c * Ts, 1, g.Tyq, tz, sz, scale, st);
+        launch_ypass<double, YM_TENSOR, NT>(g64, X64, Y64, nullptr, nullptr, 1, 1, ty, sy, 0.0, st);
+        launch_zpass<double, ZM_TENSOR_Q, NT>(g64, Y64, nullptr, Tq + c * Ts, 1, g.Tyq, tz, sz, scale, st);
       }
     }
     k_cast<R><<<1024, 256, 0, st>>>(Tq, Nhat, 6 * Ts);

@@ -24,6 +24,7 @@ struct DemagGeom {
   int Lc, Hx;      // Lc = Px/2 (0 when Px == 1), Hx = Lc + 1 (1 when Px == 1)
   int Tyq, Tzq;    // Py/2 + 1, Pz/2 + 1
   FftPlan1 plx, ply, plz;
+  FastDiv fLc, fHx, fPy, fPz, fny, fnz, frows, fpady, fpadz;
   const int* gate;  // device flag: kernels return at once when *gate == 0 (null: always run)
 };
 

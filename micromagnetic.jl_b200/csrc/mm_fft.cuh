@@ -6,10 +6,9 @@
 //     v[r] = x[i + r*L/R] * exp(s*2*pi*i * r*(i mod p) / (p*R)),   r = 0..R-1
 //     v    = DFT_R(v)
 //     y[(i - i mod p)*R + (i mod p) + r*p] = v[r]
-// and leaves the result in natural order after the last stage.  Each stage
-// is done in place: every thread first loads its butterflies into registers,
-// the block synchronises, then all threads store.  The caller guarantees
-// nlines*L <= E*blockDim.x so that one register pass covers a stage.
+// and leaves the result in natural order after the last stage.  Stages
+// ping-pong between two shared buffers, so a thread holds one butterfly at a
+// time.  Power-of-two lengths take shift/mask index arithmetic.
 //
 // Twiddles come from a table tw[t] = exp(-2*pi*i*t / (L*tw_mul)) held in
 // global memory (read through the read-only cache); tw_mul = 2 lets the
@@ -19,14 +18,16 @@
 
 namespace mm {
 
-// cos/sin of 2*pi*k/n for the odd-prime butterflies (mathematical constants)
+// cos/sin of 2*pi*k/n for the odd-prime and radix-16 butterflies (mathematical constants)
 constexpr double kS3 = 0.86602540378443864676;  // sin(2pi/3)
 constexpr double kC51 = 0.30901699437494742410, kS51 = 0.95105651629515357212;
 constexpr double kC52 = -0.80901699437494742410, kS52 = 0.58778525229247312917;
 constexpr double kC71 = 0.62348980185873353053, kS71 = 0.78183148246802980871;
 constexpr double kC72 = -0.22252093395631440429, kS72 = 0.97492791218182360702;
 constexpr double kC73 = -0.90096886790241912624, kS73 = 0.43388373911755812048;
-constexpr double kR2 = 0.70710678118654752440;  // sqrt(2)/2
+constexpr double kR2 = 0.70710678118654752440;   // cos(pi/4)
+constexpr double kC16 = 0.92387953251128675613;  // cos(pi/8)
+constexpr double kS16 = 0.38268343236508977173;  // sin(pi/8)
 
 template <bool INV, typename C> __device__ __forceinline__ void dft2(C* v) {
   C a = v[0], b = v[1];
@@ -62,6 +63,42 @@ template <bool INV, typename C> __device__ __forceinline__ void dft8(C* v) {
   v[6] = csub(e[2], o2);
   v[3] = cadd(e[3], o3);
   v[7] = csub(e[3], o3);
+}
+
+// 16 = 4 x 4: DFT4 over the four residues mod 4, twiddles w16^(r*k1), DFT4 over r
+template <bool INV, typename C> __device__ __forceinline__ void dft16(C* v) {
+  using R = decltype(C::x);
+  C a[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    a[r][0] = v[r];
+    a[r][1] = v[r + 4];
+    a[r][2] = v[r + 8];
+    a[r][3] = v[r + 12];
+    dft4<INV>(a[r]);
+  }
+  const R s = INV ? R(1) : R(-1);
+  const R c1 = static_cast<R>(kC16), s1 = static_cast<R>(kS16), h = static_cast<R>(kR2);
+  // w16^1, w16^2, w16^3, w16^4 = s i, w16^6 = h(-1 + s i), w16^9 = -w16^1
+  const C w1 = cmk<C>(c1, s * s1), w2 = cmk<C>(h, s * h), w3 = cmk<C>(s1, s * c1);
+  a[1][1] = cmul(a[1][1], w1);
+  a[1][2] = cmul(a[1][2], w2);
+  a[1][3] = cmul(a[1][3], w3);
+  a[2][1] = cmul(a[2][1], w2);
+  a[2][2] = crot<INV>(a[2][2]);
+  a[2][3] = cmul(a[2][3], cmk<C>(-h, s * h));
+  a[3][1] = cmul(a[3][1], w3);
+  a[3][2] = cmul(a[3][2], cmk<C>(-h, s * h));
+  a[3][3] = cmul(a[3][3], cmk<C>(-c1, -s * s1));
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    C t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+    dft4<INV>(t);
+    v[k1] = t[0];
+    v[k1 + 4] = t[1];
+    v[k1 + 8] = t[2];
+    v[k1 + 12] = t[3];
+  }
 }
 
 template <bool INV, typename C> __device__ __forceinline__ void dft3(C* v) {
@@ -119,71 +156,81 @@ template <int R, bool INV, typename C> __device__ __forceinline__ void dftR(C* v
   else if constexpr (R == 4) dft4<INV>(v);
   else if constexpr (R == 5) dft5<INV>(v);
   else if constexpr (R == 7) dft7<INV>(v);
-  else dft8<INV>(v);
+  else if constexpr (R == 8) dft8<INV>(v);
+  else dft16<INV>(v);
 }
 
-template <int R, bool INV, int E, typename C>
-__device__ __forceinline__ void fft_stage(C* buf, int L, int LS, int nlines, int p,
-                                          const C* __restrict__ tw, int tw_mul) {
-  constexpr int MB = (E + R - 1) / R;
+template <int R, bool INV, bool POW2, int NT, typename C>
+__device__ __forceinline__ void fft_stage(const C* __restrict__ src, C* __restrict__ dst, int L, int LS, int nlines,
+                                          int p, const C* __restrict__ tw, int tw_mul) {
   const int T = L / R;
   const int total = nlines * T;
   const int twstep = (L / (p * R)) * tw_mul;
-  C v[MB][R];
-  int dst[MB];
+  const int lgT = POW2 ? __ffs(T) - 1 : 0;
+  for (int idx = threadIdx.x; idx < total; idx += NT) {
+    int line, i, k;
+    if (POW2) {
+      line = idx >> lgT;
+      i = idx & (T - 1);
+      k = i & (p - 1);
+    } else {
+      line = idx / T;
+      i = idx - line * T;
+      k = i % p;
+    }
+    C v[R];
+    const C* s = src + line * LS + i;
 #pragma unroll
-  for (int b = 0; b < MB; ++b) {
-    const int idx = threadIdx.x + b * blockDim.x;
-    dst[b] = -1;
-    if (idx < total) {
-      const int line = idx / T;
-      const int i = idx - line * T;
-      const int k = i % p;
-      const C* src = buf + line * LS + i;
+    for (int r = 0; r < R; ++r) v[r] = s[r * T];
+    if (p > 1) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[b][r] = src[r * T];
-      if (p > 1) {
-#pragma unroll
-        for (int r = 1; r < R; ++r) {
-          C w = __ldg(tw + r * k * twstep);
-          if (INV) w.y = -w.y;
-          v[b][r] = cmul(v[b][r], w);
-        }
+      for (int r = 1; r < R; ++r) {
+        C w = __ldg(tw + r * k * twstep);
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
       }
-      dftR<R, INV>(v[b]);
-      dst[b] = line * LS + (i - k) * R + k;
     }
-  }
-  __syncthreads();
+    dftR<R, INV>(v);
+    C* d = dst + line * LS + (i - k) * R + k;
 #pragma unroll
-  for (int b = 0; b < MB; ++b) {
-    if (dst[b] >= 0) {
-#pragma unroll
-      for (int r = 0; r < R; ++r) buf[dst[b] + r * p] = v[b][r];
-    }
+    for (int r = 0; r < R; ++r) d[r * p] = v[r];
   }
   __syncthreads();
 }
 
-// Transforms nlines lines of length pl.L stored at buf[line*LS + t].
-// Must be called by every thread of the block.
-template <bool INV, int E, typename C>
-__device__ void fft_lines(C* buf, int LS, int nlines, const FftPlan1 pl, const C* __restrict__ tw,
-                          int tw_mul) {
+template <bool INV, bool POW2, int NT, typename C>
+__device__ __forceinline__ C* fft_lines_impl(C* a, C* b, int LS, int nlines, const FftPlan1 pl,
+                                             const C* __restrict__ tw, int tw_mul) {
   int p = 1;
   const int L = pl.L;
   for (int s = 0; s < pl.nst; ++s) {
     const int R = plan_radix(pl, s);
     switch (R) {
-      case 8: fft_stage<8, INV, E>(buf, L, LS, nlines, p, tw, tw_mul); break;
-      case 7: fft_stage<7, INV, E>(buf, L, LS, nlines, p, tw, tw_mul); break;
-      case 5: fft_stage<5, INV, E>(buf, L, LS, nlines, p, tw, tw_mul); break;
-      case 4: fft_stage<4, INV, E>(buf, L, LS, nlines, p, tw, tw_mul); break;
-      case 3: fft_stage<3, INV, E>(buf, L, LS, nlines, p, tw, tw_mul); break;
-      default: fft_stage<2, INV, E>(buf, L, LS, nlines, p, tw, tw_mul); break;
+      case 16:
+        if constexpr (sizeof(decltype(C::x)) == 4) fft_stage<16, INV, POW2, NT>(a, b, L, LS, nlines, p, tw, tw_mul);
+        break;
+      case 8: fft_stage<8, INV, POW2, NT>(a, b, L, LS, nlines, p, tw, tw_mul); break;
+      case 7: fft_stage<7, INV, false, NT>(a, b, L, LS, nlines, p, tw, tw_mul); break;
+      case 5: fft_stage<5, INV, false, NT>(a, b, L, LS, nlines, p, tw, tw_mul); break;
+      case 4: fft_stage<4, INV, POW2, NT>(a, b, L, LS, nlines, p, tw, tw_mul); break;
+      case 3: fft_stage<3, INV, false, NT>(a, b, L, LS, nlines, p, tw, tw_mul); break;
+      default: fft_stage<2, INV, POW2, NT>(a, b, L, LS, nlines, p, tw, tw_mul); break;
     }
+    C* t = a;
+    a = b;
+    b = t;
     p *= R;
   }
+  return a;
+}
+
+// Transforms nlines lines of length pl.L stored at a[line*LS + t], using b as
+// the second buffer of the ping-pong; returns the buffer holding the result
+// (a or b).  Must be called by every thread of the block.
+template <bool INV, int NT, typename C>
+__device__ C* fft_lines(C* a, C* b, int LS, int nlines, const FftPlan1 pl, const C* __restrict__ tw, int tw_mul) {
+  if (pl.pow2) return fft_lines_impl<INV, true, NT>(a, b, LS, nlines, pl, tw, tw_mul);
+  return fft_lines_impl<INV, false, NT>(a, b, LS, nlines, pl, tw, tw_mul);
 }
 
 }  // namespace mm

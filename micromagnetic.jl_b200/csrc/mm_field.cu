@@ -9,6 +9,20 @@ constexpr int kStageThreads = 256;
 
 int stage_blocks(int64_t N) { return static_cast<int>((N + kStageThreads - 1) / kStageThreads); }
 
+// Stage kernels run one thread per cell on a 3-D grid: blocks of BX x BY
+// cells of one z plane (BX*BY = 256, BY up to 8 so that the y neighbours of
+// a block are mostly its own rows).
+StageGrid stage_grid(int nx, int ny, int nz) {
+  StageGrid g;
+  int by = 1;
+  while (by < 8 && by < ny) by *= 2;
+  const int bx = kStageThreads / by;
+  g.block = dim3(bx, by, 1);
+  g.grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
+  g.nblocks = static_cast<int>(g.grid.x * g.grid.y * g.grid.z);
+  return g;
+}
+
 // ------------------------------------------------- compensated FP32 math ---
 // Error-free transforms (Knuth two-sum, FMA two-product) used to keep the FP32
 // form's integrator state m = hi + lo at well beyond FP32 precision.
@@ -112,11 +126,11 @@ void launch_nbmask(int nx, int ny, int nz, int pbc, const R* Ms, uint8_t* nbm, c
 // 226-304, bulk DMI 306-344, interfacial DMI 426-466) and the demag energy of
 // src/micro/demag.jl:435-456; terms with Ms == 0 contribute nothing.
 template <typename R, bool ENERGY>
-__device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __restrict__ y, int64_t I,
-                                          R m[3], R h[3], double* e) {
+__device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __restrict__ y, int I, int i, int j,
+                                          int k, R m[3], R h[3], double* e) {
   const int64_t N = a.N;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const int64_t nxy = static_cast<int64_t>(nx) * ny;
+  const int nxy = nx * ny;
   m[0] = y[I];
   m[1] = y[N + I];
   m[2] = y[2 * N + I];
@@ -128,14 +142,13 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
     for (int t = 0; t < kNTerms; ++t) e[t] = 0.0;
   }
   if (Ms != R(0) && (mask & (TB_EXCH | TB_DMI_BULK | TB_DMI_INTERFACIAL | TB_ANIS))) {
-    const int i = static_cast<int>(I % nx), j = static_cast<int>((I / nx) % ny), k = static_cast<int>(I / nxy);
     const bool px = a.pbc & 1, py = a.pbc & 2, pz = a.pbc & 4;
     const unsigned nbm = a.nbm[I];
-    int64_t nb[6];
+    int nb[6];
     nb[0] = i > 0 ? I - 1 : (px ? I + nx - 1 : -1);
     nb[1] = i < nx - 1 ? I + 1 : (px ? I - (nx - 1) : -1);
-    nb[2] = j > 0 ? I - nx : (py ? I + static_cast<int64_t>(ny - 1) * nx : -1);
-    nb[3] = j < ny - 1 ? I + nx : (py ? I - static_cast<int64_t>(ny - 1) * nx : -1);
+    nb[2] = j > 0 ? I - nx : (py ? I + (ny - 1) * nx : -1);
+    nb[3] = j < ny - 1 ? I + nx : (py ? I - (ny - 1) * nx : -1);
     nb[4] = k > 0 ? I - nxy : (pz ? I + (nz - 1) * nxy : -1);
     nb[5] = k < nz - 1 ? I + nxy : (pz ? I - (nz - 1) * nxy : -1);
     const R Ms_inv = R(1) / Ms;
@@ -143,7 +156,7 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
 #pragma unroll
     for (int d = 0; d < 6; ++d) {
       if ((nbm >> d) & 1u) {
-        const int64_t q = nb[d];
+        const int q = nb[d];
         mn[d][0] = __ldg(y + q);
         mn[d][1] = __ldg(y + N + q);
         mn[d][2] = __ldg(y + 2 * N + q);
@@ -267,7 +280,7 @@ __device__ __forceinline__ void llg_rhs(const FieldArgs<R>& a, int64_t I, const 
     return;
   }
   const R alpha = a.alpha;
-  const R c = -a.gamma / (1 + alpha * alpha);
+  const R c = a.llg_c, cl = a.llg_c_lo;
   const R mm = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
   const R mh = m[0] * h[0] + m[1] * h[1] + m[2] * h[2];
   const R h1 = mm * h[0] - mh * m[0];
@@ -279,9 +292,10 @@ __device__ __forceinline__ void llg_rhs(const FieldArgs<R>& a, int64_t I, const 
     f2 = m[2] * h1 - m[0] * h3;
     f3 = -m[1] * h1 + m[0] * h2;
   }
-  f[0] = c * (f1 - h1 * alpha);
-  f[1] = c * (f2 - h2 * alpha);
-  f[2] = c * (f3 - h3 * alpha);
+  const R g1 = f1 - h1 * alpha, g2 = f2 - h2 * alpha, g3 = f3 - h3 * alpha;
+  f[0] = c * g1 + cl * g1;
+  f[1] = c * g2 + cl * g2;
+  f[2] = c * g3 + cl * g3;
 }
 
 // Dormand-Prince 5(4) tableau (src/integrator/adaptive_rk_steps.jl:49-57)
@@ -295,17 +309,22 @@ __constant__ double c_dp_a[6][6] = {
 __constant__ double c_dp_w[7] = {71.0 / 57600, 0, -71.0 / 16695, 71.0 / 1920, -17253.0 / 339200, 22.0 / 525, -1.0 / 40};
 
 template <typename R, int MODE>
-__global__ void __launch_bounds__(kStageThreads) k_stage(FieldArgs<R> a, const R* __restrict__ y, StageArgs<R> s) {
+__global__ void __launch_bounds__(kStageThreads, 3) k_stage(FieldArgs<R> a, const R* __restrict__ y, StageArgs<R> s) {
   constexpr bool kF32 = sizeof(R) == 4;
   if (MODE == SM_DOPRI && !s.ctrl->active) return;
   const int64_t N = a.N;
-  const int64_t I = blockIdx.x * static_cast<int64_t>(kStageThreads) + threadIdx.x;
-  const bool live = I < N;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const bool live = i < a.nx && j < a.ny;
+  const int I = (k * a.ny + j) * a.nx + i;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int blin = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   double e[kNTerms];
   R m[3], h[3];
   double red = 0.0;  // SM_DOPRI stage 7: error max
   if (live) {
-    cell_heff<R, MODE == SM_ENERGY || MODE == SM_FIELD>(a, y, I, m, h, e);
+    cell_heff<R, MODE == SM_ENERGY || MODE == SM_FIELD>(a, y, I, i, j, k, m, h, e);
     if (MODE == SM_FIELD) {
       s.out[I] = h[0];
       s.out[N + I] = h[1];
@@ -445,7 +464,7 @@ __global__ void __launch_bounds__(kStageThreads) k_stage(FieldArgs<R> a, const R
   if (MODE == SM_ENERGY || (MODE == SM_DOPRI && s.stage == 7)) {
     // deterministic block reduction in FP64
     __shared__ double sh[kStageThreads / 32][kNTerms];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = tid & 31, warp = tid >> 5;
     constexpr int W = MODE == SM_ENERGY ? kNTerms : 1;
     double v[W];
 #pragma unroll
@@ -460,27 +479,27 @@ __global__ void __launch_bounds__(kStageThreads) k_stage(FieldArgs<R> a, const R
       if (lane == 0) sh[warp][t] = v[t];
     }
     __syncthreads();
-    if (threadIdx.x < W) {
-      double acc = MODE == SM_ENERGY ? 0.0 : 0.0;
+    if (tid < W) {
+      double acc = 0.0;
       for (int w = 0; w < kStageThreads / 32; ++w) {
-        const double u = sh[w][threadIdx.x];
+        const double u = sh[w][tid];
         if (MODE == SM_ENERGY) acc += u;
         else acc = (u > acc || isnan(u)) ? u : acc;
       }
-      s.partials[blockIdx.x * W + threadIdx.x] = acc;
+      s.partials[blin * W + tid] = acc;
     }
   }
 }
 
 template <typename R>
 void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<R>& sa, cudaStream_t st) {
-  const int nb = stage_blocks(fa.N);
+  const StageGrid g = stage_grid(fa.nx, fa.ny, fa.nz);
   switch (mode) {
-    case SM_FIELD: k_stage<R, SM_FIELD><<<nb, kStageThreads, 0, st>>>(fa, y, sa); break;
-    case SM_RHS: k_stage<R, SM_RHS><<<nb, kStageThreads, 0, st>>>(fa, y, sa); break;
-    case SM_RK4: k_stage<R, SM_RK4><<<nb, kStageThreads, 0, st>>>(fa, y, sa); break;
-    case SM_ENERGY: k_stage<R, SM_ENERGY><<<nb, kStageThreads, 0, st>>>(fa, y, sa); break;
-    default: k_stage<R, SM_DOPRI><<<nb, kStageThreads, 0, st>>>(fa, y, sa); break;
+    case SM_FIELD: k_stage<R, SM_FIELD><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+    case SM_RHS: k_stage<R, SM_RHS><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+    case SM_RK4: k_stage<R, SM_RK4><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+    case SM_ENERGY: k_stage<R, SM_ENERGY><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+    default: k_stage<R, SM_DOPRI><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
   }
 }
 

@@ -46,8 +46,10 @@ template <typename R> struct FieldArgs {
   const R* Hz;
   // demag field (SoA, written by the FFT passes)
   const R* Hd;
-  // LLG
-  R alpha, gamma;
+  // LLG: c = -gamma/(1 + alpha^2) evaluated in FP64 on the host and passed
+  // as c + c_lo (c_lo = 0 in the FP64 form) so that the FP32 form carries no
+  // systematic precession-frequency error from rounding the constant
+  R alpha, llg_c, llg_c_lo;
   int precession;
   const uint8_t* pins;
 };
@@ -88,6 +90,12 @@ template <typename R>
 void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<R>& sa, cudaStream_t st);
 
 int stage_blocks(int64_t N);
+
+struct StageGrid {
+  dim3 grid, block;
+  int nblocks;
+};
+StageGrid stage_grid(int nx, int ny, int nz);
 
 template <typename R>
 void launch_nbmask(int nx, int ny, int nz, int pbc, const R* Ms, uint8_t* nbm, cudaStream_t st);

@@ -248,19 +248,26 @@ def test_fp32_form_fields(mesh):
     assert abs(t32 - t64) <= TOL32 * np.abs(p64).sum()
 
 
-def test_fp32_form_rk4_1000_steps():
-    """FP32 form vs FP64 form after 1000 RK4 steps (dt = 1e-13) on a film with
-    exchange, Zeeman and demag (the 200x50x1 workload, reduced to 64x32x1)."""
-    rng = np.random.default_rng(101)
-    nx, ny, nz = 64, 32, 1
+def smooth_film_cfg(nx=64, ny=32):
+    """Film with exchange, in-plane Zeeman (30 mT) and demag started from a
+    smooth non-uniform state: its dynamics are not chaotic (a 1e-10
+    perturbation of the FP64 oracle stays ~1e-10 over 1000 steps while m
+    rotates by O(1)), so FP32-vs-FP64 differences measure arithmetic error."""
     n = nx * ny
-    m = rng.normal(size=(n, 3))
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    X, Y = np.meshgrid(x, y)
+    th = 0.4 * np.sin(2 * np.pi * X) + 0.2 * np.cos(2 * np.pi * Y)
+    m = np.stack([np.cos(th), np.sin(th), 0.1 * np.sin(2 * np.pi * (X + Y))], -1).reshape(-1, 3)
     m /= np.linalg.norm(m, axis=1, keepdims=True)
-    B = rng.uniform(0, 0.03)
-    phi = rng.uniform(0, 2 * np.pi)
-    H = np.tile([B / (4e-7 * np.pi) * np.cos(phi), B / (4e-7 * np.pi) * np.sin(phi), 0.0], n)
-    cfg = dict(nx=nx, ny=ny, nz=nz, dx=2.5e-9, dy=2.5e-9, dz=3e-9, pbc="", Ms=np.full(n, 8e5), m=m.reshape(-1),
-               terms=["exch", "zeeman", "demag"], A=1.3e-11, H=H, alpha=0.02, gamma=2.211e5)
+    H = np.tile([0.03 / (4e-7 * np.pi) * 0.8, 0.03 / (4e-7 * np.pi) * 0.6, 0.0], n)
+    return dict(nx=nx, ny=ny, nz=1, dx=2.5e-9, dy=2.5e-9, dz=3e-9, pbc="", Ms=np.full(n, 8e5), m=m.reshape(-1),
+                terms=["exch", "zeeman", "demag"], A=1.3e-11, H=H, alpha=0.02, gamma=2.211e5)
+
+
+def test_fp32_form_rk4_1000_steps():
+    """FP32 form vs FP64 form after 1000 RK4 steps (dt = 1e-13) on the smooth film."""
+    cfg = smooth_film_cfg()
     g64 = GpuSim(cfg, form=0)
     g32 = GpuSim(cfg, form=1)
     g64.rk4(1e-13, 1000)
@@ -268,3 +275,14 @@ def test_fp32_form_rk4_1000_steps():
     err = rel_maxnorm(g32.m(), g64.m())
     print("fp32 vs fp64 after 1000 RK4 steps:", err)
     assert err <= TOL32
+
+
+def test_fp32_form_rk4_random_state_short_horizon():
+    """From random m the dynamics are chaotic (test_chaos_random_state in
+    test_oracle_dynamics.py); over 50 steps FP32 stays within 1e-5 of FP64."""
+    cfg = random_config(101, 64, 32, 1, "", holes=False, terms=("exch", "zeeman", "demag"), spatial=False)
+    g64 = GpuSim(cfg, form=0)
+    g32 = GpuSim(cfg, form=1)
+    g64.rk4(1e-14, 50)
+    g32.rk4(1e-14, 50)
+    assert rel_maxnorm(g32.m(), g64.m()) <= TOL32

@@ -33,8 +33,8 @@ template <bool INV, typename C> __device__ __forceinline__ C crot(C a) {
 // ------------------------------------------------------------ FFT plans -----
 constexpr int kMaxStages = 16;
 // Radix sequence of a 1-D transform, 3 bits per stage (stage s in bits
-// 3s..3s+2: 1=2 2=3 3=4 4=5 5=7 6=8 7=16), so that device code decodes it
-// without an indexed array.
+// 3s..3s+2: 0=32 1=2 2=3 3=4 4=5 5=7 6=8 7=16), so that device code decodes
+// it without an indexed array.
 struct FftPlan1 {
   int L;                    // complex transform length (1 = identity)
   int nst;                  // number of radix stages
@@ -43,7 +43,7 @@ struct FftPlan1 {
 };
 __host__ __device__ __forceinline__ int plan_radix(const FftPlan1& p, int s) {
   const int c = static_cast<int>((p.code >> (3 * s)) & 7ull);
-  return c == 1 ? 2 : c == 2 ? 3 : c == 3 ? 4 : c == 4 ? 5 : c == 5 ? 7 : c == 6 ? 8 : 16;
+  return c == 0 ? 32 : c == 1 ? 2 : c == 2 ? 3 : c == 3 ? 4 : c == 4 ? 5 : c == 5 ? 7 : c == 6 ? 8 : 16;
 }
 
 inline int radix_code(int r) {
@@ -54,7 +54,8 @@ inline int radix_code(int r) {
     case 5: return 4;
     case 7: return 5;
     case 8: return 6;
-    default: return 7;
+    case 16: return 7;
+    default: return 0;  // 32
   }
 }
 

@@ -1,11 +1,13 @@
 // mm_demag.cu -- demag tensor assembly (FP64) and FFT convolution passes.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "mm_demag.cuh"
 #include "mm_fft.cuh"
+#include "mm_lines.cuh"
 
 namespace mm {
 
@@ -42,6 +44,18 @@ static int ilog2(int v) {
   while ((1 << l) < v) ++l;
   return l;
 }
+
+// Shared-memory budget of one strided-pass block; the kx tile W is the
+// largest power of two (up to 128 bytes of row segment) that fits.
+static int smem_budget_bytes() {
+  static int v = [] {
+    const char* e = getenv("MMCUDA_LINES_SMEM_KB");
+    const int kb = e ? atoi(e) : 100;
+    return (kb > 8 && kb <= 200 ? kb : 100) * 1024;
+  }();
+  return v;
+}
+
 
 // ============================================================== kernels ====
 enum XMode { XM_MAGN = 0, XM_TENSOR = 1 };
@@ -365,6 +379,66 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_zpass(
   }
 }
 
+// ---- hot-path strided passes (fused global I/O, line-fastest mapping) -----
+enum YLMode { YL_FWD = 0, YL_INV = 1, YL_CONV2D = 2 };
+
+// y lines of one z plane over a W-wide kx tile.  grid: (tiles, nz, 3/ncompc)
+//   YL_FWD:    X rows y < ny            -> Y rows 0..Py-1
+//   YL_INV:    Y rows 0..Py-1           -> X rows y < ny
+//   YL_CONV2D: X rows y < ny, forward y, tensor product (kz = 0), inverse y -> X
+template <typename R, int MODE, int NT>
+__global__ void __launch_bounds__(NT, 2) k_ylines(const cplx_t<R>* in, cplx_t<R>* out, const R* __restrict__ Nhat,
+                                                  DemagGeom g, int lgW, int ncompc, FastDiv fnl,
+                                                  const cplx_t<R>* __restrict__ twy, int half) {
+  using C = cplx_t<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* a = reinterpret_cast<C*>(smem_raw);
+  C* b = a + half;
+  if (g.gate && !*g.gate) return;
+  const int Py = g.Py, LS = Py | 1, Hx = g.Hx, ny = g.ny, nz = g.nz;
+  const int W = 1 << lgW;
+  const int kx0 = blockIdx.x * W, z = blockIdx.y, c0 = blockIdx.z * ncompc;
+  const int nlines = ncompc * W;
+  const int rin = MODE == YL_INV ? Py : ny, rout = MODE == YL_FWD ? Py : ny;
+  RowsIn<C> src{in + static_cast<int64_t>(c0 * nz + z) * rin * Hx, static_cast<int64_t>(nz) * rin * Hx, Hx, lgW, kx0,
+                Hx, rin};
+  RowsOut<C> dst{out + static_cast<int64_t>(c0 * nz + z) * rout * Hx, static_cast<int64_t>(nz) * rout * Hx, Hx, lgW,
+                 kx0, Hx, rout};
+  if (MODE == YL_CONV2D) {
+    C* res = line_fft_to_smem<false, NT>(src, a, b, LS, nlines, fnl, g.ply, twy, 1);
+    tensor_product<R, true, NT>(res, LS, lgW, Py, g.fPy, kx0, 0, Nhat, Hx, Py, g.Pz);
+    line_fft_from_smem<true, NT>(res, res == a ? b : a, dst, LS, nlines, fnl, g.ply, twy, 1);
+  } else {
+    line_fft<MODE == YL_INV, NT>(src, dst, a, b, LS, nlines, fnl, g.ply, twy, 1);
+  }
+}
+
+// z lines (forward z, tensor product, inverse z, in place on Y) of one ky row
+// over a W-wide kx tile.  grid: (tiles, Py); consecutive blockIdx.y take ky
+// and Py - ky so the two reads of each tensor entry are close in time (L2).
+template <typename R, int NT>
+__global__ void __launch_bounds__(NT, 2) k_zconv(cplx_t<R>* Y, const R* __restrict__ Nhat, DemagGeom g, int lgW,
+                                                 FastDiv fnl, const cplx_t<R>* __restrict__ twz, int half) {
+  using C = cplx_t<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* a = reinterpret_cast<C*>(smem_raw);
+  C* b = a + half;
+  if (g.gate && !*g.gate) return;
+  const int Pz = g.Pz, LS = Pz | 1, Hx = g.Hx, Py = g.Py, nz = g.nz;
+  const int W = 1 << lgW;
+  const int kx0 = blockIdx.x * W;
+  const int bq = blockIdx.y;
+  const int q = (bq + 1) >> 1;
+  const int ky = bq == 0 ? 0 : ((bq & 1) ? q : Py - q);
+  const int nlines = 3 * W;
+  const int64_t cs = static_cast<int64_t>(nz) * Py * Hx, rs = static_cast<int64_t>(Py) * Hx;
+  RowsIn<C> src{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
+  RowsOut<C> dst{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
+  C* res = line_fft_to_smem<false, NT>(src, a, b, LS, nlines, fnl, g.plz, twz, 1);
+  tensor_product<R, false, NT>(res, LS, lgW, Pz, g.fPz, kx0, ky, Nhat, Hx, Py, Pz);
+  line_fft_from_smem<true, NT>(res, res == a ? b : a, dst, LS, nlines, fnl, g.plz, twz, 1);
+}
+
 template <typename RO>
 __global__ void k_cast(const double* __restrict__ a, RO* __restrict__ b, int64_t n) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -496,6 +570,10 @@ static void set_smem_attrs_nt() {
   cudaFuncSetAttribute(k_ypass<R, YM_TENSOR_Q, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_zpass<R, ZM_CONV, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_zpass<R, ZM_TENSOR_Q, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_FWD, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_INV, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_zconv<R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
 
 template <typename R>
@@ -538,7 +616,7 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
              nx, ny, nz, cap, cap, cap / 3);
     return -1;
   }
-  const int maxr = sizeof(R) == 4 ? 16 : 8;
+  const int maxr = sizeof(R) == 4 ? 32 : 8;
   if (!make_fft_plan(g.Lc > 0 ? g.Lc : 1, g.plx, maxr) || !make_fft_plan(g.Py, g.ply, maxr) ||
       !make_fft_plan(g.Pz, g.plz, maxr)) {
     snprintf(err, nerr, "demag: no radix plan");
@@ -553,7 +631,7 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
   g.frows = make_fastdiv(ny * nz);
   g.fpady = make_fastdiv(std::max(1, g.Py - ny));
   g.fpadz = make_fastdiv(std::max(1, g.Pz - nz));
-  fused2d = (g.Pz == 1) && (3 * g.Py <= hot_cap<R>());
+  fused2d = (g.Pz == 1) && (2 * 3 * (g.Py | 1) * sizeof(C) <= static_cast<size_t>(smem_budget_bytes()));
   set_smem_attrs<R>();
   set_smem_attrs<double>();
   const int64_t nX = 3LL * nz * ny * g.Hx;
@@ -616,6 +694,40 @@ static void launch_zpass(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, double
 }
 
 template <typename R>
+static int lines_tile(int Hx, int L, int lines_per_col, int nbuf) {
+  using C = cplx_t<R>;
+  int W = 128 / static_cast<int>(sizeof(C));
+  const size_t per = static_cast<size_t>(std::max(1, nbuf)) * lines_per_col * (L | 1) * sizeof(C);
+  while (W > 1 && W * per > static_cast<size_t>(smem_budget_bytes())) W /= 2;
+  while (W > 1 && W / 2 >= Hx) W /= 2;
+  return W;
+}
+
+template <typename R, int MODE>
+static void launch_ylines(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* out, const R* Nhat,
+                          const cplx_t<R>* twy, cudaStream_t st) {
+  using C = cplx_t<R>;
+  const int ncompc = MODE == YL_CONV2D ? 3 : 1;
+  const int nbuf = MODE == YL_CONV2D ? 2 : line_fft_buffers(g.ply);
+  const int W = lines_tile<R>(g.Hx, g.Py, ncompc, nbuf);
+  const int half = ncompc * W * (g.Py | 1);
+  dim3 grid((g.Hx + W - 1) / W, g.nz, 3 / ncompc);
+  const size_t sm = static_cast<size_t>(std::max(1, nbuf)) * sizeof(C) * half;
+  k_ylines<R, MODE, kHotNT><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc,
+                                                      make_fastdiv(ncompc * W), twy, half);
+}
+
+template <typename R>
+static void launch_zconv(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st) {
+  using C = cplx_t<R>;
+  const int W = lines_tile<R>(g.Hx, g.Pz, 3, 2);
+  const int half = 3 * W * (g.Pz | 1);
+  dim3 grid((g.Hx + W - 1) / W, g.Py, 1);
+  const size_t sm = 2 * sizeof(C) * half;
+  k_zconv<R, kHotNT><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz, half);
+}
+
+template <typename R>
 static bool run_pass(const DemagPlan<R>& p, DemagGeom g, int which, const R* m, const R* mu0Ms, R* Hd,
                      cudaStream_t st) {
   using C = cplx_t<R>;
@@ -626,15 +738,15 @@ static bool run_pass(const DemagPlan<R>& p, DemagGeom g, int which, const R* m, 
       return true;
     case 1:
       if (p.fused2d) return false;
-      launch_ypass<R, YM_FWD, NT>(g, p.X, p.Y, p.Nhat, nullptr, 1, 3, p.twy, 1, 0.0, st);
+      launch_ylines<R, YL_FWD>(g, p.X, p.Y, p.Nhat, p.twy, st);
       return true;
     case 2:
-      if (p.fused2d) launch_ypass<R, YM_CONV2D, NT>(g, p.X, p.X, p.Nhat, nullptr, 3, 3, p.twy, 1, 0.0, st);
-      else launch_zpass<R, ZM_CONV, NT>(g, p.Y, p.Nhat, nullptr, 3, g.Py / 2 + 1, p.twz, 1, 0.0, st);
+      if (p.fused2d) launch_ylines<R, YL_CONV2D>(g, p.X, p.X, p.Nhat, p.twy, st);
+      else launch_zconv<R>(g, p.Y, p.Nhat, p.twz, st);
       return true;
     case 3:
       if (p.fused2d) return false;
-      launch_ypass<R, YM_INV, NT>(g, p.Y, p.X, p.Nhat, nullptr, 1, 3, p.twy, 1, 0.0, st);
+      launch_ylines<R, YL_INV>(g, p.Y, p.X, p.Nhat, p.twy, st);
       return true;
     case 4: {
       const int lines = 3 * g.ny * g.nz;

@@ -101,6 +101,46 @@ template <bool INV, typename C> __device__ __forceinline__ void dft16(C* v) {
   }
 }
 
+// cos, sin of 2*pi*k/32, k = 0..15 (mathematical constants)
+__constant__ const double c_w32[16][2] = {
+    {1.00000000000000000000, 0.00000000000000000000},
+    {0.98078528040323043058, 0.19509032201612824808},
+    {0.92387953251128673848, 0.38268343236508978178},
+    {0.83146961230254523567, 0.55557023301960217765},
+    {0.70710678118654757274, 0.70710678118654746172},
+    {0.55557023301960228867, 0.83146961230254523567},
+    {0.38268343236508983729, 0.92387953251128673848},
+    {0.19509032201612833135, 0.98078528040323043058},
+    {0.00000000000000006123, 1.00000000000000000000},
+    {-0.19509032201612819257, 0.98078528040323043058},
+    {-0.38268343236508972627, 0.92387953251128673848},
+    {-0.55557023301960195560, 0.83146961230254545772},
+    {-0.70710678118654746172, 0.70710678118654757274},
+    {-0.83146961230254534669, 0.55557023301960217765},
+    {-0.92387953251128673848, 0.38268343236508989280},
+    {-0.98078528040323043058, 0.19509032201612860891},
+};
+
+// 32 = 2 x 16: DFT16 of the even and odd samples, twiddles w32^k
+template <bool INV, typename C> __device__ __forceinline__ void dft32(C* v) {
+  using R = decltype(C::x);
+  C e[16], o[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    e[i] = v[2 * i];
+    o[i] = v[2 * i + 1];
+  }
+  dft16<INV>(e);
+  dft16<INV>(o);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const R c = static_cast<R>(c_w32[k][0]), sn = static_cast<R>(c_w32[k][1]);
+    const C t = cmul(o[k], cmk<C>(c, INV ? sn : -sn));
+    v[k] = cadd(e[k], t);
+    v[k + 16] = csub(e[k], t);
+  }
+}
+
 template <bool INV, typename C> __device__ __forceinline__ void dft3(C* v) {
   using R = decltype(C::x);
   C t = cadd(v[1], v[2]);
@@ -157,7 +197,8 @@ template <int R, bool INV, typename C> __device__ __forceinline__ void dftR(C* v
   else if constexpr (R == 5) dft5<INV>(v);
   else if constexpr (R == 7) dft7<INV>(v);
   else if constexpr (R == 8) dft8<INV>(v);
-  else dft16<INV>(v);
+  else if constexpr (R == 16) dft16<INV>(v);
+  else dft32<INV>(v);
 }
 
 template <int R, bool INV, bool POW2, int NT, typename C>
@@ -206,6 +247,9 @@ __device__ __forceinline__ C* fft_lines_impl(C* a, C* b, int LS, int nlines, con
   for (int s = 0; s < pl.nst; ++s) {
     const int R = plan_radix(pl, s);
     switch (R) {
+      case 32:
+        if constexpr (sizeof(decltype(C::x)) == 4) fft_stage<32, INV, POW2, NT>(a, b, L, LS, nlines, p, tw, tw_mul);
+        break;
       case 16:
         if constexpr (sizeof(decltype(C::x)) == 4) fft_stage<16, INV, POW2, NT>(a, b, L, LS, nlines, p, tw, tw_mul);
         break;

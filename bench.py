@@ -237,6 +237,8 @@ def run_native(args):
     dt = w["dt"]
     forms = {"fp32": _lib.MM_FP32, "fp64": _lib.MM_FP64}
     results = {}
+    if args.integrator == "dopri":
+        return run_dopri(args, w, wname, n, forms, rank, ws, device, dist)
     for fname in ((args.only,) if args.only else ("fp32", "fp64")):
         h, m0 = setup_native(w, forms[fname], device)
         stream = torch.cuda.ExternalStream(h.stream(), device=device)
@@ -269,6 +271,7 @@ def run_native(args):
         if sampler:
             res["clocks"] = sampler.summary()
         if args.quick:
+            results[fname] = res
             h.close()
             del stream
             continue
@@ -353,6 +356,53 @@ def run_native(args):
         dist.destroy_process_group()
 
 
+def run_dopri(args, w, wname, n, forms, rank, ws, device, dist):
+    """Dormand-Prince (tol 1e-6) through mm_run_until: cell-steps/s over
+    accepted steps, the step control running on the device."""
+    import torch
+    from mmcuda import _lib
+
+    out = {}
+    for fname in ((args.only,) if args.only else ("fp32", "fp64")):
+        h, _ = setup_native(w, forms[fname], device)
+        h.call("mm_dopri_set_tol", 1e-6)
+        st = _lib.Stats()
+        L = _lib.load()
+        _lib.check(L.mm_run_until(h.h, 1e-15, ctypes.byref(st)))  # initial step + first attempts
+        for _ in range(args.warmup):
+            _lib.check(L.mm_advance_step(h.h, ctypes.byref(st)))
+        t0, n0, a0, r0 = st.t, st.nsteps, st.attempts, st.rejected
+        span = args.steps * st.step_next
+        stream = torch.cuda.ExternalStream(h.stream(), device=device)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(L.mm_run_until(h.h, t0 + span, ctypes.byref(st)))
+        e1.record(stream)
+        e1.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], device=f"cuda:{device}")
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        steps = st.nsteps - n0
+        out[fname] = {"value": ws * n * steps / (ms / 1e3), "ms_per_step": ms / max(1, steps), "accepted": steps,
+                      "attempts": st.attempts - a0, "rejected": st.rejected - r0, "t_span": span}
+        h.close()
+    if rank == 0:
+        r = out.get("fp32") or out.get("fp64")
+        line = {"metric": "LLG cell-steps/s (H_eff+demag+Dormand-Prince)", "value": r["value"], "unit": "cell-steps/s",
+                "n_gpus": ws, "steps": r["accepted"], "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if "fp32" in out else "f64", "data": "synthetic (seeded numpy PCG64)",
+                "config": {"workload": f"{wname}: {w['nx']}x{w['ny']}x{w['nz']} Dormand-Prince tol 1e-6"},
+                "forms": out}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -363,6 +413,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", choices=["fp32", "fp64"], help="time one form only (profiling runs)")
     ap.add_argument("--quick", action="store_true", help="timed steps only: no e2e, kernel timing or CPU leg")
+    ap.add_argument("--integrator", default="rk4", choices=["rk4", "dopri"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -66,7 +66,7 @@ template <typename R, int MODE, int NT>
 __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_fwd_x(
     const R* __restrict__ m, const R* __restrict__ Ms, const double* __restrict__ Tr, int tsign,
     cplx_t<R>* __restrict__ X, DemagGeom g, int lines_total, int nl, const cplx_t<R>* __restrict__ twx,
-    int half) {
+    int half, FastDiv fnl) {
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_fwd_x(
     buf[l * LS + t] = cmk<C>(v[0], v[1]);
   }
   __syncthreads();
-  buf = fft_lines<false, NT>(buf, buf2, LS, nlh, g.plx, twx, 2);
+  buf = line_fft_to_smem<false, NT>(SmemLines<C>{buf, LS}, buf2, buf, LS, nl, fnl, g.plx, twx, 2);
   const int Hx = g.Hx;
   const R one_half = R(0.5);
   for (int e = threadIdx.x; e < nlh * Hx; e += NT) {
@@ -134,7 +134,7 @@ __global__ void k_fwd_x1(const R* __restrict__ m, const R* __restrict__ Ms, cons
 template <typename R, int NT>
 __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_inv_x(
     const cplx_t<R>* __restrict__ X, R* __restrict__ H, DemagGeom g, int lines_total, int nl,
-    const cplx_t<R>* __restrict__ twx, int half) {
+    const cplx_t<R>* __restrict__ twx, int half, FastDiv fnl) {
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_inv_x(
     buf[l * LS + k] = cadd(cadd(a, b), crot<true>(cmul(csub(a, b), w)));
   }
   __syncthreads();
-  buf = fft_lines<true, NT>(buf, buf2, LS, nlh, g.plx, twx, 2);
+  buf = line_fft_to_smem<true, NT>(SmemLines<C>{buf, LS}, buf2, buf, LS, nl, fnl, g.plx, twx, 2);
   for (int e = threadIdx.x; e < nlh * Lc; e += NT) {
     const int l = fdiv(e, g.fLc), t = e - l * Lc;
     const int line = line0 + l;
@@ -667,7 +667,7 @@ static void launch_fwd_x(const DemagGeom& g, const R* m, const R* Ms, const doub
   const int blocks = (lines + nl - 1) / nl;
   const int half = nl * (g.Lc | 1);
   const size_t sm = 2 * sizeof(C) * half;
-  k_fwd_x<R, MODE, NT><<<blocks, NT, sm, st>>>(m, Ms, Tr, tsign, X, g, lines, nl, twx, half);
+  k_fwd_x<R, MODE, NT><<<blocks, NT, sm, st>>>(m, Ms, Tr, tsign, X, g, lines, nl, twx, half, make_fastdiv(nl));
 }
 
 template <typename R, int MODE, int NT>
@@ -756,7 +756,7 @@ static bool run_pass(const DemagPlan<R>& p, DemagGeom g, int which, const R* m, 
         const int nl = std::max(1, PassCfg<R, NT>::cap / g.Lc);
         const int half = nl * (g.Lc | 1);
         const size_t sm = 2 * sizeof(C) * half;
-        k_inv_x<R, NT><<<(lines + nl - 1) / nl, NT, sm, st>>>(p.X, Hd, g, lines, nl, p.twx, half);
+        k_inv_x<R, NT><<<(lines + nl - 1) / nl, NT, sm, st>>>(p.X, Hd, g, lines, nl, p.twx, half, make_fastdiv(nl));
       }
       return true;
     }

@@ -131,58 +131,80 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
   const int64_t N = a.N;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int nxy = nx * ny;
+  const unsigned mask = a.mask;
+  const bool local = (mask & (TB_EXCH | TB_DMI_BULK | TB_DMI_INTERFACIAL | TB_ANIS)) != 0;
+  // Every load is issued before any use: neighbour indices are clamped to the
+  // cell itself where a neighbour does not exist (the mask bit then drops the
+  // term), so no load waits on another.
+  const bool px = a.pbc & 1, py = a.pbc & 2, pz = a.pbc & 4;
+  int nb[6];
+  nb[0] = i > 0 ? I - 1 : (px ? I + nx - 1 : I);
+  nb[1] = i < nx - 1 ? I + 1 : (px ? I - (nx - 1) : I);
+  nb[2] = j > 0 ? I - nx : (py ? I + (ny - 1) * nx : I);
+  nb[3] = j < ny - 1 ? I + nx : (py ? I - (ny - 1) * nx : I);
+  nb[4] = k > 0 ? I - nxy : (pz ? I + (nz - 1) * nxy : I);
+  nb[5] = k < nz - 1 ? I + nxy : (pz ? I - (nz - 1) * nxy : I);
   m[0] = y[I];
   m[1] = y[N + I];
   m[2] = y[2 * N + I];
-  h[0] = h[1] = h[2] = R(0);
   const R Ms = a.Ms[I];
-  const unsigned mask = a.mask;
+  unsigned nbm = 0;
+  R mn[6][3];
+  if (local) {
+    nbm = a.nbm[I];
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+      mn[d][0] = __ldg(y + nb[d]);
+      mn[d][1] = __ldg(y + N + nb[d]);
+      mn[d][2] = __ldg(y + 2 * N + nb[d]);
+    }
+  }
+  R An[6] = {R(0), R(0), R(0), R(0), R(0), R(0)}, AI = R(0);
+  if ((mask & TB_EXCH) && a.A) {
+    AI = a.A[I];
+#pragma unroll
+    for (int d = 0; d < 6; ++d) An[d] = __ldg(a.A + nb[d]);
+  }
+  R Dn[4] = {R(0), R(0), R(0), R(0)}, DI = a.D_uni;
+  if ((mask & TB_DMI_INTERFACIAL) && a.D) {
+    DI = a.D[I];
+#pragma unroll
+    for (int d = 0; d < 4; ++d) Dn[d] = __ldg(a.D + nb[d]);
+  }
+  const R Ku = ((mask & TB_ANIS) && a.Ku) ? a.Ku[I] : a.Ku_uni;
+  R hd[3] = {R(0), R(0), R(0)};
+  if (mask & TB_DEMAG) {
+    hd[0] = a.Hd[I];
+    hd[1] = a.Hd[N + I];
+    hd[2] = a.Hd[2 * N + I];
+  }
+  R zx = a.hz_x, zy = a.hz_y, zz = a.hz_z;  // uniform part plus the per-cell part
+  if ((mask & TB_ZEEMAN) && a.Hz) {
+    zx += a.Hz[I];
+    zy += a.Hz[N + I];
+    zz += a.Hz[2 * N + I];
+  }
+
+  h[0] = h[1] = h[2] = R(0);
   if (ENERGY) {
 #pragma unroll
     for (int t = 0; t < kNTerms; ++t) e[t] = 0.0;
   }
-  if (Ms != R(0) && (mask & (TB_EXCH | TB_DMI_BULK | TB_DMI_INTERFACIAL | TB_ANIS))) {
-    const bool px = a.pbc & 1, py = a.pbc & 2, pz = a.pbc & 4;
-    const unsigned nbm = a.nbm[I];
-    int nb[6];
-    nb[0] = i > 0 ? I - 1 : (px ? I + nx - 1 : -1);
-    nb[1] = i < nx - 1 ? I + 1 : (px ? I - (nx - 1) : -1);
-    nb[2] = j > 0 ? I - nx : (py ? I + (ny - 1) * nx : -1);
-    nb[3] = j < ny - 1 ? I + nx : (py ? I - (ny - 1) * nx : -1);
-    nb[4] = k > 0 ? I - nxy : (pz ? I + (nz - 1) * nxy : -1);
-    nb[5] = k < nz - 1 ? I + nxy : (pz ? I - (nz - 1) * nxy : -1);
+  if (Ms != R(0) && local) {
     const R Ms_inv = R(1) / Ms;
-    R mn[6][3];
-#pragma unroll
-    for (int d = 0; d < 6; ++d) {
-      if ((nbm >> d) & 1u) {
-        const int q = nb[d];
-        mn[d][0] = __ldg(y + q);
-        mn[d][1] = __ldg(y + N + q);
-        mn[d][2] = __ldg(y + 2 * N + q);
-      } else {
-        mn[d][0] = mn[d][1] = mn[d][2] = R(0);
-      }
-    }
     // exchange
     if (mask & TB_EXCH) {
       R fx = 0, fy = 0, fz = 0;
       const R coef[6] = {a.ex_x, a.ex_x, a.ex_y, a.ex_y, a.ex_z, a.ex_z};
-      bool on = true;
-      R AI = R(0);
-      if (a.A) {
-        AI = a.A[I];
-        on = AI != R(0);
-      }
+      const bool on = a.A ? (AI != R(0)) : true;
       if (on) {
 #pragma unroll
         for (int d = 0; d < 6; ++d) {
           if ((nbm >> d) & 1u) {
             R c = coef[d];
             if (a.A) {
-              const R An = __ldg(a.A + nb[d]);
-              if (An == R(0)) continue;
-              const R Aeff = 2 * AI * An / (AI + An);
+              if (An[d] == R(0)) continue;
+              const R Aeff = 2 * AI * An[d] / (AI + An[d]);
               c = Aeff * coef[d];
             }
             fx += c * (mn[d][0] - m[0]);
@@ -211,37 +233,32 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
       h[2] += fz * Ms_inv;
     }
     // interfacial DMI: r = +y,-y,-x,+x for d = -x,+x,-y,+y; harmonic mean of D
-    if (mask & TB_DMI_INTERFACIAL) {
-      const R DI = a.D ? a.D[I] : a.D_uni;
-      if (DI != R(0)) {
-        R fx = 0, fy = 0, fz = 0;
-        const R dd[4] = {a.id_x, a.id_x, a.id_y, a.id_y};
+    if ((mask & TB_DMI_INTERFACIAL) && DI != R(0)) {
+      R fx = 0, fy = 0, fz = 0;
+      const R dd[4] = {a.id_x, a.id_x, a.id_y, a.id_y};
 #pragma unroll
-        for (int d = 0; d < 4; ++d) {
-          if (!((nbm >> d) & 1u)) continue;
-          R c;
-          if (a.D) {
-            const R Dn = __ldg(a.D + nb[d]);
-            if (Dn == R(0)) continue;
-            c = (2 * DI * Dn / (DI + Dn)) * dd[d];
-          } else {
-            c = DI * dd[d];
-          }
-          // r x m_nb
-          if (d == 0) { fx += c * mn[0][2]; fz += c * (-mn[0][0]); }
-          else if (d == 1) { fx += c * (-mn[1][2]); fz += c * mn[1][0]; }
-          else if (d == 2) { fy += c * mn[2][2]; fz += c * (-mn[2][1]); }
-          else { fy += c * (-mn[3][2]); fz += c * mn[3][1]; }
+      for (int d = 0; d < 4; ++d) {
+        if (!((nbm >> d) & 1u)) continue;
+        R c;
+        if (a.D) {
+          if (Dn[d] == R(0)) continue;
+          c = (2 * DI * Dn[d] / (DI + Dn[d])) * dd[d];
+        } else {
+          c = DI * dd[d];
         }
-        if (ENERGY) e[3] = -0.5 * (double(fx) * m[0] + double(fy) * m[1] + double(fz) * m[2]) * double(a.V);
-        h[0] += fx * Ms_inv;
-        h[1] += fy * Ms_inv;
-        h[2] += fz * Ms_inv;
+        // r x m_nb
+        if (d == 0) { fx += c * mn[0][2]; fz += c * (-mn[0][0]); }
+        else if (d == 1) { fx += c * (-mn[1][2]); fz += c * mn[1][0]; }
+        else if (d == 2) { fy += c * mn[2][2]; fz += c * (-mn[2][1]); }
+        else { fy += c * (-mn[3][2]); fz += c * mn[3][1]; }
       }
+      if (ENERGY) e[3] = -0.5 * (double(fx) * m[0] + double(fy) * m[1] + double(fz) * m[2]) * double(a.V);
+      h[0] += fx * Ms_inv;
+      h[1] += fy * Ms_inv;
+      h[2] += fz * Ms_inv;
     }
     // uniaxial anisotropy
     if (mask & TB_ANIS) {
-      const R Ku = a.Ku ? a.Ku[I] : a.Ku_uni;
       const R inv2 = R(2) / Ms;
       const R sa = m[0] * a.ux + m[1] * a.uy + m[2] * a.uz;
       h[0] += Ku * sa * a.ux * inv2;
@@ -251,20 +268,13 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
     }
   }
   if (mask & TB_DEMAG) {
-    const R dx = a.Hd[I], dy = a.Hd[N + I], dz = a.Hd[2 * N + I];
-    h[0] += dx;
-    h[1] += dy;
-    h[2] += dz;
-    if (ENERGY) e[5] = -0.5 * double(Ms) * double(a.V) * (double(m[0]) * dx + double(m[1]) * dy + double(m[2]) * dz);
+    h[0] += hd[0];
+    h[1] += hd[1];
+    h[2] += hd[2];
+    if (ENERGY)
+      e[5] = -0.5 * double(Ms) * double(a.V) * (double(m[0]) * hd[0] + double(m[1]) * hd[1] + double(m[2]) * hd[2]);
   }
   if (mask & TB_ZEEMAN) {
-    // uniform part plus the per-cell part (accumulated add_zeeman fields)
-    R zx = a.hz_x, zy = a.hz_y, zz = a.hz_z;
-    if (a.Hz) {
-      zx += a.Hz[I];
-      zy += a.Hz[N + I];
-      zz += a.Hz[2 * N + I];
-    }
     h[0] += zx;
     h[1] += zy;
     h[2] += zz;
@@ -309,7 +319,7 @@ __constant__ double c_dp_a[6][6] = {
 __constant__ double c_dp_w[7] = {71.0 / 57600, 0, -71.0 / 16695, 71.0 / 1920, -17253.0 / 339200, 22.0 / 525, -1.0 / 40};
 
 template <typename R, int MODE>
-__global__ void __launch_bounds__(kStageThreads, 3) k_stage(FieldArgs<R> a, const R* __restrict__ y, StageArgs<R> s) {
+__global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage(FieldArgs<R> a, const R* __restrict__ y, StageArgs<R> s) {
   constexpr bool kF32 = sizeof(R) == 4;
   if (MODE == SM_DOPRI && !s.ctrl->active) return;
   const int64_t N = a.N;
@@ -323,6 +333,16 @@ __global__ void __launch_bounds__(kStageThreads, 3) k_stage(FieldArgs<R> a, cons
   double e[kNTerms];
   R m[3], h[3];
   double red = 0.0;  // SM_DOPRI stage 7: error max
+  // RK4 operands of this cell, loaded together with the field inputs
+  R mN[3], mL[3], av[3];
+  if (MODE == SM_RK4 && live) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      mN[c] = s.m[c * N + I];
+      mL[c] = kF32 ? s.m_lo[c * N + I] : R(0);
+      av[c] = s.stage > 1 ? s.acc[c * N + I] : R(0);
+    }
+  }
   if (live) {
     cell_heff<R, MODE == SM_ENERGY || MODE == SM_FIELD>(a, y, I, i, j, k, m, h, e);
     if (MODE == SM_FIELD) {
@@ -347,20 +367,17 @@ __global__ void __launch_bounds__(kStageThreads, 3) k_stage(FieldArgs<R> a, cons
       llg_rhs(a, I, m, h, f);
       const int st = s.stage;
       if (st < 4) {
-        R acc[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const R kc = f[c];
-          acc[c] = st == 1 ? kc : s.acc[c * N + I] + 2 * kc;
-          s.acc[c * N + I] = acc[c];
+          s.acc[c * N + I] = st == 1 ? kc : av[c] + 2 * kc;
         }
         const R cf = static_cast<R>(st == 3 ? s.h : 0.5 * s.h);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const R m0 = s.m[c * N + I];
           R v;
-          if (kF32) v = m0 + (s.m_lo[c * N + I] + cf * f[c]);
-          else v = m0 + cf * f[c];
+          if (kF32) v = mN[c] + (mL[c] + cf * f[c]);
+          else v = mN[c] + cf * f[c];
           s.ynext[c * N + I] = v;
         }
       } else {
@@ -370,16 +387,16 @@ __global__ void __launch_bounds__(kStageThreads, 3) k_stage(FieldArgs<R> a, cons
           float lo[3];
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
-            mv[c] = s.m[c * N + I];
-            lo[c] = s.m_lo[c * N + I];
-            df_add(mv[c], lo[c], c6 * (s.acc[c * N + I] + f[c]));
+            mv[c] = mN[c];
+            lo[c] = mL[c];
+            df_add(mv[c], lo[c], c6 * (av[c] + f[c]));
           }
           df_normalise(mv, lo);
 #pragma unroll
           for (int c = 0; c < 3; ++c) s.m_lo[c * N + I] = lo[c];
         } else {
 #pragma unroll
-          for (int c = 0; c < 3; ++c) mv[c] = s.m[c * N + I] + c6 * (s.acc[c * N + I] + f[c]);
+          for (int c = 0; c < 3; ++c) mv[c] = mN[c] + c6 * (av[c] + f[c]);
           plain_normalise(mv);
         }
 #pragma unroll

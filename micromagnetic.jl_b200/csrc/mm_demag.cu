@@ -439,6 +439,86 @@ __global__ void __launch_bounds__(NT, 2) k_zconv(cplx_t<R>* Y, const R* __restri
   line_fft_from_smem<true, NT>(res, res == a ? b : a, dst, LS, nlines, fnl, g.plz, twz, 1);
 }
 
+// z convolution for Pz = RA * RB (powers of two): forward radix-RA stage from
+// the Y rows into shared memory; then, per butterfly i < RA and in registers,
+// the forward radix-RB stage (outputs kz = i + r*RA), the tensor product at
+// those kz for the three components, and the inverse radix-RB stage (its
+// inputs are the same positions), written back in place after a barrier;
+// finally the inverse radix-RA stage straight to the Y rows kz < nz.
+// One shared buffer; requires W * RA <= NT (one middle task per thread).
+template <typename R, int RA, int RB, int NT>
+__global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_zconv2(cplx_t<R>* Y, const R* __restrict__ Nhat, DemagGeom g, int lgW,
+                                                  FastDiv fnl, const cplx_t<R>* __restrict__ twz) {
+  using C = cplx_t<R>;
+  constexpr int L = RA * RB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* a = reinterpret_cast<C*>(smem_raw);
+  if (g.gate && !*g.gate) return;
+  const int LS = L | 1, Hx = g.Hx, Py = g.Py, nz = g.nz;
+  const int W = 1 << lgW;
+  const int kx0 = blockIdx.x * W;
+  const int bq = blockIdx.y;
+  const int q = (bq + 1) >> 1;
+  const int ky = bq == 0 ? 0 : ((bq & 1) ? q : Py - q);
+  const int nlines = 3 * W;
+  const int64_t cs = static_cast<int64_t>(nz) * Py * Hx, rs = static_cast<int64_t>(Py) * Hx;
+  RowsIn<C> src{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
+  RowsOut<C> dst{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
+  SmemLines<C> A{a, LS};
+  lstage<RA, false, true, NT>(src, A, L, nlines, fnl, 1, twz, 1);
+  // fused middle: thread -> (w, i), w fastest
+  const int task = threadIdx.x;
+  const bool act = task < W * RA;
+  const int w = task & (W - 1), i = task >> lgW;
+  const int kx = kx0 + w;
+  C v[3][RB];
+  if (act) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int r = 0; r < RB; ++r) v[c][r] = A.load(c * W + w, i + r * RA);
+      // forward radix-RB stage, span p = RA, k = i: twiddles w_L^(r*i)
+#pragma unroll
+      for (int r = 1; r < RB; ++r) v[c][r] = cmul(v[c][r], __ldg(twz + r * i));
+      dftR<RB, false>(v[c]);
+    }
+    if (kx < Hx) {
+      const int Tyq = Py / 2 + 1, Tzq = L / 2 + 1;
+      const int64_t Ts = static_cast<int64_t>(Tzq) * Tyq * Hx;
+      const bool fy = ky > Py / 2;
+      const int kyq = fy ? Py - ky : ky;
+      const R sy = fy ? R(-1) : R(1);
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const int kz = i + r * RA;
+        const bool fz = kz > L / 2;
+        const int kzq = fz ? L - kz : kz;
+        const R sz = fz ? R(-1) : R(1);
+        const int64_t b = (static_cast<int64_t>(kzq) * Tyq + kyq) * Hx + kx;
+        const R xx = __ldg(Nhat + b), yy = __ldg(Nhat + Ts + b), zz = __ldg(Nhat + 2 * Ts + b);
+        const R xy = sy * __ldg(Nhat + 3 * Ts + b), xz = sz * __ldg(Nhat + 4 * Ts + b),
+                yz = sy * sz * __ldg(Nhat + 5 * Ts + b);
+        const C p0 = v[0][r], p1 = v[1][r], p2 = v[2][r];
+        v[0][r] = cmk<C>(xx * p0.x + xy * p1.x + xz * p2.x, xx * p0.y + xy * p1.y + xz * p2.y);
+        v[1][r] = cmk<C>(xy * p0.x + yy * p1.x + yz * p2.x, xy * p0.y + yy * p1.y + yz * p2.y);
+        v[2][r] = cmk<C>(xz * p0.x + yz * p1.x + zz * p2.x, xz * p0.y + yz * p1.y + zz * p2.y);
+      }
+    }
+    // inverse radix-RB stage, span 1: outputs at i*RB + r
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dftR<RB, true>(v[c]);
+  }
+  __syncthreads();
+  if (act) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < RB; ++r) A.store(c * W + w, i * RB + r, v[c][r]);
+  }
+  __syncthreads();
+  lstage<RA, true, true, NT>(A, dst, L, nlines, fnl, RB, twz, 1);
+}
+
 template <typename RO>
 __global__ void k_cast(const double* __restrict__ a, RO* __restrict__ b, int64_t n) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -717,9 +797,48 @@ static void launch_ylines(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* ou
                                                       make_fastdiv(ncompc * W), twy, half);
 }
 
+template <typename R, int RA, int RB>
+static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st) {
+  using C = cplx_t<R>;
+  constexpr int L = RA * RB;
+  int W = lines_tile<R>(g.Hx, L, 3, 1);
+  while (W * RA > kHotNT) W /= 2;
+  const size_t sm = sizeof(C) * 3 * W * (L | 1);
+  static uint64_t done = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!((done >> dev) & 1ull)) {
+    cudaFuncSetAttribute(k_zconv2<R, RA, RB, kHotNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    done |= 1ull << dev;
+  }
+  dim3 grid((g.Hx + W - 1) / W, g.Py, 1);
+  k_zconv2<R, RA, RB, kHotNT><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz);
+}
+
+// Power-of-two z lengths with a fused-middle kernel: L = RA * RB
+template <typename R>
+static bool try_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st) {
+  switch (g.Pz) {
+    case 4: launch_zconv2<R, 2, 2>(g, Y, Nhat, twz, st); return true;
+    case 8: launch_zconv2<R, 4, 2>(g, Y, Nhat, twz, st); return true;
+    case 16: launch_zconv2<R, 4, 4>(g, Y, Nhat, twz, st); return true;
+    case 32: launch_zconv2<R, 8, 4>(g, Y, Nhat, twz, st); return true;
+    case 64: launch_zconv2<R, 8, 8>(g, Y, Nhat, twz, st); return true;
+    case 128: launch_zconv2<R, 16, 8>(g, Y, Nhat, twz, st); return true;
+    case 256:
+      if constexpr (sizeof(R) == 4) {
+        launch_zconv2<R, 32, 8>(g, Y, Nhat, twz, st);
+        return true;
+      }
+      return false;
+    default: return false;
+  }
+}
+
 template <typename R>
 static void launch_zconv(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st) {
   using C = cplx_t<R>;
+  if (try_zconv2<R>(g, Y, Nhat, twz, st)) return;
   const int W = lines_tile<R>(g.Hx, g.Pz, 3, 2);
   const int half = 3 * W * (g.Pz | 1);
   dim3 grid((g.Hx + W - 1) / W, g.Py, 1);

@@ -174,6 +174,25 @@ int mm_kernel_time(mm_handle* h, int kernel, int reps, double* ms_per_launch, do
 /* Number of kernel launches in one RK4 step. */
 int mm_rk4_launches_per_step(mm_handle* h, int* launches);
 
+/* ---- energies without device allocation ----------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (a host whose pool allocator must own all device memory, a latency-critical
+ * path where cudaMalloc's implicit synchronisation is not acceptable, code
+ * with no handle): total energies (J, FP64, indexed by mm_term; demag and
+ * interfacial DMI entries are 0) of uniform exchange A, bulk DMI D (all
+ * axes), uniaxial anisotropy Ku along (ax, ay, az) and a uniform Zeeman field
+ * (Hx, Hy, Hz) for m_soa_dev (device, SoA [mx..., my..., mz...], float64) and
+ * Ms_dev (device, A/m, float64), written to energies_dev (device, 6 doubles),
+ * enqueued on `stream` (cudaStream_t, 0 = legacy default stream).
+ * Allocates nothing: the per-block partial sums live in a static device array
+ * of the library (3 MiB on every GPU that loads it), so meshes are limited to
+ * 2^24 cells (MM_ERR_ARG beyond).  The first call on a device looks the
+ * array's device address up (cudaGetSymbolAddress) and should come before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU race. */
+int mm_energy_noalloc(const mm_mesh_desc* mesh, const double* m_soa_dev, const double* Ms_dev, double A, double D,
+                      double Ku, double ax, double ay, double az, double Hx, double Hy, double Hz,
+                      double* energies_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

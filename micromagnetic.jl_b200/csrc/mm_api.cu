@@ -33,6 +33,13 @@ static int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+// Sets the calling thread's last error message (used by translation units
+// outside this file) and returns code.
+int set_last_error(int code, const char* msg) {
+  g_err = msg;
+  return code;
+}
+
 #define MM_CUDA(call)                                                                          \
   do {                                                                                         \
     cudaError_t e_ = (call);                                                                   \

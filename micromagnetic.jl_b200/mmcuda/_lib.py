@@ -36,6 +36,7 @@ EXPORTS = (
     "mm_add_demag", "mm_add_demag_tensor", "mm_effective_field", "mm_term_field", "mm_energy",
     "mm_llg_rhs", "mm_average_m", "mm_rk4_run", "mm_rk4_state", "mm_dopri_set_tol", "mm_run_until",
     "mm_advance_step", "mm_dopri_reset", "mm_relax", "mm_kernel_time", "mm_rk4_launches_per_step",
+    "mm_energy_noalloc",
 )
 KERNELS = ("demag_fwd_x", "demag_fwd_y", "demag_conv", "demag_inv_y", "demag_inv_x", "rk4_stage", "rk4_step")
 
@@ -110,6 +111,7 @@ def load():
         "mm_relax": ([_vp, i, i64, d, ctypes.POINTER(i64), _dp], i),
         "mm_kernel_time": ([_vp, i, i, _dp, _dp], i),
         "mm_rk4_launches_per_step": ([_vp, ctypes.POINTER(i)], i),
+        "mm_energy_noalloc": ([ctypes.POINTER(MeshDesc), _vp, _vp] + [d] * 9 + [_vp, _vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

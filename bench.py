@@ -45,6 +45,14 @@ WORKLOADS = {
     "c1": dict(nx=200, ny=50, nz=1, dx=2.5e-9, dy=2.5e-9, dz=3e-9, Ms=8e5, A=1.3e-11, Dbulk=None, Ku=None,
                axis=(0, 0, 1), demag=True, alpha=0.02, gamma=2.211e5, dt=1e-13, seed=101, zeeman="inplane30mT"),
 }
+# batched workloads: many meshes advanced by one graph launch per RK4 step
+BATCHES = {
+    # 48 films, nx, ny ~ U{32..256}, nz ~ U{1..4}, 2 nm cells, interfacial DMI
+    # D ~ U[1,4]e-3, Ms ~ U[4,9]e5, A ~ U[0.8,1.5]e-11, demag, random m (seed 103)
+    "c3": dict(kind="films", count=48, seed=103),
+    # 32 NEB images of one 128x128x1 film, m interpolated between two random states
+    "c3neb": dict(kind="neb", count=32, seed=103, nx=128, ny=128),
+}
 # the CPU baseline times a bounded block of the same physics
 CPU_SAMPLE = {"c2": (128, 128, 32), "c5": (256, 256, 16), "c1": (200, 50, 1)}
 
@@ -127,6 +135,94 @@ class ClockSampler:
                           and "Not" not in s[5 + i]})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
+
+
+def setup_batch(wname, form, device):
+    """Handles of a batched workload (all on one device) and their total cells."""
+    from mmcuda import _lib
+
+    spec = BATCHES[wname]
+    rng = np.random.default_rng(spec["seed"])
+    handles, cells = [], 0
+    if spec["kind"] == "films":
+        for _ in range(spec["count"]):
+            nx, ny, nz = int(rng.integers(32, 257)), int(rng.integers(32, 257)), int(rng.integers(1, 5))
+            D, Ms, A = rng.uniform(1e-3, 4e-3), rng.uniform(4e5, 9e5), rng.uniform(0.8e-11, 1.5e-11)
+            n = nx * ny * nz
+            m = rng.standard_normal((n, 3))
+            m /= np.linalg.norm(m, axis=1, keepdims=True)
+            h = _lib.Handle(nx, ny, nz, 2e-9, 2e-9, 2e-9, 0, form, device)
+            h.call("mm_set_Ms", None, Ms)
+            h.set_m(m.reshape(-1))
+            h.call("mm_set_llg", 0.1, 2.211e5, 1)
+            h.call("mm_add_exch", None, A, A, A)
+            h.call("mm_add_dmi_interfacial", None, D)
+            h.call("mm_add_demag", 0, 0, 0)
+            handles.append(h)
+            cells += n
+    else:
+        nx, ny = spec["nx"], spec["ny"]
+        n = nx * ny
+        m1 = rng.standard_normal((n, 3))
+        m2 = rng.standard_normal((n, 3))
+        for k in range(spec["count"]):
+            s = k / (spec["count"] - 1)
+            m = (1 - s) * m1 / np.linalg.norm(m1, axis=1, keepdims=True) + s * m2 / np.linalg.norm(m2, axis=1, keepdims=True)
+            m /= np.linalg.norm(m, axis=1, keepdims=True)
+            h = _lib.Handle(nx, ny, 1, 2e-9, 2e-9, 2e-9, 0, form, device)
+            h.call("mm_set_Ms", None, 8e5)
+            h.set_m(m.reshape(-1))
+            h.call("mm_set_llg", 0.1, 2.211e5, 1)
+            h.call("mm_add_exch", None, 1.3e-11, 1.3e-11, 1.3e-11)
+            h.call("mm_add_dmi_interfacial", None, 2e-3)
+            h.call("mm_add_demag", 0, 0, 0)
+            handles.append(h)
+            cells += n
+    return handles, cells
+
+
+def run_batch(args, rank, ws, device, dist):
+    import torch
+    from mmcuda import _lib
+
+    wname = args.workload
+    out = {}
+    for fname, form in (("fp32", _lib.MM_FP32), ("fp64", _lib.MM_FP64)):
+        if args.only and fname != args.only:
+            continue
+        handles, cells = setup_batch(wname, form, device)
+        b = _lib.Batch(handles)
+        b.rk4_run(5e-14, args.warmup)
+        stream = torch.cuda.ExternalStream(b.stream(), device=device)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.rk4_run(5e-14, args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], device=f"cuda:{device}")
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        out[fname] = {"value": ws * cells * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                      "instances": len(handles), "cells": cells,
+                      "launches_per_step": sum(h.rk4_launches() for h in handles)}
+        b.close()
+        for h in handles:
+            h.close()
+    if rank == 0:
+        r = out.get("fp32") or out.get("fp64")
+        line = {"metric": "LLG cell-steps/s (H_eff+demag+RK4), batched", "value": r["value"], "unit": "cell-steps/s",
+                "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if "fp32" in out else "f64", "data": "synthetic (seeded numpy PCG64)",
+                "config": {"workload": f"{wname}: {r['instances']} meshes, {r['cells']} cells, one graph per step"},
+                "forms": out}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def cpu_baseline(wname, steps=1):
@@ -232,6 +328,8 @@ def run_native(args):
     from mmcuda import _lib
 
     wname = args.workload
+    if wname in BATCHES:
+        return run_batch(args, rank, ws, device, dist)
     w = WORKLOADS[wname]
     n = w["nx"] * w["ny"] * w["nz"]
     dt = w["dt"]
@@ -408,7 +506,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + sorted(BATCHES))
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", choices=["fp32", "fp64"], help="time one form only (profiling runs)")

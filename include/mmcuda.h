@@ -174,6 +174,19 @@ int mm_kernel_time(mm_handle* h, int kernel, int reps, double* ms_per_launch, do
 /* Number of kernel launches in one RK4 step. */
 int mm_rk4_launches_per_step(mm_handle* h, int* launches);
 
+/* ---- batches: several meshes (ensembles, NEB images) stepped together ----
+ * The reference evaluates NEB images one after another (src/neb/neb.jl:220-232).
+ * A batch captures one RK4 step of every handle (same device, same dt) as
+ * parallel branches of one CUDA graph and replays it once per step; work
+ * queued on the handles before mm_batch_rk4_run precedes the batch and work
+ * queued after it follows.  The handles stay owned by the caller and must
+ * outlive the batch. */
+typedef struct mm_batch mm_batch;
+int mm_batch_create(mm_handle* const* handles, int n, mm_batch** out);
+int mm_batch_rk4_run(mm_batch* b, double dt, int64_t nsteps);
+int mm_batch_get_stream(mm_batch* b, void** stream);
+int mm_batch_destroy(mm_batch* b);
+
 /* ---- energies without device allocation ----------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (a host whose pool allocator must own all device memory, a latency-critical

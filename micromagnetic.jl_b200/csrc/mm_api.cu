@@ -91,6 +91,12 @@ class EngineBase {
   virtual int relax(int driver, int64_t max_steps, double stop, int64_t* steps, double* max_dmdt) = 0;
   virtual int kernel_time(int kernel, int reps, double* ms, double* bytes) = 0;
   virtual int rk4_launches() const = 0;
+  // batch support: buffers ready, one RK4 step enqueued on the handle's stream,
+  // step counters advanced after a batch ran n steps
+  virtual int rk4_prepare() = 0;
+  virtual void rk4_enqueue(double dt) = 0;
+  virtual void rk4_count(int64_t n, double dt) = 0;
+  virtual uint64_t params_version() const = 0;
   virtual cudaStream_t stream() const = 0;
   virtual size_t device_bytes() const = 0;
   int device = 0;
@@ -490,6 +496,20 @@ class Engine : public EngineBase {
     return MM_OK;
   }
 
+  int rk4_prepare() override {
+    if (int rc = need_ms()) return rc;
+    int rc;
+    if (!acc && (rc = alloc(acc, 3 * N))) return rc;
+    if (!yB && (rc = alloc(yB, 3 * N))) return rc;
+    return MM_OK;
+  }
+  void rk4_enqueue(double dt) override { enqueue_rk4_step(dt); }
+  void rk4_count(int64_t n, double dt) override {
+    rk_n += n;
+    rk_t = static_cast<double>(rk_n) * dt;
+  }
+  uint64_t params_version() const override { return version; }
+
   int rk4_launches() const override {
     const int passes = ((mask & TB_DEMAG) && demag) ? demag->launches_per_apply() : 0;
     return 4 * (passes + 1);
@@ -866,6 +886,28 @@ struct mm_handle {
   std::unique_ptr<mm::EngineBase> eng;
 };
 
+// A set of handles on one device stepped together: one RK4 step of every
+// instance is captured as parallel branches (fork/join over the handles' own
+// streams) of a single CUDA graph, launched once per step on the batch stream.
+struct mm_batch {
+  std::vector<mm_handle*> hs;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t fork = nullptr, done = nullptr;
+  std::vector<cudaEvent_t> joins;
+  cudaGraphExec_t graph = nullptr;
+  double dt = 0.0;
+  std::vector<uint64_t> versions;
+  ~mm_batch() {
+    cudaSetDevice(device);
+    if (graph) cudaGraphExecDestroy(graph);
+    for (cudaEvent_t e : joins) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (done) cudaEventDestroy(done);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
 using mm::fail;
 
 #define MM_HANDLE(h)                                                          \
@@ -1027,6 +1069,92 @@ int mm_rk4_launches_per_step(mm_handle* h, int* n) {
   if (!n) return fail(MM_ERR_ARG, "null output");
   *n = h->eng->rk4_launches();
   return MM_OK;
+}
+
+int mm_batch_create(mm_handle* const* handles, int n, mm_batch** out) {
+  if (!handles || !out || n < 1) return fail(MM_ERR_ARG, "mm_batch_create: need n >= 1 handles");
+  *out = nullptr;
+  const int dev = handles[0] && handles[0]->eng ? handles[0]->eng->device : -1;
+  for (int i = 0; i < n; ++i) {
+    if (!handles[i] || !handles[i]->eng) return fail(MM_ERR_ARG, "mm_batch_create: null handle %d", i);
+    if (handles[i]->eng->device != dev) return fail(MM_ERR_ARG, "mm_batch_create: handles on different devices");
+    for (int j = 0; j < i; ++j)
+      if (handles[j] == handles[i]) return fail(MM_ERR_ARG, "mm_batch_create: handle %d repeated", i);
+  }
+  if (cudaSetDevice(dev) != cudaSuccess) return fail(MM_ERR_CUDA, "cudaSetDevice failed");
+  auto b = std::make_unique<mm_batch>();
+  b->device = dev;
+  b->hs.assign(handles, handles + n);
+  if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess)
+    return fail(MM_ERR_CUDA, "mm_batch_create: stream/event creation failed");
+  b->joins.resize(n);
+  for (int i = 0; i < n; ++i)
+    if (cudaEventCreateWithFlags(&b->joins[i], cudaEventDisableTiming) != cudaSuccess)
+      return fail(MM_ERR_CUDA, "mm_batch_create: event creation failed");
+  *out = b.release();
+  return MM_OK;
+}
+
+int mm_batch_destroy(mm_batch* b) {
+  delete b;
+  return MM_OK;
+}
+
+int mm_batch_get_stream(mm_batch* b, void** s) {
+  if (!b || !s) return fail(MM_ERR_ARG, "null argument");
+  *s = static_cast<void*>(b->st);
+  return MM_OK;
+}
+
+int mm_batch_rk4_run(mm_batch* b, double dt, int64_t nsteps) {
+  if (!b) return fail(MM_ERR_ARG, "null batch");
+  if (nsteps < 0 || !(dt > 0)) return fail(MM_ERR_ARG, "rk4: need dt > 0 and nsteps >= 0");
+  if (cudaSetDevice(b->device) != cudaSuccess) return fail(MM_ERR_CUDA, "cudaSetDevice failed");
+  try {
+    const int n = static_cast<int>(b->hs.size());
+    bool stale = !b->graph || b->dt != dt || static_cast<int>(b->versions.size()) != n;
+    for (int i = 0; i < n && !stale; ++i) stale = b->versions[i] != b->hs[i]->eng->params_version();
+    for (int i = 0; i < n; ++i)
+      if (int rc = b->hs[i]->eng->rk4_prepare()) return rc;
+    // earlier work of every handle precedes the batch
+    for (int i = 0; i < n; ++i) {
+      MM_CUDA(cudaEventRecord(b->joins[i], b->hs[i]->eng->stream()));
+      MM_CUDA(cudaStreamWaitEvent(b->st, b->joins[i], 0));
+    }
+    if (stale) {
+      if (b->graph) cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+      cudaGraph_t g;
+      MM_CUDA(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+      MM_CUDA(cudaEventRecord(b->fork, b->st));
+      for (int i = 0; i < n; ++i) {
+        cudaStream_t hs = b->hs[i]->eng->stream();
+        MM_CUDA(cudaStreamWaitEvent(hs, b->fork, 0));
+        b->hs[i]->eng->rk4_enqueue(dt);
+        MM_CUDA(cudaEventRecord(b->joins[i], hs));
+        MM_CUDA(cudaStreamWaitEvent(b->st, b->joins[i], 0));
+      }
+      MM_CUDA(cudaStreamEndCapture(b->st, &g));
+      MM_CUDA(cudaGraphInstantiate(&b->graph, g, 0));
+      cudaGraphDestroy(g);
+      b->dt = dt;
+      b->versions.resize(n);
+      for (int i = 0; i < n; ++i) b->versions[i] = b->hs[i]->eng->params_version();
+    }
+    for (int64_t k = 0; k < nsteps; ++k) MM_CUDA(cudaGraphLaunch(b->graph, b->st));
+    // later work of every handle follows the batch
+    MM_CUDA(cudaEventRecord(b->done, b->st));
+    for (int i = 0; i < n; ++i) {
+      MM_CUDA(cudaStreamWaitEvent(b->hs[i]->eng->stream(), b->done, 0));
+      b->hs[i]->eng->rk4_count(nsteps, dt);
+    }
+    MM_CUDA(cudaGetLastError());
+    return MM_OK;
+  } catch (...) {
+    return fail(MM_ERR_CUDA, "mm_batch_rk4_run: exception");
+  }
 }
 
 }  // extern "C"

@@ -36,7 +36,7 @@ EXPORTS = (
     "mm_add_demag", "mm_add_demag_tensor", "mm_effective_field", "mm_term_field", "mm_energy",
     "mm_llg_rhs", "mm_average_m", "mm_rk4_run", "mm_rk4_state", "mm_dopri_set_tol", "mm_run_until",
     "mm_advance_step", "mm_dopri_reset", "mm_relax", "mm_kernel_time", "mm_rk4_launches_per_step",
-    "mm_energy_noalloc",
+    "mm_energy_noalloc", "mm_batch_create", "mm_batch_rk4_run", "mm_batch_get_stream", "mm_batch_destroy",
 )
 KERNELS = ("demag_fwd_x", "demag_fwd_y", "demag_conv", "demag_inv_y", "demag_inv_x", "rk4_stage", "rk4_step")
 
@@ -112,6 +112,10 @@ def load():
         "mm_kernel_time": ([_vp, i, i, _dp, _dp], i),
         "mm_rk4_launches_per_step": ([_vp, ctypes.POINTER(i)], i),
         "mm_energy_noalloc": ([ctypes.POINTER(MeshDesc), _vp, _vp] + [d] * 9 + [_vp, _vp], i),
+        "mm_batch_create": ([ctypes.POINTER(_vp), i, ctypes.POINTER(_vp)], i),
+        "mm_batch_rk4_run": ([_vp, d, i64], i),
+        "mm_batch_get_stream": ([_vp, ctypes.POINTER(_vp)], i),
+        "mm_batch_destroy": ([_vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -137,6 +141,32 @@ def dptr(a: np.ndarray | None):
         return None
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(_dp)
+
+
+class Batch:
+    """Owns one mm_batch over a list of Handles (kept alive by the batch)."""
+
+    def __init__(self, handles):
+        self.handles = list(handles)
+        arr = (_vp * len(self.handles))(*[h.h for h in self.handles])
+        self.b = _vp()
+        check(load().mm_batch_create(arr, len(self.handles), ctypes.byref(self.b)))
+
+    def rk4_run(self, dt, nsteps):
+        check(load().mm_batch_rk4_run(self.b, float(dt), int(nsteps)))
+
+    def stream(self) -> int:
+        s = _vp()
+        check(load().mm_batch_get_stream(self.b, ctypes.byref(s)))
+        return int(s.value or 0)
+
+    def close(self):
+        if getattr(self, "b", None) and _lib is not None:
+            _lib.mm_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        self.close()
 
 
 class Handle:

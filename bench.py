@@ -44,6 +44,14 @@ WORKLOADS = {
                axis=(0, 0, 1), demag=True, alpha=0.1, gamma=2.211e5, dt=5e-14, seed=105, zeeman=None),
     "c1": dict(nx=200, ny=50, nz=1, dx=2.5e-9, dy=2.5e-9, dz=3e-9, Ms=8e5, A=1.3e-11, Dbulk=None, Ku=None,
                axis=(0, 0, 1), demag=True, alpha=0.02, gamma=2.211e5, dt=1e-13, seed=101, zeeman="inplane30mT"),
+    # the reference's paper benchmark (figures/cpb/fig9/bench.jl:8-31): Heun,
+    # 4 nm cells, A=1e-13, demag, H=(0, 100 mT, 0), alpha 0.01, N x N x 1
+    "fig9": dict(nx=1000, ny=1000, nz=1, dx=4e-9, dy=4e-9, dz=4e-9, Ms=8e5, A=1e-13, Dbulk=None, Ku=None,
+                 axis=(0, 0, 1), demag=True, alpha=0.01, gamma=2.211e5, dt=1e-14, seed=109, zeeman="y100mT",
+                 integrator="heun", published=9.80e8),
+    "fig9_4000": dict(nx=4000, ny=4000, nz=1, dx=4e-9, dy=4e-9, dz=4e-9, Ms=8e5, A=1e-13, Dbulk=None, Ku=None,
+                      axis=(0, 0, 1), demag=True, alpha=0.01, gamma=2.211e5, dt=1e-14, seed=109, zeeman="y100mT",
+                      integrator="heun", published=1.045e9),
 }
 # batched workloads: many meshes advanced by one graph launch per RK4 step
 BATCHES = {
@@ -54,7 +62,8 @@ BATCHES = {
     "c3neb": dict(kind="neb", count=32, seed=103, nx=128, ny=128),
 }
 # the CPU baseline times a bounded block of the same physics
-CPU_SAMPLE = {"c2": (128, 128, 32), "c5": (256, 256, 16), "c1": (200, 50, 1)}
+CPU_SAMPLE = {"c2": (128, 128, 32), "c5": (256, 256, 16), "c1": (200, 50, 1), "fig9": (1000, 1000, 1),
+              "fig9_4000": (1000, 1000, 1)}
 
 
 def synth_inputs(w, shape=None):
@@ -68,6 +77,8 @@ def synth_inputs(w, shape=None):
         r = 0.03 * math.sqrt(rng.uniform())
         phi = rng.uniform(0, 2 * math.pi)
         H = (r * math.cos(phi) / MU0, r * math.sin(phi) / MU0, 0.0)
+    elif w["zeeman"] == "y100mT":
+        H = (0.0, 0.1 / MU0, 0.0)
     return m.reshape(-1), H
 
 
@@ -248,13 +259,17 @@ def cpu_baseline(wname, steps=1):
         s.add_zeeman(np.asarray(H))
     if w["demag"]:
         s.add_demag()
-    s.rk4(w["dt"], 1)  # warm-up (plans, pages)
+    heun = w.get("integrator") == "heun"
+    step = s.heun if heun else s.rk4
+    step(w["dt"], 1)  # warm-up (plans, pages)
     t0 = time.perf_counter()
-    s.rk4(w["dt"], steps)
+    step(w["dt"], steps)
     dt = time.perf_counter() - t0
-    return {"value": n * steps / dt, "unit": "cell-steps/s", "cores": max_threads(), "kind": "port",
-            "sample": f"{nx}x{ny}x{nz} block of the {wname} physics, FP64, {steps} RK4 step(s) after 1 warm-up, "
-                      f"{dt:.1f} s"}
+    evals = 2 if heun else 1
+    return {"value": evals * n * steps / dt, "unit": "cell-evals/s" if heun else "cell-steps/s",
+            "cores": max_threads(), "kind": "port",
+            "sample": f"{nx}x{ny}x{nz} block of the {wname} physics, FP64, {steps} "
+                      f"{'Heun' if heun else 'RK4'} step(s) after 1 warm-up, {dt:.1f} s"}
 
 
 def dist_init():
@@ -307,13 +322,18 @@ def run_reference(args):
         vals.append(base["value"])
     v = statistics.median(vals)
     n = w["nx"] * w["ny"] * w["nz"]
-    line = {"metric": "LLG cell-steps/s (H_eff+demag+RK4)", "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
-            "steps": len(vals), "warmup": args.warmup, "ms_per_step": 1e3 * n / v, "higher_is_better": True,
+    heun = w.get("integrator") == "heun"
+    evals = 2 if heun else 1
+    line = {"metric": ("LLG cell-evals/s (H_eff+demag+Heun, 2 evals per step)" if heun
+                       else "LLG cell-steps/s (H_eff+demag+RK4)"),
+            "value": v, "unit": base["unit"], "n_gpus": args.gpus,
+            "steps": len(vals), "warmup": args.warmup, "ms_per_step": 1e3 * evals * n / v, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy PCG64)",
-            "config": {"workload": f"{wname}: {w['nx']}x{w['ny']}x{w['nz']} RK4", "form": "fp64", "sample": base["sample"]},
+            "config": {"workload": f"{wname}: {w['nx']}x{w['ny']}x{w['nz']} {'Heun' if heun else 'RK4'}",
+                       "form": "fp64", "sample": base["sample"]},
             "impl": "reference",
             "cpu_baseline": {**base, "value": v},
-            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": v, "unit": base["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -335,13 +355,16 @@ def run_native(args):
     dt = w["dt"]
     forms = {"fp32": _lib.MM_FP32, "fp64": _lib.MM_FP64}
     results = {}
-    if args.integrator == "dopri":
+    integ = args.integrator or w.get("integrator", "rk4")
+    if integ == "dopri":
         return run_dopri(args, w, wname, n, forms, rank, ws, device, dist)
+    heun = integ == "heun"
+    step_fn = "mm_heun_run" if heun else "mm_rk4_run"
     for fname in ((args.only,) if args.only else ("fp32", "fp64")):
         h, m0 = setup_native(w, forms[fname], device)
         stream = torch.cuda.ExternalStream(h.stream(), device=device)
         for _ in range(args.warmup):
-            h.call("mm_rk4_run", dt, 1)
+            h.call(step_fn, dt, 1)
         h.call("mm_synchronize")
         if dist is not None:
             dist.barrier()
@@ -351,7 +374,7 @@ def run_native(args):
         if sampler:
             sampler.__enter__()
         e0.record(stream)
-        h.call("mm_rk4_run", dt, args.steps)
+        h.call(step_fn, dt, args.steps)
         e1.record(stream)
         e1.synchronize()
         if sampler:
@@ -364,8 +387,10 @@ def run_native(args):
         if dist is not None:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_max = float(t.item())
+        # a Heun step is two of the four field + stage passes of an RK4 step
+        lps = h.rk4_launches() // 2 if heun else h.rk4_launches()
         res = {"ms_per_step": ms_max / args.steps, "value": ws * n * args.steps / (ms_max / 1e3),
-               "launches_per_step": h.rk4_launches(), "device_bytes": h.device_bytes()}
+               "launches_per_step": lps, "device_bytes": h.device_bytes()}
         if sampler:
             res["clocks"] = sampler.summary()
         if args.quick:
@@ -390,7 +415,7 @@ def run_native(args):
             k2 = max(3, args.steps // 10)
             for _ in range(2):
                 h.call("mm_set_m", pin_in_p)
-                h.call("mm_rk4_run", dt, 1)
+                h.call(step_fn, dt, 1)
                 h.call("mm_get_m", pin_out_p)
             if dist is not None:
                 dist.barrier()
@@ -398,7 +423,7 @@ def run_native(args):
             e0.record(stream)
             for _ in range(k2):
                 h.call("mm_set_m", pin_in_p)
-                h.call("mm_rk4_run", dt, 1)
+                h.call(step_fn, dt, 1)
                 h.call("mm_get_m", pin_out_p)
             e1.record(stream)
             e1.synchronize()
@@ -424,20 +449,30 @@ def run_native(args):
         dom = max(kern, key=lambda k: kern[k]["ms"])
         traffic = profiled_traffic(wname, "fp32").get(dom)
         ach = kern[dom]["alg_bytes"] / (kern[dom]["ms"] * 1e-3) / 1e9
-        step = r["kernels"].get("rk4_step", {})
+        step = r["kernels"].get("rk4_step", {}) if not heun else {}
+        # Heun is quoted per right-hand-side evaluation, two per step
+        # (figures/cpb/fig9/bench.jl:28-31)
+        evals = 2 if heun else 1
+        unit = "cell-evals/s" if heun else "cell-steps/s"
+        if heun:
+            r["e2e"]["value"] *= evals
+            r["e2e"]["unit"] = unit
         line = {
-            "metric": "LLG cell-steps/s (H_eff+demag+RK4)",
-            "value": r["value"], "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps,
+            "metric": ("LLG cell-evals/s (H_eff+demag+Heun, 2 evals per step)" if heun
+                       else "LLG cell-steps/s (H_eff+demag+RK4)"),
+            "value": evals * r["value"], "unit": unit, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy PCG64)",
+            "vs_baseline": (evals * r["value"] / w["published"]) if w.get("published") else None,
+            "dtype": "f32", "data": "synthetic (seeded numpy PCG64)",
             "config": {"workload": f"{wname}: {w['nx']}x{w['ny']}x{w['nz']} cells, exch"
                                    + (" + bulk DMI" if w["Dbulk"] else "") + (" + anis" if w["Ku"] else "")
-                                   + (" + zeeman" if w["zeeman"] else "") + " + demag, RK4 dt=%g" % dt,
+                                   + (" + zeeman" if w["zeeman"] else "") + " + demag, "
+                                   + ("Heun" if heun else "RK4") + " dt=%g" % dt,
                        "form": "fp32 (compensated RK state; fp64 tensor/energies)",
                        "parallelism": f"replicas x{ws}", "l2": "working set > 126 MB L2 (inputs larger than L2)"},
             "e2e": r["e2e"],
             "gpu_launches": r["launches_per_step"] * args.steps,
-            "fp64": {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
+            "fp64": {"value": evals * results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
                      "fp32_over_fp64": r["value"] / results["fp64"]["value"]},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "peak_kind": peak_kind,
@@ -511,7 +546,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", choices=["fp32", "fp64"], help="time one form only (profiling runs)")
     ap.add_argument("--quick", action="store_true", help="timed steps only: no e2e, kernel timing or CPU leg")
-    ap.add_argument("--integrator", default="rk4", choices=["rk4", "dopri"])
+    ap.add_argument("--integrator", default=None, choices=["rk4", "heun", "dopri"],
+                    help="default: the workload's own (RK4, or Heun for fig9)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -136,8 +136,10 @@ int mm_average_m(mm_handle* h, double* m3);
 
 /* advance_step(sim, ::RungeKutta) x nsteps  src/integrator/rk.jl:23-52 */
 int mm_rk4_run(mm_handle* h, double dt, int64_t nsteps);
-/* RungeKutta t and nsteps (t = nsteps * dt) */
+/* RungeKutta / ModifiedEuler t and nsteps (t = nsteps * dt) */
 int mm_rk4_state(mm_handle* h, double* t, int64_t* nsteps);
+/* advance_step(sim, ::ModifiedEuler) x nsteps (Heun)  src/integrator/heun.jl:28-49 */
+int mm_heun_run(mm_handle* h, double dt, int64_t nsteps);
 
 /* Dormand-Prince (DOPRI54) tolerance, default 1e-6  src/driver.jl:126,134 */
 int mm_dopri_set_tol(mm_handle* h, double tol);
@@ -148,6 +150,19 @@ int mm_run_until(mm_handle* h, double t_end, mm_stats* stats);
 int mm_advance_step(mm_handle* h, mm_stats* stats);
 /* Reset the adaptive integrator (t = 0, step sizes and counters cleared). */
 int mm_dopri_reset(mm_handle* h);
+
+/* Adaptive Runge-Kutta methods: Sim(mesh; integrator="DormandPrince" |
+ * "BS23" | "CashKarp54" | "Fehlberg54")  src/driver.jl:102-140,
+ * src/integrator/adaptive_rk.jl:248-266 */
+typedef enum {
+  MM_RK_DORMAND_PRINCE = 0,
+  MM_RK_BS23 = 1,
+  MM_RK_CASH_KARP54 = 2,
+  MM_RK_FEHLBERG54 = 3
+} mm_rk_method;
+/* Select the method used by mm_run_until / mm_advance_step / mm_relax(LLG);
+ * resets the adaptive state as a new Sim would (default MM_RK_DORMAND_PRINCE). */
+int mm_set_adaptive_method(mm_handle* h, int method);
 
 /* relax(sim; max_steps, stopping_dmdt)  src/sim.jl:392-490 with the SD
  * driver (src/sd.jl:9-98) or the LLG driver with Dormand-Prince */

@@ -84,10 +84,12 @@ class EngineBase {
   virtual int average_m(double* m3) = 0;
   virtual int rk4_run(double dt, int64_t n) = 0;
   virtual int rk4_state(double* t, int64_t* n) = 0;
+  virtual int heun_run(double dt, int64_t n) = 0;
   virtual int dopri_tol(double tol) = 0;
   virtual int run_until(double t_end, mm_stats* st) = 0;
   virtual int advance_step(mm_stats* st) = 0;
   virtual int dopri_reset() = 0;
+  virtual int set_method(int method) = 0;
   virtual int relax(int driver, int64_t max_steps, double stop, int64_t* steps, double* max_dmdt) = 0;
   virtual int kernel_time(int kernel, int reps, double* ms, double* bytes) = 0;
   virtual int rk4_launches() const = 0;
@@ -111,6 +113,7 @@ class Engine : public EngineBase {
     cudaSetDevice(device);
     if (rk_graph) cudaGraphExecDestroy(rk_graph);
     if (dp_graph) cudaGraphExecDestroy(dp_graph);
+    if (he_graph) cudaGraphExecDestroy(he_graph);
     demag.reset();
     for (void* p : allocs_) cudaFree(p);
     if (st_) cudaStreamDestroy(st_);
@@ -166,6 +169,13 @@ class Engine : public EngineBase {
     MM_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, st_));
     MM_CUDA(cudaStreamSynchronize(st_));
     if (hflag) return fail(MM_ERR_NAN, "NaN is given by the input m0!");
+    if (ctrl && hctrl.fsal) {
+      // a new state: the stored last-stage derivative of an FSAL method no
+      // longer belongs to y_current, so the next attempt evaluates k1
+      if (int rc = pull_ctrl()) return rc;
+      hctrl.succeed = 0;
+      return push_ctrl();
+    }
     return MM_OK;
   }
 
@@ -465,6 +475,51 @@ class Engine : public EngineBase {
     }
   }
 
+  // advance_step(sim, ::ModifiedEuler) x nsteps  src/integrator/heun.jl:28-49
+  void enqueue_heun_step(double h) {
+    const FieldArgs<R> fa = fargs(~0u);
+    for (int st = 1; st <= 2; ++st) {
+      const R* yin = st == 1 ? m : yA;
+      if ((mask & TB_DEMAG) && demag) demag->apply(yin, Ms, Hd, st_);
+      StageArgs<R> sa{};
+      sa.m = m;
+      sa.m_lo = m_lo;
+      sa.acc = acc;
+      sa.ynext = yA;
+      sa.h = h;
+      sa.stage = st;
+      sa.scheme = 1;
+      launch_stage<R>(SM_RK4, fa, yin, sa, st_);
+    }
+  }
+
+  int heun_run(double dt, int64_t n) override {
+    if (int rc = need_ms()) return rc;
+    if (n < 0 || !(dt > 0)) return fail(MM_ERR_ARG, "heun: need dt > 0 and nsteps >= 0");
+    int rc;
+    if (!acc && (rc = alloc(acc, 3 * N))) return rc;
+    if (!he_graph || he_dt != dt || he_version != version) {
+      if (he_graph) cudaGraphExecDestroy(he_graph);
+      he_graph = nullptr;
+      cudaGraph_t g;
+      MM_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+      enqueue_heun_step(dt);
+      MM_CUDA(cudaStreamEndCapture(st_, &g));
+      MM_CUDA(cudaGraphInstantiate(&he_graph, g, 0));
+      cudaGraphDestroy(g);
+      he_dt = dt;
+      he_version = version;
+    }
+    for (int64_t i = 0; i < n; ++i) MM_CUDA(cudaGraphLaunch(he_graph, st_));
+    rk_n += n;
+    rk_t = static_cast<double>(rk_n) * dt;  // integrator.t = nsteps * h (heun.jl:45)
+    MM_CUDA(cudaGetLastError());
+    return MM_OK;
+  }
+  cudaGraphExec_t he_graph = nullptr;
+  double he_dt = 0.0;
+  uint64_t he_version = 0;
+
   int rk4_run(double dt, int64_t n) override {
     if (int rc = need_ms()) return rc;
     if (n < 0 || !(dt > 0)) return fail(MM_ERR_ARG, "rk4: need dt > 0 and nsteps >= 0");
@@ -613,21 +668,47 @@ class Engine : public EngineBase {
     if ((rc = alloc(yB, 3 * N)) || (rc = alloc(yn, 3 * N)) || (kF32 && (rc = alloc(yn_lo, 3 * N))) ||
         (rc = alloc(ctrl, 1)))
       return rc;
-    hctrl = DopriCtrl{};
-    hctrl.tol = tol;
-    hctrl.inner = 1;
+    fresh_ctrl();
     MM_CUDA(cudaMemcpyAsync(ctrl, &hctrl, sizeof(DopriCtrl), cudaMemcpyHostToDevice, st_));
     MM_CUDA(cudaStreamSynchronize(st_));
     return MM_OK;
   }
 
+  // AdaptiveRK(n_total, method, rhs_fun, tol) state  src/integrator/adaptive_rk.jl:57-87
+  void fresh_ctrl() {
+    const RkTableau& tb = rk_tableau(method);
+    hctrl = DopriCtrl{};
+    hctrl.tol = tol;
+    hctrl.inner = 1;
+    hctrl.fsal = tb.fsal;
+    hctrl.order = tb.order_emb;
+    hctrl.nstage = tb.nstage;
+  }
+
+  // Sim(mesh; integrator=...) with an adaptive method  src/driver.jl:102-140
+  int set_method(int mth) override {
+    if (mth < 0 || mth >= RK_NMETHODS) return fail(MM_ERR_ARG, "unknown adaptive method %d", mth);
+    method = mth;
+    if (dp_graph) cudaGraphExecDestroy(dp_graph);
+    dp_graph = nullptr;
+    if (!ctrl) return MM_OK;
+    fresh_ctrl();
+    return push_ctrl();
+  }
+  int method = RK_DOPRI54;
+
+  // stage s of one attempt reads the output of stage s-1 (m for s = 1) and
+  // writes the next input to yA / yB alternately, the solution to yn
   void enqueue_dopri_attempt() {
     const FieldArgs<R> fa = fargs(~0u);
-    for (int s = 1; s <= 7; ++s) {
-      const R* yin = s == 1 ? m : (s == 7 ? yn : (s % 2 == 0 ? yA : yB));
-      R* target = s == 6 ? yn : (s % 2 == 1 ? yA : yB);
-      if ((mask & TB_DEMAG) && demag) demag->apply(yin, Ms, Hd, st_, &ctrl->active);
+    const RkTableau& tb = rk_tableau(method);
+    auto target_of = [&](int s) { return s == tb.sol ? yn : (s % 2 == 1 ? yA : yB); };
+    for (int s = 1; s <= tb.nstage; ++s) {
+      const R* yin = s == 1 ? m : target_of(s - 1);
+      R* target = s <= tb.sol ? target_of(s) : nullptr;
+      if ((mask & TB_DEMAG) && demag) demag->apply(yin, Ms, Hd, st_, s == 1 ? &ctrl->eval1 : &ctrl->active);
       StageArgs<R> sa{};
+      sa.method = method;
       sa.m = m;
       sa.m_lo = m_lo;
       sa.ynext = target;
@@ -659,7 +740,7 @@ class Engine : public EngineBase {
     double mx = 0.0;
     MM_CUDA(cudaMemcpyAsync(&mx, scal, sizeof(double), cudaMemcpyDeviceToHost, st_));
     MM_CUDA(cudaStreamSynchronize(st_));
-    const double order_main = 5.0;
+    const double order_main = rk_tableau(method).order_main;
     const double r_step = mx / (0.824 * std::pow(hctrl.tol, 1.0 / order_main));
     double abs_step = 1e-12, tmp = 1e-12;
     if (abs_step * r_step > 0.001) tmp = 0.001 / r_step;
@@ -718,9 +799,7 @@ class Engine : public EngineBase {
 
   int dopri_reset() override {
     if (!ctrl) return MM_OK;
-    hctrl = DopriCtrl{};
-    hctrl.tol = tol;
-    hctrl.inner = 1;
+    fresh_ctrl();
     return push_ctrl();
   }
 
@@ -751,6 +830,7 @@ class Engine : public EngineBase {
     hctrl.inner = 1;
     hctrl.single = 0;
     hctrl.active = 1;
+    hctrl.eval1 = (hctrl.fsal && hctrl.succeed) ? 0 : 1;
     if (int rc = push_ctrl()) return rc;
     if (int rc = run_attempts()) return rc;
     fill_stats(hctrl, st);
@@ -772,6 +852,7 @@ class Engine : public EngineBase {
     hctrl.inner = 1;
     hctrl.single = 1;
     hctrl.active = 1;
+    hctrl.eval1 = (hctrl.fsal && hctrl.succeed) ? 0 : 1;
     if (int rc = push_ctrl()) return rc;
     if (int rc = run_attempts()) return rc;
     fill_stats(hctrl, st);
@@ -1050,10 +1131,12 @@ int mm_average_m(mm_handle* h, double* m3) {
 }
 int mm_rk4_run(mm_handle* h, double dt, int64_t n) { MM_HANDLE(h); MM_GUARD(h->eng->rk4_run(dt, n)); }
 int mm_rk4_state(mm_handle* h, double* t, int64_t* n) { MM_HANDLE(h); MM_GUARD(h->eng->rk4_state(t, n)); }
+int mm_heun_run(mm_handle* h, double dt, int64_t n) { MM_HANDLE(h); MM_GUARD(h->eng->heun_run(dt, n)); }
 int mm_dopri_set_tol(mm_handle* h, double tol) { MM_HANDLE(h); MM_GUARD(h->eng->dopri_tol(tol)); }
 int mm_run_until(mm_handle* h, double t, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h->eng->run_until(t, s)); }
 int mm_advance_step(mm_handle* h, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h->eng->advance_step(s)); }
 int mm_dopri_reset(mm_handle* h) { MM_HANDLE(h); MM_GUARD(h->eng->dopri_reset()); }
+int mm_set_adaptive_method(mm_handle* h, int method) { MM_HANDLE(h); MM_GUARD(h->eng->set_method(method)); }
 int mm_relax(mm_handle* h, int driver, int64_t max_steps, double stop, int64_t* steps, double* mx) {
   MM_HANDLE(h);
   if (driver != MM_DRIVER_SD && driver != MM_DRIVER_LLG) return fail(MM_ERR_ARG, "driver must be SD or LLG");

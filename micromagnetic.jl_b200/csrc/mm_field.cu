@@ -308,15 +308,44 @@ __device__ __forceinline__ void llg_rhs(const FieldArgs<R>& a, int64_t I, const 
   f[2] = c * g3 + cl * g3;
 }
 
-// Dormand-Prince 5(4) tableau (src/integrator/adaptive_rk_steps.jl:49-57)
-__constant__ double c_dp_a[6][6] = {
-    {1.0 / 5, 0, 0, 0, 0, 0},
-    {3.0 / 40, 9.0 / 40, 0, 0, 0, 0},
-    {44.0 / 45, -56.0 / 15, 32.0 / 9, 0, 0, 0},
-    {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729, 0, 0},
-    {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656, 0},
-    {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}};
-__constant__ double c_dp_w[7] = {71.0 / 57600, 0, -71.0 / 16695, 71.0 / 1920, -17253.0 / 339200, 22.0 / 525, -1.0 / 40};
+// Butcher tables of the adaptive methods (src/integrator/adaptive_rk_steps.jl:
+// bs23 11-47, dopri54 49-107, cashkarp54 110-168, fehlberg54 171-229), laid
+// out as RkTableau: rows a[s-1] give the input of stage s+1; row sol-1 is the
+// solution; w are the error weights.
+#define MM_RK_TABLES                                                                                          \
+  {                                                                                                           \
+    {7, 6, 7, 0, 5, 4,                                                                                        \
+     {{1.0 / 5},                                                                                              \
+      {3.0 / 40, 9.0 / 40},                                                                                   \
+      {44.0 / 45, -56.0 / 15, 32.0 / 9},                                                                      \
+      {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729},                                        \
+      {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656},                              \
+      {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}},                                 \
+     {71.0 / 57600, 0, -71.0 / 16695, 71.0 / 1920, -17253.0 / 339200, 22.0 / 525, -1.0 / 40}},               \
+    {4, 3, 4, 1, 3, 2,                                                                                        \
+     {{0.5}, {0, 0.75}, {2.0 / 9, 1.0 / 3, 4.0 / 9}},                                                         \
+     {-5.0 / 72, 1.0 / 12, 1.0 / 9, -1.0 / 8}},                                                               \
+    {6, 6, 6, 0, 5, 4,                                                                                        \
+     {{1.0 / 5},                                                                                              \
+      {3.0 / 40, 9.0 / 40},                                                                                   \
+      {3.0 / 10, -9.0 / 10, 6.0 / 5},                                                                         \
+      {-11.0 / 54, 5.0 / 2, -70.0 / 27, 35.0 / 27},                                                           \
+      {1631.0 / 55296, 175.0 / 512, 575.0 / 13824, 44275.0 / 110592, 253.0 / 4096},                           \
+      {37.0 / 378, 0, 250.0 / 621, 125.0 / 594, 0, 512.0 / 1771}},                                            \
+     {-277.0 / 64512, 0, 6925.0 / 370944, -6925.0 / 202752, -277.0 / 14336, 277.0 / 7084}},                  \
+    {6, 6, 6, 0, 5, 4,                                                                                        \
+     {{1.0 / 4},                                                                                              \
+      {3.0 / 32, 9.0 / 32},                                                                                   \
+      {1932.0 / 2197, -7200.0 / 2197, 7296.0 / 2197},                                                         \
+      {439.0 / 216, -8.0, 3680.0 / 513, -845.0 / 4104},                                                       \
+      {-8.0 / 27, 2.0, -3544.0 / 2565, 1859.0 / 4104, -11.0 / 40},                                            \
+      {16.0 / 135, 0, 6656.0 / 12825, 28561.0 / 56430, -9.0 / 50, 2.0 / 55}},                                 \
+     {-1.0 / 360, 0, 128.0 / 4275, 2197.0 / 75240, -1.0 / 50, -2.0 / 55}},                                    \
+  }
+
+__constant__ RkTableau c_rk[RK_NMETHODS] = MM_RK_TABLES;
+static const RkTableau h_rk[RK_NMETHODS] = MM_RK_TABLES;
+const RkTableau& rk_tableau(int method) { return h_rk[method]; }
 
 template <typename R, int MODE>
 __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage(FieldArgs<R> a, const R* __restrict__ y, StageArgs<R> s) {
@@ -343,8 +372,10 @@ __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage
       av[c] = s.stage > 1 ? s.acc[c * N + I] : R(0);
     }
   }
+  // FSAL: stage 1 takes k1 from the last stage of the accepted attempt
+  const bool reuse = MODE == SM_DOPRI && s.stage == 1 && !s.ctrl->eval1;
   if (live) {
-    cell_heff<R, MODE == SM_ENERGY || MODE == SM_FIELD>(a, y, I, i, j, k, m, h, e);
+    if (!reuse) cell_heff<R, MODE == SM_ENERGY || MODE == SM_FIELD>(a, y, I, i, j, k, m, h, e);
     if (MODE == SM_FIELD) {
       s.out[I] = h[0];
       s.out[N + I] = h[1];
@@ -361,6 +392,40 @@ __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage
       s.out[I] = f[0];
       s.out[N + I] = f[1];
       s.out[2 * N + I] = f[2];
+    } else if (MODE == SM_RK4 && s.scheme == 1) {
+      // advance_step(::ModifiedEuler)  src/integrator/heun.jl:28-49:
+      // k1 = f(m); y = m + h k1; k2 = f(y); m = normalise(m + (h/2) k1 + (h/2) k2)
+      R f[3];
+      llg_rhs(a, I, m, h, f);
+      if (s.stage == 1) {
+        const R hh = static_cast<R>(s.h);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          s.acc[c * N + I] = f[c];
+          s.ynext[c * N + I] = kF32 ? mN[c] + (mL[c] + hh * f[c]) : mN[c] + hh * f[c];
+        }
+      } else {
+        const R h2 = static_cast<R>(0.5 * s.h);
+        R mv[3];
+        if constexpr (kF32) {
+          float lo[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            mv[c] = mN[c];
+            lo[c] = mL[c];
+            df_add(mv[c], lo[c], h2 * av[c] + h2 * f[c]);
+          }
+          df_normalise(mv, lo);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s.m_lo[c * N + I] = lo[c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) mv[c] = mN[c] + h2 * av[c] + h2 * f[c];
+          plain_normalise(mv);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s.m[c * N + I] = mv[c];
+      }
     } else if (MODE == SM_RK4) {
       // advance_step(::RungeKutta)  src/integrator/rk.jl:23-52
       R f[3];
@@ -403,15 +468,25 @@ __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage
         for (int c = 0; c < 3; ++c) s.m[c * N + I] = mv[c];
       }
     } else if (MODE == SM_DOPRI) {
-      // rk_step_dopri54!  src/integrator/adaptive_rk_steps.jl:49-107
-      R f[3];
-      llg_rhs(a, I, m, h, f);
+      // rk_step_bs23! / rk_step_dopri54! / rk_step_cashkarp54! /
+      // rk_step_fehlberg54!  src/integrator/adaptive_rk_steps.jl:11-229
+      const RkTableau& tb = c_rk[s.method];
       const int st = s.stage;
-      const double hstep = s.ctrl->step;
+      R f[3];
+      if (reuse) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) s.k[st - 1][c * N + I] = f[c];
-      if (st <= 6) {
-        const double* arow = c_dp_a[st - 1];
+        for (int c = 0; c < 3; ++c) f[c] = s.k[tb.nstage - 1][c * N + I];
+      } else {
+        llg_rhs(a, I, m, h, f);
+      }
+      const double hstep = s.ctrl->step;
+      if (st < tb.err || (tb.fsal && st == tb.nstage)) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s.k[st - 1][c * N + I] = f[c];
+      }
+      R yabs[3];  // y_next of the error norm
+      if (st <= tb.sol) {
+        const double* arow = tb.a[st - 1];
         R v[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -433,14 +508,14 @@ __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage
             v[c] = static_cast<R>(acc);
           }
         }
-        if (st < 6) {
+        if (st < tb.sol) {
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             if constexpr (kF32) v[c] = s.m[c * N + I] + (s.m_lo[c * N + I] + v[c]);
             s.ynext[c * N + I] = v[c];
           }
         } else {
-          // 5th-order solution, normalised before k7 (adaptive_rk_steps.jl:92-96)
+          // the solution is normalised before it is used (adaptive_rk_steps.jl:35,96,156,217)
           if constexpr (kF32) {
             float hi[3], lo[3];
 #pragma unroll
@@ -454,31 +529,38 @@ __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage
             for (int c = 0; c < 3; ++c) {
               s.ynext[c * N + I] = hi[c];
               s.ynext_lo[c * N + I] = lo[c];
+              yabs[c] = hi[c];
             }
           } else {
             plain_normalise(v);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) s.ynext[c * N + I] = v[c];
+            for (int c = 0; c < 3; ++c) {
+              s.ynext[c * N + I] = v[c];
+              yabs[c] = v[c];
+            }
           }
         }
       } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) yabs[c] = m[c];
+      }
+      if (st == tb.err) {
         // error estimate: max |sum_j w_j k_j| / (1 + |y_next|)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           double et = 0.0;
-          et = c_dp_w[0] * double(s.k[0][c * N + I]);
-          et += c_dp_w[2] * double(s.k[2][c * N + I]);
-          et += c_dp_w[3] * double(s.k[3][c * N + I]);
-          et += c_dp_w[4] * double(s.k[4][c * N + I]);
-          et += c_dp_w[5] * double(s.k[5][c * N + I]);
-          et += c_dp_w[6] * double(f[c]);
-          const double v = fabs(et / (1.0 + fabs(double(m[c]))));
+          for (int j = 0; j < st; ++j) {
+            if (tb.w[j] == 0.0) continue;
+            const double kj = j == st - 1 ? double(f[c]) : double(s.k[j][c * N + I]);
+            et += tb.w[j] * kj;
+          }
+          const double v = fabs(et / (1.0 + fabs(double(yabs[c]))));
           red = (v > red || isnan(v)) ? v : red;
         }
       }
     }
   }
-  if (MODE == SM_ENERGY || (MODE == SM_DOPRI && s.stage == 7)) {
+  if (MODE == SM_ENERGY || (MODE == SM_DOPRI && s.stage == c_rk[s.method].err)) {
     // deterministic block reduction in FP64
     __shared__ double sh[kStageThreads / 32][kNTerms];
     const int lane = tid & 31, warp = tid >> 5;

@@ -56,7 +56,23 @@ template <typename R> struct FieldArgs {
 
 enum StageMode { SM_FIELD = 0, SM_RHS = 1, SM_RK4 = 2, SM_ENERGY = 3, SM_DOPRI = 4 };
 
-// Dormand-Prince device-side controller state (src/integrator/adaptive_rk.jl:93-186)
+// Adaptive Runge-Kutta methods of src/integrator/adaptive_rk.jl:248-266
+enum RkMethod { RK_DOPRI54 = 0, RK_BS23 = 1, RK_CASHKARP54 = 2, RK_FEHLBERG54 = 3, RK_NMETHODS = 4 };
+
+// One embedded pair in the layout the stage kernel walks (the Butcher tables
+// of src/integrator/adaptive_rk_steps.jl).  Stage s (1-based) evaluates
+// k_s = f(y_s); for s <= sol it then forms sum_j a[s-1][j] h k_{j+1}, which
+// is the input of stage s+1, or for s == sol the solution y_next (normalised).
+// The error sum_j w[j] k_{j+1} is taken at stage err (sol, or sol+1 when it
+// needs f(y_next)).
+struct RkTableau {
+  int nstage, sol, err, fsal, order_main, order_emb;
+  double a[7][7];
+  double w[7];
+};
+const RkTableau& rk_tableau(int method);  // host copy
+
+// Adaptive RK device-side controller state (src/integrator/adaptive_rk.jl:93-186)
 struct DopriCtrl {
   double t, step, step_next, t_final, tol;
   double err;               // last scaled error norm
@@ -68,6 +84,9 @@ struct DopriCtrl {
   int need_init;            // compute_initial_step pending
   int single;               // stop after one accepted step (advance_step)
   double init_rmax;         // max |f| for the initial step
+  int succeed;              // integrator.succeed: last attempt that reached the acceptance test
+  int eval1;                // stage 1 evaluates f (0: FSAL reuse of the last stage, or inactive)
+  int fsal, order, nstage;  // of the method in use
 };
 
 template <typename R> struct StageArgs {
@@ -80,10 +99,12 @@ template <typename R> struct StageArgs {
   R* acc;                   // RK4 accumulator
   R* ynext;                 // next stage input
   R* ynext_lo;              // DOPRI stage 7: low part of y_next
-  R* k[7];                  // DOPRI stage derivatives
-  double h;                 // RK4 step
+  R* k[7];                  // adaptive RK stage derivatives
+  double h;                 // RK4 / Heun step
   int stage;                // 1-based
-  const DopriCtrl* ctrl;    // DOPRI: step size and active flag
+  int scheme;               // fixed-step scheme: 0 RK4, 1 Heun (modified Euler)
+  int method;               // SM_DOPRI: RkMethod
+  const DopriCtrl* ctrl;    // SM_DOPRI: step size and active flag
 };
 
 template <typename R>

@@ -34,15 +34,16 @@ __global__ void k_dopri_control(DopriCtrl* __restrict__ c, const double* __restr
   }
   if (threadIdx.x != 0) return;
   const double safety = 0.824, facmax = 5.0, facmin = 0.2;
-  const int order = 4;  // embedded order of DOPRI54
+  const int order = c->order;  // order_embedded of the method
   c->attempts += 1;
-  c->nfevals += 7;
+  c->nfevals += c->eval1 + (c->nstage - 1);
   const double err = sh[0] * c->step / c->tol;
   c->err = err;
   if (isnan(err)) {
     c->step_next = 1e-14;
     c->status = 1;
     c->active = 0;
+    c->eval1 = 0;
     c->accepted_last = 0;
     return;
   }
@@ -50,9 +51,13 @@ __global__ void k_dopri_control(DopriCtrl* __restrict__ c, const double* __restr
   if (c->inner > 50) {
     c->status = 2;
     c->active = 0;
+    c->eval1 = 0;
     c->accepted_last = 0;
     return;
   }
+  c->succeed = err <= 1.0;
+  // the next attempt reuses the last stage as k1 after an accepted FSAL step
+  c->eval1 = (c->succeed && c->fsal) ? 0 : 1;
   if (err <= 1.0) {
     c->accepted_last = 1;
     c->nsteps += 1;
@@ -62,6 +67,7 @@ __global__ void k_dopri_control(DopriCtrl* __restrict__ c, const double* __restr
     c->inner = 1;
     if (c->single || !(c->t < c->t_final)) {
       c->active = 0;
+      c->eval1 = 0;
     } else {
       if (c->step_next + c->t > c->t_final) c->step_next = c->t_final - c->t;
       c->step = c->step_next;

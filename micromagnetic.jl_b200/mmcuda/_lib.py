@@ -24,6 +24,8 @@ STATUS = {
     -7: "MM_ERR_UNSUPPORTED",
 }
 MM_FP64, MM_FP32 = 0, 1
+MM_RK_DORMAND_PRINCE, MM_RK_BS23, MM_RK_CASH_KARP54, MM_RK_FEHLBERG54 = 0, 1, 2, 3
+RK_METHODS = {"DormandPrince": 0, "DOPRI54": 0, "BS23": 1, "CashKarp54": 2, "Fehlberg54": 3, "RKF54": 3}
 TERM_ZEEMAN, TERM_EXCH, TERM_DMI_BULK, TERM_DMI_INTERFACIAL, TERM_ANIS, TERM_DEMAG = range(6)
 NTERMS = 6
 DRIVER_SD, DRIVER_LLG = 0, 1
@@ -37,6 +39,7 @@ EXPORTS = (
     "mm_llg_rhs", "mm_average_m", "mm_rk4_run", "mm_rk4_state", "mm_dopri_set_tol", "mm_run_until",
     "mm_advance_step", "mm_dopri_reset", "mm_relax", "mm_kernel_time", "mm_rk4_launches_per_step",
     "mm_energy_noalloc", "mm_batch_create", "mm_batch_rk4_run", "mm_batch_get_stream", "mm_batch_destroy",
+    "mm_heun_run", "mm_set_adaptive_method",
 )
 KERNELS = ("demag_fwd_x", "demag_fwd_y", "demag_conv", "demag_inv_y", "demag_inv_x", "rk4_stage", "rk4_step")
 
@@ -104,6 +107,8 @@ def load():
         "mm_average_m": ([_vp, _dp], i),
         "mm_rk4_run": ([_vp, d, i64], i),
         "mm_rk4_state": ([_vp, _dp, ctypes.POINTER(i64)], i),
+        "mm_heun_run": ([_vp, d, i64], i),
+        "mm_set_adaptive_method": ([_vp, i], i),
         "mm_dopri_set_tol": ([_vp, d], i),
         "mm_run_until": ([_vp, d, ctypes.POINTER(Stats)], i),
         "mm_advance_step": ([_vp, ctypes.POINTER(Stats)], i),

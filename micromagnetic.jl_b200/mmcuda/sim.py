@@ -155,16 +155,30 @@ class Term:
         return e
 
 
+# integrator name -> fixed-step entry point and default step, or adaptive
+# method index (src/driver.jl:102-140)
+_FIXED = {"RungeKutta": ("mm_rk4_run", 5e-14), "Heun": ("mm_heun_run", 1e-14)}
+_INTEGRATORS = set(_FIXED) | set(_lib.RK_METHODS)
+
+
 class _Integrator:
-    def __init__(self, sim, kind):
+    def __init__(self, sim, name):
         self._sim = sim
-        self.kind = kind          # "RungeKutta" or "DormandPrince"
-        self._step = 5e-14 if kind == "RungeKutta" else 0.0  # src/driver.jl:130
+        self.name = name
+        self.adaptive = name in _lib.RK_METHODS
+        self.kind = "AdaptiveRK" if self.adaptive else name
+        self._step = 0.0 if self.adaptive else _FIXED[name][1]
         self._tol = 1e-6          # src/driver.jl:126
+        if self.adaptive:
+            sim._h.call("mm_set_adaptive_method", _lib.RK_METHODS[name])
+
+    def run_fixed(self, nsteps, dt=None):
+        """nsteps of the fixed-step scheme, one CUDA graph launch per step."""
+        self._sim._h.call(_FIXED[self.name][0], float(self._step if dt is None else dt), int(nsteps))
 
     @property
     def step(self):
-        if self.kind == "DormandPrince":
+        if self.adaptive:
             return self._sim._stats().get("step", 0.0)
         return self._step
 
@@ -183,7 +197,7 @@ class _Integrator:
 
     @property
     def t(self):
-        if self.kind == "RungeKutta":
+        if not self.adaptive:
             import ctypes
 
             t = ctypes.c_double()
@@ -193,7 +207,7 @@ class _Integrator:
 
     @property
     def nsteps(self):
-        if self.kind == "RungeKutta":
+        if not self.adaptive:
             import ctypes
 
             n = ctypes.c_int64()
@@ -219,9 +233,6 @@ class _Driver:
     precession = property(lambda s: s._precession, lambda s, v: (setattr(s, "_precession", bool(v)), s._push()))
 
 
-_INTEGRATORS = {"RungeKutta": "RungeKutta", "DormandPrince": "DormandPrince", "DOPRI54": "DormandPrince"}
-
-
 class Sim:
     """Sim(mesh; driver="LLG", name="dyn", integrator="DormandPrince", save_data=true)
     src/sim.jl:48-107 for an FDMesh; the state lives on `device`."""
@@ -232,7 +243,7 @@ class Sim:
             raise NotImplementedError(f"driver {driver!r} is outside the accelerated path (LLG, SD)")
         if driver == "LLG" and integrator not in _INTEGRATORS:
             raise NotImplementedError(
-                f"integrator {integrator!r} is outside the accelerated path (RungeKutta, DormandPrince)")
+                f"integrator {integrator!r} is outside the accelerated path ({', '.join(sorted(_INTEGRATORS))})")
         self.mesh = mesh
         self.name = name
         self.n_total = mesh.n_total
@@ -241,7 +252,7 @@ class Sim:
         self.precision = _precision[0]
         self._h = Handle(mesh.nx, mesh.ny, mesh.nz, mesh.dx, mesh.dy, mesh.dz, mesh.pbc_bits, _form(), device)
         self.driver_name = driver
-        self.driver = _Driver(self, driver, _INTEGRATORS.get(integrator, "DormandPrince"))
+        self.driver = _Driver(self, driver, integrator)
         self.driver._push()
         self.interactions: list[Term] = []
         self._Ms = np.zeros(self.n_total)
@@ -439,8 +450,8 @@ def advance_step(sim: Sim):
     integ = sim.driver.integrator
     if integ is None:
         raise ValueError("advance_step needs the LLG driver")
-    if integ.kind == "RungeKutta":
-        sim._h.call("mm_rk4_run", float(integ._step), 1)
+    if not integ.adaptive:
+        integ.run_fixed(1)
         return True
     st = _lib.Stats()
     import ctypes
@@ -469,14 +480,15 @@ def run_step(sim: Sim, driver=None):
 def run_rk4(sim: Sim, nsteps: int, dt: float | None = None):
     """nsteps fixed RK4 steps (RungeKutta advance_step repeated, one graph launch each)."""
     integ = sim.driver.integrator
-    h = float(integ._step if dt is None else dt)
-    sim._h.call("mm_rk4_run", h, int(nsteps))
+    if integ is None or integ.adaptive:
+        raise ValueError("run_rk4 needs a fixed-step integrator (RungeKutta or Heun)")
+    integ.run_fixed(nsteps, dt)
 
 
 def run_until(sim: Sim, t_end: float, save_data=True):
     """run_until(sim, t_end; save_data)  src/sim.jl:547-579."""
     integ = sim.driver.integrator
-    if integ is None or integ.kind != "DormandPrince":
+    if integ is None or not integ.adaptive:
         raise ValueError("run_until needs an adaptive integrator (integrate_to_time is defined for AdaptiveRK only)")
     st = _lib.Stats()
     import ctypes
@@ -524,9 +536,11 @@ def set_driver(sim: Sim, driver="LLG", integrator="DormandPrince", **args):
     """set_driver(sim; driver, integrator, args...)  src/sim.jl:586-626 (alpha, gamma, precession)."""
     if driver not in ("LLG", "SD"):
         raise NotImplementedError(f"driver {driver!r} is outside the accelerated path")
-    if driver != sim.driver_name or (sim.driver.integrator and _INTEGRATORS.get(integrator) != sim.driver.integrator.kind):
+    if driver == "LLG" and integrator not in _INTEGRATORS:
+        raise NotImplementedError(f"integrator {integrator!r} is outside the accelerated path")
+    if driver != sim.driver_name or (sim.driver.integrator and integrator != sim.driver.integrator.name):
         old = sim.driver
-        sim.driver = _Driver(sim, driver, _INTEGRATORS.get(integrator, "DormandPrince"))
+        sim.driver = _Driver(sim, driver, integrator)
         sim.driver._alpha, sim.driver._gamma, sim.driver._precession = old._alpha, old._gamma, old._precession
         sim.driver_name = driver
         sim._h.call("mm_dopri_reset")

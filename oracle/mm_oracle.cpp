@@ -286,6 +286,7 @@ struct Sim {
   double facmax = 5.0, facmin = 0.2, safety = 0.824;
   int64_t nsteps = 0, nfevals = 0;
   bool succeed = false;
+  int method = 0;  // 0 DOPRI54, 1 BS23, 2 CashKarp54, 3 Fehlberg54
   std::vector<double> y_current, y_next, y_temp;
   std::vector<double> ks[7];
   // SD driver (src/sd.jl; src/driver.jl:95-102)
@@ -628,6 +629,23 @@ void rk4_step(Sim& s, double h) {
   s.rk_t = s.rk_nsteps * h;
 }
 
+// advance_step(sim, ::ModifiedEuler)  src/integrator/heun.jl:28-49
+// (vector_add2 / vector_add3 of src/util.jl)
+void heun_step(Sim& s, double h) {
+  const int64_t n3 = 3 * s.mesh.n;
+  std::vector<double>& k1 = s.ks[0];
+  std::vector<double>& k2 = s.ks[1];
+  std::vector<double>& y = s.prespin;
+  double* m = s.m.data();
+  llg_rhs(s, k1.data(), m);
+  for (int64_t i = 0; i < n3; ++i) y[i] = m[i] + h * k1[i];
+  llg_rhs(s, k2.data(), y.data());
+  for (int64_t i = 0; i < n3; ++i) m[i] = m[i] + (0.5 * h) * k1[i] + (0.5 * h) * k2[i];
+  normalise(m, s.mesh.n);
+  s.rk_nsteps += 1;
+  s.rk_t = s.rk_nsteps * h;
+}
+
 // rk_step_dopri54!  src/integrator/adaptive_rk_steps.jl:49-... (vector_add2..6b
 // of src/util.jl:86-183; error norm with atol = rtol = tol)
 double dopri54_attempt(Sim& s, double step, double t) {
@@ -692,14 +710,122 @@ double dopri54_attempt(Sim& s, double step, double t) {
   return mx * step / s.tol;
 }
 
-// compute_initial_step  src/integrator/adaptive_rk.jl:151-165 (order_main = 5)
+// rk_step_bs23!  src/integrator/adaptive_rk_steps.jl:11-47 (FSAL: k1 = k4
+// after an accepted attempt)
+double bs23_attempt(Sim& s, double step, double t) {
+  const int64_t n3 = 3 * s.mesh.n;
+  double* y0 = s.y_current.data();
+  double* yn = s.y_next.data();
+  double* yt = s.y_temp.data();
+  double *k1 = s.ks[0].data(), *k2 = s.ks[1].data(), *k3 = s.ks[2].data(), *k4 = s.ks[3].data();
+  if (s.succeed && t >= s.t) {
+    for (int64_t i = 0; i < n3; ++i) k1[i] = k4[i];
+  } else {
+    llg_rhs(s, k1, y0);
+    s.nfevals += 1;
+  }
+  for (int64_t i = 0; i < n3; ++i) yt[i] = y0[i] + step * 0.5 * k1[i];
+  llg_rhs(s, k2, yt);
+  for (int64_t i = 0; i < n3; ++i) yt[i] = y0[i] + step * 0.75 * k2[i];
+  llg_rhs(s, k3, yt);
+  for (int64_t i = 0; i < n3; ++i) yn[i] = y0[i] + step * (2.0 / 9 * k1[i] + 1.0 / 3 * k2[i] + 4.0 / 9 * k3[i]);
+  normalise(yn, s.mesh.n);
+  llg_rhs(s, k4, yn);
+  s.nfevals += 3;
+  double mx = 0.0;
+  bool nan = false;
+  for (int64_t i = 0; i < n3; ++i) {
+    yt[i] = -(5.0 / 72) * k1[i] + (1.0 / 12) * k2[i] + (1.0 / 9) * k3[i] + (-1.0 / 8) * k4[i];
+    double v = std::fabs(yt[i] / (1 + std::fabs(yn[i])));
+    if (std::isnan(v)) nan = true;
+    if (v > mx) mx = v;
+  }
+  if (nan) return std::nan("");
+  return mx * step / s.tol;
+}
+
+// The six-stage 5(4) pairs: table IV (Cash-Karp) and table III (Fehlberg)
+// of src/integrator/adaptive_rk_steps.jl:110-229.  b2..b6 build the stage
+// inputs, c the solution, w the error (c2 = w2 = 0).
+struct SixStage {
+  double b[5][5];
+  double c[6];
+  double w[6];
+};
+const SixStage kCashKarp54 = {{{1.0 / 5},
+                               {3.0 / 40, 9.0 / 40},
+                               {3.0 / 10, -9.0 / 10, 6.0 / 5},
+                               {-11.0 / 54, 5.0 / 2, -70.0 / 27, 35.0 / 27},
+                               {1631.0 / 55296, 175.0 / 512, 575.0 / 13824, 44275.0 / 110592, 253.0 / 4096}},
+                              {37.0 / 378, 0, 250.0 / 621, 125.0 / 594, 0, 512.0 / 1771},
+                              {-277.0 / 64512, 0, 6925.0 / 370944, -6925.0 / 202752, -277.0 / 14336, 277.0 / 7084}};
+const SixStage kFehlberg54 = {{{1.0 / 4},
+                               {3.0 / 32, 9.0 / 32},
+                               {1932.0 / 2197, -7200.0 / 2197, 7296.0 / 2197},
+                               {439.0 / 216, -8.0, 3680.0 / 513, -845.0 / 4104},
+                               {-8.0 / 27, 2.0, -3544.0 / 2565, 1859.0 / 4104, -11.0 / 40}},
+                              {16.0 / 135, 0, 6656.0 / 12825, 28561.0 / 56430, -9.0 / 50, 2.0 / 55},
+                              {-1.0 / 360, 0, 128.0 / 4275, 2197.0 / 75240, -1.0 / 50, -2.0 / 55}};
+
+// rk_step_cashkarp54! / rk_step_fehlberg54!  src/integrator/adaptive_rk_steps.jl:110-229
+double six_stage_attempt(Sim& s, double step, const SixStage& tb) {
+  const int64_t n3 = 3 * s.mesh.n;
+  double* y0 = s.y_current.data();
+  double* yn = s.y_next.data();
+  double* k[6];
+  for (int j = 0; j < 6; ++j) k[j] = s.ks[j].data();
+  llg_rhs(s, k[0], y0);
+  for (int st = 1; st < 6; ++st) {
+    double cf[5];
+    for (int j = 0; j < st; ++j) cf[j] = tb.b[st - 1][j] * step;
+    for (int64_t i = 0; i < n3; ++i) {
+      double v = y0[i];
+      for (int j = 0; j < st; ++j) v += cf[j] * k[j][i];
+      yn[i] = v;
+    }
+    llg_rhs(s, k[st], yn);
+  }
+  double cs[6];
+  for (int j = 0; j < 6; ++j) cs[j] = tb.c[j] * step;
+  for (int64_t i = 0; i < n3; ++i)
+    yn[i] = y0[i] + cs[0] * k[0][i] + cs[2] * k[2][i] + cs[3] * k[3][i] + cs[4] * k[4][i] + cs[5] * k[5][i];
+  normalise(yn, s.mesh.n);
+  s.nfevals += 6;
+  double* yt = s.y_temp.data();
+  double mx = 0.0;
+  bool nan = false;
+  for (int64_t i = 0; i < n3; ++i) {
+    yt[i] = tb.w[0] * k[0][i] + tb.w[2] * k[2][i] + tb.w[3] * k[3][i] + tb.w[4] * k[4][i] + tb.w[5] * k[5][i];
+    double v = std::fabs(yt[i] / (1 + std::fabs(yn[i])));
+    if (std::isnan(v)) nan = true;
+    if (v > mx) mx = v;
+  }
+  if (nan) return std::nan("");
+  return mx * step / s.tol;
+}
+
+// method-specific step function  src/integrator/adaptive_rk.jl:67-89
+double rk_attempt(Sim& s, double step, double t) {
+  switch (s.method) {
+    case 1: return bs23_attempt(s, step, t);
+    case 2: return six_stage_attempt(s, step, kCashKarp54);
+    case 3: return six_stage_attempt(s, step, kFehlberg54);
+    default: return dopri54_attempt(s, step, t);
+  }
+}
+// (order_main, order_embedded) of DOPRI54, BS23, CashKarp54, Fehlberg54
+// (src/integrator/adaptive_rk.jl:248-266)
+int order_main(const Sim& s) { return s.method == 1 ? 3 : 5; }
+int order_embedded(const Sim& s) { return s.method == 1 ? 2 : 4; }
+
+// compute_initial_step  src/integrator/adaptive_rk.jl:151-165
 double compute_initial_step(Sim& s, double dt) {
   double abs_step = dt, abs_step_tmp = dt;
   s.step = 1e-15;
   llg_rhs(s, s.y_temp.data(), s.y_current.data());
   double mx = 0.0;
   for (double v : s.y_temp) mx = std::max(mx, std::fabs(v));
-  double r_step = mx / (s.safety * std::pow(s.tol, 1.0 / 5));
+  double r_step = mx / (s.safety * std::pow(s.tol, 1.0 / order_main(s)));
   s.nfevals += 1;
   if (abs_step * r_step > 0.001) abs_step_tmp = 0.001 / r_step;
   return std::min(abs_step, abs_step_tmp);
@@ -709,13 +835,13 @@ double compute_initial_step(Sim& s, double dt) {
 // returns 1 on success, 0 on failure (NaN or too many attempts)
 int dopri_advance(Sim& s, int64_t* attempts) {
   const int max_nsteps = 50;
-  const int order = 4;  // order_embedded of DOPRI54
+  const int order = order_embedded(s);
   double t = s.t;
   if (s.step_next <= 0) s.step_next = compute_initial_step(s, 1e-12);
   s.step = s.step_next;
   int nstep = 1;
   while (true) {
-    double err = dopri54_attempt(s, s.step, t);
+    double err = rk_attempt(s, s.step, t);
     if (attempts) *attempts += 1;
     if (std::isnan(err)) { s.step_next = 1e-14; return 0; }
     nstep += 1;
@@ -1018,6 +1144,23 @@ void orc_rk4(void* h, double dt, int64_t nsteps) {
 }
 
 double orc_rk4_time(void* h) { return static_cast<Sim*>(h)->rk_t; }
+
+void orc_heun(void* h, double dt, int64_t nsteps) {
+  Sim* s = static_cast<Sim*>(h);
+  for (int64_t i = 0; i < nsteps; ++i) heun_step(*s, dt);
+}
+
+// a new AdaptiveRK of the given method (Sim(mesh; integrator=...), src/driver.jl:102-140)
+void orc_set_method(void* h, int method) {
+  Sim* s = static_cast<Sim*>(h);
+  s->method = method;
+  s->t = 0.0;
+  s->step = 0.0;
+  s->step_next = 0.0;
+  s->nsteps = 0;
+  s->nfevals = 0;
+  s->succeed = false;
+}
 
 void orc_dopri_set(void* h, double tol) {
   Sim* s = static_cast<Sim*>(h);

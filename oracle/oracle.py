@@ -58,6 +58,8 @@ def lib():
         L.orc_energy.argtypes = [vp, _dp]
         L.orc_energy.restype = ctypes.c_double
         L.orc_rk4.argtypes = [vp, ctypes.c_double, ctypes.c_int64]
+        L.orc_heun.argtypes = [vp, ctypes.c_double, ctypes.c_int64]
+        L.orc_set_method.argtypes = [vp, ctypes.c_int]
         L.orc_rk4_time.argtypes = [vp]
         L.orc_rk4_time.restype = ctypes.c_double
         L.orc_dopri_set.argtypes = [vp, ctypes.c_double]
@@ -189,6 +191,13 @@ class OracleSim:
 
     def rk4(self, dt, nsteps):
         lib().orc_rk4(self.h, float(dt), int(nsteps))
+
+    def set_method(self, method):
+        """0 DormandPrince, 1 BS23, 2 CashKarp54, 3 Fehlberg54."""
+        lib().orc_set_method(self.h, int(method))
+
+    def heun(self, dt, nsteps):
+        lib().orc_heun(self.h, float(dt), int(nsteps))
 
     def rk4_time(self):
         return lib().orc_rk4_time(self.h)

@@ -135,6 +135,9 @@ class GpuSim:
     def rk4(self, dt, n):
         self.h.call("mm_rk4_run", dt, n)
 
+    def heun(self, dt, n):
+        self.h.call("mm_heun_run", dt, n)
+
     def m(self):
         return self.h.get_m()
 
@@ -145,3 +148,6 @@ class GpuSim:
 
     def set_tol(self, tol):
         self.h.call("mm_dopri_set_tol", tol)
+
+    def set_method(self, method):
+        self.h.call("mm_set_adaptive_method", method)

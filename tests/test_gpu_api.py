@@ -1,0 +1,73 @@
+"""The reference's own LLG tests (test/test_llg.jl) written against the Python
+mirror of its API, run on the GPU in both precisions as the reference's
+test_functions does (test/test_utils.jl:3-30)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def analytical(alpha, gamma, H0, t):
+    """test/test_llg.jl:13-21."""
+    p = gamma / (1 + alpha * alpha)
+    beta = p * H0 * t
+    return np.cos(beta) / np.cosh(alpha * beta), np.sin(beta) / np.cosh(alpha * beta), np.tanh(alpha * beta)
+
+
+@pytest.fixture(params=[np.float32, np.float64], ids=["Float32", "Float64"])
+def api(request):
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import mmcuda
+
+    mmcuda.set_precision(request.param)
+    yield mmcuda
+    mmcuda.set_precision(np.float64)
+
+
+@pytest.mark.parametrize("integrator", ["DormandPrince", "BS23", "CashKarp54", "Fehlberg54"])
+def test_llg(api, integrator):
+    """test_llg(integrator)  test/test_llg.jl:23-56."""
+    tol = 1e-7 if integrator == "BS23" else 1e-8
+    error = 2e-6 if integrator == "BS23" else 8e-7
+    mesh = api.FDMesh(nx=1, ny=1, dx=1e-9)
+    sim = api.Sim(mesh, name="spin", integrator=integrator, save_data=False)
+    api.set_Ms(sim, 8e5)
+    sim.driver.gamma = 2.21e5
+    sim.driver.alpha = 0.05
+    sim.driver.integrator.tol = tol
+    api.add_zeeman(sim, (0, 0, 1e5))
+    api.init_m0(sim, (1.0, 0, 0))
+    for i in range(1, 11):
+        api.run_until(sim, 1e-10 * i)
+    mx, my, mz = analytical(0.05, 2.21e5, 1e5, 1e-9)
+    m = sim.spin
+    assert abs(mx - m[0]) < error
+    assert abs(my - m[1]) < error
+    assert abs(mz - m[2]) < error
+    sim.close()
+
+
+@pytest.mark.parametrize("integrator", ["Heun", "RungeKutta"])
+def test_llg_fixed(api, integrator):
+    """test_llg_fixed(integrator)  test/test_llg.jl:58-90: 500 run_step calls of dt = 1e-13."""
+    mesh = api.FDMesh(nx=1, ny=1, dx=1e-9)
+    sim = api.Sim(mesh, name="spin", integrator=integrator, save_data=False)
+    api.set_Ms(sim, 8e5)
+    sim.driver.alpha = 0.05
+    sim.driver.gamma = 2.21e5
+    sim.driver.integrator.step = 1e-13
+    api.add_exch(sim, 1.3e-11)
+    api.add_zeeman(sim, (0, 0, 1e5))
+    api.init_m0(sim, (1.0, 0, 0))
+    for _ in range(500):
+        api.run_step(sim, sim.driver)
+    assert abs(sim.driver.integrator.t - 5e-11) < 1e-22
+    assert sim.driver.integrator.nsteps == 500
+    mx, my, mz = analytical(0.05, 2.21e5, 1e5, 5e-11)
+    m = sim.spin
+    assert abs(mx - m[0]) < 8e-6
+    assert abs(my - m[1]) < 8e-6
+    assert abs(mz - m[2]) < 8e-6
+    sim.close()

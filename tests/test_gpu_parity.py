@@ -168,6 +168,49 @@ def test_dopri_run_until_fp64():
         assert rel_maxnorm(g.m(), o.get_m()) <= 1e-11
 
 
+@pytest.mark.parametrize("method", [1, 2, 3])
+def test_adaptive_methods_run_until_fp64(method):
+    """run_until with BS23 (FSAL), CashKarp54, Fehlberg54
+    (src/integrator/adaptive_rk_steps.jl:11-229): same accepted steps,
+    function evaluations and state as the oracle."""
+    from oracle.oracle import demag_tensor
+
+    cfg = random_config(40 + method, 12, 10, 2, "")
+    T = demag_tensor(12, 10, 2, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, _ = build_oracle(cfg, tensor=T)
+    g = GpuSim(cfg, form=0, tensor=T)
+    o.set_method(method)
+    g.set_method(method)
+    o.set_tol(1e-6)
+    g.set_tol(1e-6)
+    for t in (2e-13, 5e-13):
+        ok, so = o.run_until(t)
+        rc, sg = g.run_until(t)
+        assert ok and rc == 0
+        assert sg["nsteps"] == so["nsteps"] and sg["nfevals"] == so["nfevals"]
+        assert abs(sg["t"] - so["t"]) <= 1e-15 * t
+        assert rel_maxnorm(g.m(), o.get_m()) <= 1e-11
+
+
+@pytest.mark.parametrize("mesh", [(20, 5, 3, ""), (16, 16, 1, "xy"), (9, 11, 4, "z")])
+def test_heun_steps_fp64(mesh):
+    """One and ten Heun steps (src/integrator/heun.jl:28-49) with all terms."""
+    nx, ny, nz, pbc = mesh
+    cfg = random_config(5, nx, ny, nz, pbc)
+    from oracle.oracle import demag_tensor
+
+    T = demag_tensor(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, _ = build_oracle(cfg, tensor=T)
+    g = GpuSim(cfg, form=0, tensor=T)
+    dt = 1e-14
+    o.heun(dt, 1)
+    g.heun(dt, 1)
+    assert rel_maxnorm(g.m(), o.get_m()) <= TOL64
+    o.heun(dt, 9)
+    g.heun(dt, 9)
+    assert rel_maxnorm(g.m(), o.get_m()) <= 1e-11
+
+
 def analytical(alpha, gamma, H0, t):
     p = gamma / (1 + alpha * alpha)
     beta = p * H0 * t
@@ -193,6 +236,30 @@ def test_macrospin_rk4_and_dopri(form):
     exp = analytical(0.05, 2.21e5, 1e5, 1e-9)
     m = g.m()
     assert all(abs(m[i] - exp[i]) < 8e-7 for i in range(3))
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_macrospin_heun_and_adaptive_methods(form):
+    """test/test_llg.jl:23-120 on the GPU for Heun (dt 1e-13, 500 steps,
+    |err| < 8e-6) and BS23 / CashKarp54 / Fehlberg54 (run_until 0.1..1 ns)."""
+    cfg = dict(nx=1, ny=1, nz=1, dx=1e-9, dy=1e-9, dz=1e-9, pbc="", Ms=np.array([8e5]), m=np.array([1.0, 0, 0]),
+               terms=["exch", "zeeman"], A=1.3e-11, H=np.array([0, 0, 1e5]), alpha=0.05, gamma=2.21e5)
+    g = GpuSim(cfg, form=form)
+    g.heun(1e-13, 500)
+    exp = analytical(0.05, 2.21e5, 1e5, 5e-11)
+    m = g.m()
+    assert all(abs(m[i] - exp[i]) < 8e-6 for i in range(3))
+    cfg["terms"] = ["zeeman"]
+    exp = analytical(0.05, 2.21e5, 1e5, 1e-9)
+    for method, tol, err in ((1, 1e-7, 2e-6), (2, 1e-8, 8e-7), (3, 1e-8, 8e-7)):
+        g = GpuSim(cfg, form=form)
+        g.set_method(method)
+        g.set_tol(tol)
+        for i in range(1, 11):
+            rc, _ = g.run_until(1e-10 * i)
+            assert rc == 0
+        m = g.m()
+        assert all(abs(m[i] - exp[i]) < err for i in range(3)), (method, m, exp)
 
 
 def test_energies_fp64():

@@ -238,6 +238,40 @@ def test_llg_dopri_macrospin():
     assert all(abs(m[i] - exp[i]) < 8e-7 for i in range(3))
 
 
+@pytest.mark.parametrize("method,tol,err", [(1, 1e-7, 2e-6), (2, 1e-8, 8e-7), (3, 1e-8, 8e-7)])
+def test_llg_adaptive_methods_macrospin(method, tol, err):
+    """test/test_llg.jl:23-56 with BS23 (tol 1e-7, |err| < 2e-6), CashKarp54 and
+    Fehlberg54 (tol 1e-8, |err| < 8e-7)."""
+    s = OracleSim(1, 1, 1, 1e-9, 1e-9, 1e-9)
+    s.set_Ms(8e5)
+    s.set_llg(0.05, 2.21e5)
+    s.set_method(method)
+    s.set_tol(tol)
+    s.add_zeeman([0, 0, 1e5])
+    s.set_m([1.0, 0, 0])
+    for i in range(1, 11):
+        ok, st = s.run_until(1e-10 * i)
+        assert ok
+    m = s.get_m()
+    exp = analytical(0.05, 2.21e5, 1e5, 1e-9)
+    assert all(abs(m[i] - exp[i]) < err for i in range(3))
+
+
+def test_llg_heun_macrospin():
+    """test/test_llg.jl:58-90 with integrator="Heun": dt=1e-13, 500 steps, |err| < 8e-6."""
+    s = OracleSim(1, 1, 1, 1e-9, 1e-9, 1e-9)
+    s.set_Ms(8e5)
+    s.set_llg(0.05, 2.21e5)
+    s.add_exch(Ax=1.3e-11, Ay=1.3e-11, Az=1.3e-11)
+    s.add_zeeman([0, 0, 1e5])
+    s.set_m([1.0, 0, 0])
+    s.heun(1e-13, 500)
+    assert abs(s.rk4_time() - 5e-11) < 1e-24
+    m = s.get_m()
+    exp = analytical(0.05, 2.21e5, 1e5, 5e-11)
+    assert all(abs(m[i] - exp[i]) < 8e-6 for i in range(3))
+
+
 def _dw_sim():
     """test/test_relax.jl:8-31: 500x1x11 domain wall, exch + anis along x."""
     nx, ny, nz = 500, 1, 11

@@ -164,6 +164,24 @@ typedef enum {
  * resets the adaptive state as a new Sim would (default MM_RK_DORMAND_PRINCE). */
 int mm_set_adaptive_method(mm_handle* h, int method);
 
+/* ---- OOMMF OVF 2.0 files (src/ovf2.jl) ----------------------------------
+ * Data blocks in the AoS cell order of mm_set_m / mm_get_m.  A path without
+ * the ".ovf" suffix gets it appended, as save_ovf / read_ovf do.  The mm_ovf_*
+ * functions are host-only (no device needed). */
+typedef enum { MM_OVF_TEXT = 0, MM_OVF_BINARY4 = 4, MM_OVF_BINARY8 = 8 } mm_ovf_type;
+/* save_ovf(ovf::OVF2, fname; type)  src/ovf2.jl:70-153 (mag2ovf :293-343) */
+int mm_ovf_write(const char* path, const mm_mesh_desc* mesh, const double* m_aos, int type, const char* title);
+/* header fields of read_ovf(fname)  src/ovf2.jl:246-291 (pbc = 0); the
+ * Title into title[title_cap] (truncated, NUL-terminated) when title != NULL */
+int mm_ovf_read_header(const char* path, mm_mesh_desc* mesh, int* type, char* title, size_t title_cap);
+/* data of read_ovf(fname) as float64; ncells must equal xnodes*ynodes*znodes */
+int mm_ovf_read(const char* path, double* m_aos, int64_t ncells);
+/* save_ovf(sim, fname; type)  src/ovf2.jl:44-62: the handle's m */
+int mm_save_ovf(mm_handle* h, const char* path, int type, const char* title);
+/* read_ovf(sim, fname)  src/ovf2.jl:197-208: m of the handle from a file
+ * whose cell count matches (MM_ERR_ARG "The ovf does not match the sim.mesh") */
+int mm_load_ovf(mm_handle* h, const char* path);
+
 /* relax(sim; max_steps, stopping_dmdt)  src/sim.jl:392-490 with the SD
  * driver (src/sd.jl:9-98) or the LLG driver with Dormand-Prince */
 int mm_relax(mm_handle* h, int driver, int64_t max_steps, double stopping_dmdt, int64_t* steps_done,

@@ -965,6 +965,7 @@ class Engine : public EngineBase {
 
 struct mm_handle {
   std::unique_ptr<mm::EngineBase> eng;
+  mm_mesh_desc mesh{};
 };
 
 // A set of handles on one device stepped together: one RK4 step of every
@@ -1042,6 +1043,7 @@ int mm_create(const mm_mesh_desc* d, int form, int device, mm_handle** out) {
       h->eng = std::move(e);
     }
     if (rc) return rc;
+    h->mesh = *d;
     *out = h.release();
     return MM_OK;
   } catch (...) {
@@ -1137,6 +1139,22 @@ int mm_run_until(mm_handle* h, double t, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h
 int mm_advance_step(mm_handle* h, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h->eng->advance_step(s)); }
 int mm_dopri_reset(mm_handle* h) { MM_HANDLE(h); MM_GUARD(h->eng->dopri_reset()); }
 int mm_set_adaptive_method(mm_handle* h, int method) { MM_HANDLE(h); MM_GUARD(h->eng->set_method(method)); }
+
+int mm_save_ovf(mm_handle* h, const char* path, int type, const char* title) {
+  MM_HANDLE(h);
+  const mm_mesh_desc& d = h->mesh;
+  std::vector<double> m(static_cast<size_t>(3) * d.nx * d.ny * d.nz);
+  if (int rc = h->eng->get_m(m.data())) return rc;
+  return mm_ovf_write(path, &d, m.data(), type, title);
+}
+
+int mm_load_ovf(mm_handle* h, const char* path) {
+  MM_HANDLE(h);
+  const mm_mesh_desc& d = h->mesh;
+  std::vector<double> m(static_cast<size_t>(3) * d.nx * d.ny * d.nz);
+  if (int rc = mm_ovf_read(path, m.data(), static_cast<int64_t>(d.nx) * d.ny * d.nz)) return rc;
+  MM_GUARD(h->eng->set_m(m.data()));
+}
 int mm_relax(mm_handle* h, int driver, int64_t max_steps, double stop, int64_t* steps, double* mx) {
   MM_HANDLE(h);
   if (driver != MM_DRIVER_SD && driver != MM_DRIVER_LLG) return fail(MM_ERR_ARG, "driver must be SD or LLG");

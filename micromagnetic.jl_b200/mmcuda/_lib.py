@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmmcuda.so")
 
 MM_OK = 0
+MM_ERR_ARG, MM_ERR_CUDA, MM_ERR_NAN, MM_ERR_NOCONVERGE = -1, -2, -3, -4
 STATUS = {
     -1: "MM_ERR_ARG",
     -2: "MM_ERR_CUDA",
@@ -25,6 +26,7 @@ STATUS = {
 }
 MM_FP64, MM_FP32 = 0, 1
 MM_RK_DORMAND_PRINCE, MM_RK_BS23, MM_RK_CASH_KARP54, MM_RK_FEHLBERG54 = 0, 1, 2, 3
+MM_OVF_TEXT, MM_OVF_BINARY4, MM_OVF_BINARY8 = 0, 4, 8
 RK_METHODS = {"DormandPrince": 0, "DOPRI54": 0, "BS23": 1, "CashKarp54": 2, "Fehlberg54": 3, "RKF54": 3}
 TERM_ZEEMAN, TERM_EXCH, TERM_DMI_BULK, TERM_DMI_INTERFACIAL, TERM_ANIS, TERM_DEMAG = range(6)
 NTERMS = 6
@@ -39,7 +41,8 @@ EXPORTS = (
     "mm_llg_rhs", "mm_average_m", "mm_rk4_run", "mm_rk4_state", "mm_dopri_set_tol", "mm_run_until",
     "mm_advance_step", "mm_dopri_reset", "mm_relax", "mm_kernel_time", "mm_rk4_launches_per_step",
     "mm_energy_noalloc", "mm_batch_create", "mm_batch_rk4_run", "mm_batch_get_stream", "mm_batch_destroy",
-    "mm_heun_run", "mm_set_adaptive_method",
+    "mm_heun_run", "mm_set_adaptive_method", "mm_ovf_write", "mm_ovf_read_header", "mm_ovf_read",
+    "mm_save_ovf", "mm_load_ovf",
 )
 KERNELS = ("demag_fwd_x", "demag_fwd_y", "demag_conv", "demag_inv_y", "demag_inv_x", "rk4_stage", "rk4_step")
 
@@ -109,6 +112,12 @@ def load():
         "mm_rk4_state": ([_vp, _dp, ctypes.POINTER(i64)], i),
         "mm_heun_run": ([_vp, d, i64], i),
         "mm_set_adaptive_method": ([_vp, i], i),
+        "mm_ovf_write": ([ctypes.c_char_p, ctypes.POINTER(MeshDesc), _dp, i, ctypes.c_char_p], i),
+        "mm_ovf_read_header": ([ctypes.c_char_p, ctypes.POINTER(MeshDesc), ctypes.POINTER(i), ctypes.c_char_p,
+                                ctypes.c_size_t], i),
+        "mm_ovf_read": ([ctypes.c_char_p, _dp, i64], i),
+        "mm_save_ovf": ([_vp, ctypes.c_char_p, i, ctypes.c_char_p], i),
+        "mm_load_ovf": ([_vp, ctypes.c_char_p], i),
         "mm_dopri_set_tol": ([_vp, d], i),
         "mm_run_until": ([_vp, d, ctypes.POINTER(Stats)], i),
         "mm_advance_step": ([_vp, ctypes.POINTER(Stats)], i),

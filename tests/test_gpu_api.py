@@ -71,3 +71,23 @@ def test_llg_fixed(api, integrator):
     assert abs(my - m[1]) < 8e-6
     assert abs(mz - m[2]) < 8e-6
     sim.close()
+
+
+@pytest.mark.parametrize("ovf_type", ["Float64", "Float32", "String"])
+def test_ovf_sim(api, tmp_path, ovf_type):
+    """init_saving / test_sim_reading  test/test_ovf.jl:8-29 on a device Sim."""
+    m = np.array([0.6, 0.8, 0, 0.6, 0.8, 0])
+    mesh = api.FDMesh(nx=2, ny=1, nz=1, dx=1e-9, dy=1e-9, dz=1e-9)
+    sim = api.Sim(mesh, name="saving", save_data=False)
+    api.set_Ms(sim, 8.0e5)
+    api.init_m0(sim, m)
+    f = str(tmp_path / ovf_type)
+    api.save_ovf(sim, f, type=ovf_type)
+    sim2 = api.Sim(mesh, name="reading", save_data=False)
+    api.set_Ms(sim2, 8.0e5)
+    api.read_ovf(sim2, f)
+    assert np.allclose(sim2.spin, m, atol=1e-6)
+    ovf = api.read_ovf(f)
+    assert ovf.name == "saving" and len(ovf.data) == 6 and np.max(np.abs(ovf.data - m)) < 1e-6
+    sim.close()
+    sim2.close()

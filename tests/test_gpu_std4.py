@@ -1,0 +1,59 @@
+"""mumag standard problem 4 end to end on the GPU, written as the reference's
+tutorial (docs/tutorials/micromagnetics/std4.jl:19-61) against the Python
+mirror of its API: SD relax to the S state, then 1 ns of LLG switching with
+Dormand-Prince.  <m>(t) is compared with the CPU oracle's run of the same
+protocol and with OOMMF's curve shipped by the reference
+(tests/golden/make_std4.py makes both fixtures)."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+# the GPU runs the oracle's algorithm; the summation order differs, so an
+# accept/reject decision of the step controller near err = 1 may differ and
+# move <m> by O(tol) = 1e-6 per step; FP32 rounds the field to 1e-7
+TOL_ORACLE = {"Float64": 1e-5, "Float32": 1e-4}
+# the oracle's own run (std4_oracle.npz) is within 1.8e-5 of OOMMF's curve
+TOL_OOMMF = {"Float64": 5e-5, "Float32": 3e-4}
+
+
+@pytest.mark.parametrize("precision", ["Float64", "Float32"])
+def test_std4(precision):
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import mmcuda as mm
+
+    ref = np.load(os.path.join(GOLD, "std4_oracle.npz"))
+    oommf = np.load(os.path.join(GOLD, "std4_oommf.npz"))
+    mm.set_precision(np.float32 if precision == "Float32" else np.float64)
+    try:
+        mesh = mm.FDMesh(nx=200, ny=50, nz=1, dx=2.5e-9, dy=2.5e-9, dz=3e-9)
+        sim = mm.Sim(mesh, driver="SD", name="std4", save_data=False)
+        mm.set_Ms(sim, 8e5)
+        mm.add_exch(sim, 1.3e-11)
+        mm.add_demag(sim)
+        mm.init_m0(sim, (1, 0.25, 0.1))
+        mm.relax(sim, stopping_dmdt=0.01)
+        m_relaxed = mm.average_m(sim)
+        if precision == "Float64":
+            assert sim.relax_steps == int(ref["relax_steps"])
+        assert np.max(np.abs(m_relaxed - ref["m_relaxed_avg"])) < TOL_ORACLE[precision]
+        mm.set_driver(sim, driver="LLG", alpha=0.02, gamma=2.211e5)
+        mm.add_zeeman(sim, (-24.6 * mm.mT, 4.3 * mm.mT, 0))
+        ms = [m_relaxed]
+        for i in range(1, 101):
+            assert mm.run_until(sim, i * 1e-11, save_data=False)
+            ms.append(mm.average_m(sim))
+        ms = np.array(ms)
+        d_oracle = np.max(np.abs(ms - ref["m"]))
+        d_oommf = np.max(np.abs(ms[1:] - oommf["m"]))
+        print(f"std4 {precision}: max |<m> - oracle| = {d_oracle:.3e}, max |<m> - OOMMF| = {d_oommf:.3e}")
+        assert d_oracle < TOL_ORACLE[precision]
+        assert d_oommf < TOL_OOMMF[precision]
+        sim.close()
+    finally:
+        mm.set_precision(np.float64)

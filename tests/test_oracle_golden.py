@@ -295,3 +295,14 @@ def test_relax_domain_wall(driver):
     s.relax(driver, max_steps=2000, stopping_dmdt=0.1)
     m = s.get_m().reshape(-1, 3).mean(0)
     assert abs(m[0]) < 0.01 and abs(m[1]) < 0.04 and abs(m[2]) < 0.01
+
+
+def test_std4_oracle_fixture_matches_oommf():
+    """The oracle's run of mumag standard problem 4 (tests/golden/make_std4.py:
+    SD relax, then 1 ns of Dormand-Prince LLG) against OOMMF's <m>(t) shipped
+    with the reference (docs/src/micromagnetics/assets/std4_oommf.txt)."""
+    gold = os.path.join(os.path.dirname(__file__), "golden")
+    r = np.load(os.path.join(gold, "std4_oracle.npz"))
+    o = np.load(os.path.join(gold, "std4_oommf.npz"))
+    assert np.allclose(r["t"][1:], o["t"], rtol=1e-12, atol=0)
+    assert np.max(np.abs(r["m"][1:] - o["m"])) < 2e-5

@@ -164,6 +164,22 @@ typedef enum {
  * resets the adaptive state as a new Sim would (default MM_RK_DORMAND_PRINCE). */
 int mm_set_adaptive_method(mm_handle* h, int method);
 
+/* ---- Adjoint of fixed-step RK4 ------------------------------------------
+ * The reference has no differentiation of this path; these give reverse-mode
+ * gradients of a loss L(m_T) through nsteps RK4 steps of
+ * advance_step(sim, ::RungeKutta) (src/integrator/rk.jl:23-52) with the
+ * handle's terms (discrete adjoint: exact for the scheme up to rounding).
+ * mm_adjoint_record runs the steps from the current m (advancing it to m_T,
+ * like mm_rk4_run) and keeps (m) every ckpt_every steps on the device.
+ * mm_adjoint_backward takes dL/dm_T (AoS, 3N) and returns, for any non-NULL
+ * output: dL/dm0 (AoS, 3N), dL/dMs per cell (N, Ms in A/m), dL/dKu per cell
+ * (N, uniaxial anisotropy) and dL/dD per cell (N, interfacial DMI; for a
+ * uniform D the scalar gradient is the sum).  Segments of ckpt_every steps
+ * are recomputed forward (3N*ckpt_every state words kept); m is left at m_T.
+ * Changing parameters between the two calls is refused (MM_ERR_STATE). */
+int mm_adjoint_record(mm_handle* h, double dt, int64_t nsteps, int64_t ckpt_every);
+int mm_adjoint_backward(mm_handle* h, const double* dL_dmT, double* g_m0, double* g_Ms, double* g_Ku, double* g_D);
+
 /* ---- OOMMF OVF 2.0 files (src/ovf2.jl) ----------------------------------
  * Data blocks in the AoS cell order of mm_set_m / mm_get_m.  A path without
  * the ".ovf" suffix gets it appended, as save_ovf / read_ovf do.  The mm_ovf_*

@@ -90,6 +90,8 @@ class EngineBase {
   virtual int advance_step(mm_stats* st) = 0;
   virtual int dopri_reset() = 0;
   virtual int set_method(int method) = 0;
+  virtual int adjoint_record(double dt, int64_t nsteps, int64_t ckpt) = 0;
+  virtual int adjoint_backward(const double* dLdm, double* gm0, double* gMs, double* gKu, double* gD) = 0;
   virtual int relax(int driver, int64_t max_steps, double stop, int64_t* steps, double* max_dmdt) = 0;
   virtual int kernel_time(int kernel, int reps, double* ms, double* bytes) = 0;
   virtual int rk4_launches() const = 0;
@@ -917,6 +919,174 @@ class Engine : public EngineBase {
     return MM_OK;
   }
 
+  // ---------------------------------------------------------- adjoint --
+  // Reverse mode through nsteps fixed RK4 steps with checkpointing: the
+  // recorded run keeps (m, m_lo) every `ck` steps; the backward sweep
+  // recomputes one segment forward at a time (states of the segment kept),
+  // then walks it backwards, recomputing each step's stage inputs, demag
+  // fields and slopes before the stage VJPs.
+  int adjoint_record(double dt, int64_t n, int64_t ck) override {
+    if (int rc = need_ms()) return rc;
+    if (n < 1 || !(dt > 0) || ck < 1) return fail(MM_ERR_ARG, "adjoint: need dt > 0, nsteps >= 1, ckpt_every >= 1");
+    const int64_t nck = (n + ck - 1) / ck;
+    MM_CUDA(cudaStreamSynchronize(st_));
+    adj_release();
+    int rc;
+    if ((rc = alloc(adj_ck, nck * 3 * N)) || (kF32 && (rc = alloc(adj_ck_lo, nck * 3 * N)))) return rc;
+    adj_n = n;
+    adj_every = ck;
+    adj_nck = nck;
+    adj_dt = dt;
+    for (int64_t s = 0; s < n; ++s) {
+      if (s % ck == 0) {
+        const int64_t slot = s / ck;
+        MM_CUDA(cudaMemcpyAsync(adj_ck + slot * 3 * N, m, sizeof(R) * 3 * N, cudaMemcpyDeviceToDevice, st_));
+        if (kF32)
+          MM_CUDA(cudaMemcpyAsync(adj_ck_lo + slot * 3 * N, m_lo, sizeof(R) * 3 * N, cudaMemcpyDeviceToDevice, st_));
+      }
+      if ((rc = rk4_run(dt, 1))) return rc;
+    }
+    adj_version = version;
+    MM_CUDA(cudaStreamSynchronize(st_));
+    return MM_OK;
+  }
+
+  void adj_release() {
+    release(adj_ck, adj_nck * 3 * N);
+    release(adj_ck_lo, adj_nck * 3 * N);
+    adj_n = adj_nck = 0;
+  }
+
+  int adj_buffers() {
+    int rc;
+    const int64_t n3 = 3 * N;
+    if (adj_seg_cap < adj_every) {
+      release(adj_seg, adj_seg_cap * n3);
+      release(adj_seg_lo, adj_seg_cap * n3);
+      adj_seg_cap = 0;
+      if ((rc = alloc(adj_seg, adj_every * n3)) || (kF32 && (rc = alloc(adj_seg_lo, adj_every * n3)))) return rc;
+      adj_seg_cap = adj_every;
+    }
+    if (adj_lam) return MM_OK;
+    for (int i = 0; i < 4; ++i)
+      if ((rc = alloc(adj_Y[i], n3)) || (rc = alloc(adj_k[i], n3)) || (rc = alloc(adj_Hd[i], n3))) return rc;
+    if ((rc = alloc(adj_q, n3)) || (rc = alloc(adj_w, n3)) || (rc = alloc(adj_Hdw, n3)) || (rc = alloc(adj_a, n3)) ||
+        (rc = alloc(adj_mu, n3)) || (rc = alloc(adj_g, n3)) || (rc = alloc(adj_gMs, N)) || (rc = alloc(adj_gKu, N)) ||
+        (rc = alloc(adj_gD, N)) || (rc = alloc(adj_end, n3)) || (kF32 && (rc = alloc(adj_end_lo, n3))) ||
+        (rc = alloc(adj_lam, n3)))
+      return rc;
+    return MM_OK;
+  }
+
+  // the slopes k1..k4 of the RK4 step from y (+ y_lo), with their stage
+  // inputs and demag fields kept for the VJPs
+  void adj_recompute_stages(const R* y, const R* ylo, double h) {
+    static const double cin[4] = {0.0, 0.5, 0.5, 1.0};
+    for (int i = 0; i < 4; ++i) {
+      const R* Yi = y;
+      if (i > 0) {
+        launch_adj_stage_input<R>(y, ylo, adj_k[i - 1], cin[i] * h, adj_Y[i], 3 * N, st_);
+        Yi = adj_Y[i];
+      }
+      adj_Yp[i] = Yi;
+      FieldArgs<R> fa = fargs(~0u);
+      if ((mask & TB_DEMAG) && demag) {
+        demag->apply(Yi, Ms, adj_Hd[i], st_);
+        fa.Hd = adj_Hd[i];
+      }
+      StageArgs<R> sa{};
+      sa.out = adj_k[i];
+      launch_stage<R>(SM_RHS, fa, Yi, sa, st_);
+    }
+  }
+
+  // one step backwards: adj_lam holds dL/dy_{n+1} on entry, dL/dy_n on exit
+  void adj_step_back(const R* y, const R* ylo, double h) {
+    adj_recompute_stages(y, ylo, h);
+    const R* const ks[4] = {adj_k[0], adj_k[1], adj_k[2], adj_k[3]};
+    launch_adj_normalise<R>(y, ylo, ks, h, adj_lam, adj_mu, adj_g, N, st_);
+    const unsigned loc = TB_EXCH | TB_DMI_BULK | TB_DMI_INTERFACIAL | TB_ANIS;
+    const bool dem = (mask & TB_DEMAG) && demag;
+    const bool zee = (mask & TB_ZEEMAN) != 0;
+    AdjGrads gr{adj_gMs, (mask & TB_ANIS) ? adj_gKu : nullptr, (mask & TB_DMI_INTERFACIAL) ? adj_gD : nullptr};
+    static const double wt[4] = {1.0, 2.0, 2.0, 1.0};
+    static const double cin[4] = {0.0, 0.5, 0.5, 1.0};
+    for (int i = 3; i >= 0; --i) {
+      launch_adj_rhs<R>(fargs(loc), zee, adj_Yp[i], dem ? adj_Hd[i] : nullptr, adj_g, adj_q, adj_w, adj_a, gr, st_);
+      FieldArgs<R> fl = fargs(loc | TB_DEMAG);
+      if (dem) {
+        demag->apply(adj_w, Ms, adj_Hdw, st_);
+        fl.Hd = adj_Hdw;
+      }
+      const double cm = i > 0 ? wt[i - 1] * h / 6.0 : 0.0;
+      const double ca = i > 0 ? cin[i] * h : 0.0;
+      launch_adj_field<R>(fl, adj_w, adj_q, adj_Yp[i], adj_a, adj_lam, adj_mu, cm, ca, i > 0 ? adj_g : nullptr, gr,
+                          st_);
+    }
+  }
+
+  int adjoint_backward(const double* dLdm, double* gm0, double* gMs, double* gKu, double* gD) override {
+    if (!adj_n) return fail(MM_ERR_STATE, "mm_adjoint_record must run first");
+    if (adj_version != version) return fail(MM_ERR_STATE, "parameters changed since mm_adjoint_record");
+    if (!dLdm) return fail(MM_ERR_ARG, "null dL/dm");
+    int rc;
+    if ((rc = adj_buffers())) return rc;
+    const int64_t n3 = 3 * N;
+    // dL/dm_T (AoS) -> SoA FP64
+    int* flag = reinterpret_cast<int*>(scal + 63);
+    MM_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st_));
+    MM_CUDA(cudaMemcpyAsync(stage64, dLdm, sizeof(double) * n3, cudaMemcpyHostToDevice, st_));
+    launch_aos_to_soa<double>(stage64, adj_lam, nullptr, N, flag, st_);
+    MM_CUDA(cudaMemsetAsync(adj_gMs, 0, sizeof(double) * N, st_));
+    MM_CUDA(cudaMemsetAsync(adj_gKu, 0, sizeof(double) * N, st_));
+    MM_CUDA(cudaMemsetAsync(adj_gD, 0, sizeof(double) * N, st_));
+    // keep the final state; the segment recomputation steps m
+    MM_CUDA(cudaMemcpyAsync(adj_end, m, sizeof(R) * n3, cudaMemcpyDeviceToDevice, st_));
+    if (kF32) MM_CUDA(cudaMemcpyAsync(adj_end_lo, m_lo, sizeof(R) * n3, cudaMemcpyDeviceToDevice, st_));
+    const int64_t rk_n0 = rk_n;
+    const double rk_t0 = rk_t;
+    for (int64_t sg = adj_nck - 1; sg >= 0; --sg) {
+      const int64_t s0 = sg * adj_every, s1 = std::min(adj_n, s0 + adj_every);
+      MM_CUDA(cudaMemcpyAsync(m, adj_ck + sg * n3, sizeof(R) * n3, cudaMemcpyDeviceToDevice, st_));
+      if (kF32) MM_CUDA(cudaMemcpyAsync(m_lo, adj_ck_lo + sg * n3, sizeof(R) * n3, cudaMemcpyDeviceToDevice, st_));
+      for (int64_t s = s0; s < s1; ++s) {
+        MM_CUDA(cudaMemcpyAsync(adj_seg + (s - s0) * n3, m, sizeof(R) * n3, cudaMemcpyDeviceToDevice, st_));
+        if (kF32)
+          MM_CUDA(cudaMemcpyAsync(adj_seg_lo + (s - s0) * n3, m_lo, sizeof(R) * n3, cudaMemcpyDeviceToDevice, st_));
+        if (s + 1 < s1 && (rc = rk4_run(adj_dt, 1))) return rc;
+      }
+      for (int64_t s = s1 - 1; s >= s0; --s)
+        adj_step_back(adj_seg + (s - s0) * n3, kF32 ? adj_seg_lo + (s - s0) * n3 : nullptr, adj_dt);
+      MM_CUDA(cudaGetLastError());
+    }
+    rk_n = rk_n0;
+    rk_t = rk_t0;
+    MM_CUDA(cudaMemcpyAsync(m, adj_end, sizeof(R) * n3, cudaMemcpyDeviceToDevice, st_));
+    if (kF32) MM_CUDA(cudaMemcpyAsync(m_lo, adj_end_lo, sizeof(R) * n3, cudaMemcpyDeviceToDevice, st_));
+    int hflag = 0;
+    MM_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    if (gm0) {
+      launch_soa_to_aos<double>(adj_lam, nullptr, stage64, N, st_);
+      MM_CUDA(cudaMemcpyAsync(gm0, stage64, sizeof(double) * n3, cudaMemcpyDeviceToHost, st_));
+    }
+    if (gMs) MM_CUDA(cudaMemcpyAsync(gMs, adj_gMs, sizeof(double) * N, cudaMemcpyDeviceToHost, st_));
+    if (gKu) MM_CUDA(cudaMemcpyAsync(gKu, adj_gKu, sizeof(double) * N, cudaMemcpyDeviceToHost, st_));
+    if (gD) MM_CUDA(cudaMemcpyAsync(gD, adj_gD, sizeof(double) * N, cudaMemcpyDeviceToHost, st_));
+    MM_CUDA(cudaStreamSynchronize(st_));
+    if (hflag) return fail(MM_ERR_NAN, "NaN in dL/dm");
+    return MM_OK;
+  }
+
+  R *adj_ck = nullptr, *adj_ck_lo = nullptr, *adj_seg = nullptr, *adj_seg_lo = nullptr;
+  R *adj_Y[4] = {}, *adj_k[4] = {}, *adj_Hd[4] = {};
+  const R* adj_Yp[4] = {};
+  R *adj_q = nullptr, *adj_w = nullptr, *adj_Hdw = nullptr, *adj_end = nullptr, *adj_end_lo = nullptr;
+  double *adj_lam = nullptr, *adj_mu = nullptr, *adj_g = nullptr, *adj_a = nullptr;
+  double *adj_gMs = nullptr, *adj_gKu = nullptr, *adj_gD = nullptr;
+  int64_t adj_n = 0, adj_every = 0, adj_nck = 0, adj_seg_cap = 0;
+  double adj_dt = 0.0;
+  uint64_t adj_version = 0;
+
   // ------------------------------------------------------------ state --
   int nx = 1, ny = 1, nz = 1, pbc = 0;
   int64_t N = 1;
@@ -955,6 +1125,19 @@ class Engine : public EngineBase {
     bytes_ += b;
     p = static_cast<T*>(q);
     return MM_OK;
+  }
+  // free a buffer of alloc() (after the stream has drained)
+  template <typename T>
+  void release(T*& p, int64_t n) {
+    if (!p) return;
+    for (size_t i = 0; i < allocs_.size(); ++i)
+      if (allocs_[i] == static_cast<void*>(p)) {
+        allocs_.erase(allocs_.begin() + static_cast<std::ptrdiff_t>(i));
+        break;
+      }
+    cudaFree(p);
+    bytes_ -= sizeof(T) * static_cast<size_t>(n);
+    p = nullptr;
   }
   cudaStream_t st_ = nullptr;
   std::vector<void*> allocs_;
@@ -1139,6 +1322,15 @@ int mm_run_until(mm_handle* h, double t, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h
 int mm_advance_step(mm_handle* h, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h->eng->advance_step(s)); }
 int mm_dopri_reset(mm_handle* h) { MM_HANDLE(h); MM_GUARD(h->eng->dopri_reset()); }
 int mm_set_adaptive_method(mm_handle* h, int method) { MM_HANDLE(h); MM_GUARD(h->eng->set_method(method)); }
+
+int mm_adjoint_record(mm_handle* h, double dt, int64_t nsteps, int64_t ckpt_every) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->adjoint_record(dt, nsteps, ckpt_every));
+}
+int mm_adjoint_backward(mm_handle* h, const double* dL_dmT, double* g_m0, double* g_Ms, double* g_Ku, double* g_D) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->adjoint_backward(dL_dmT, g_m0, g_Ms, g_Ku, g_D));
+}
 
 int mm_save_ovf(mm_handle* h, const char* path, int type, const char* title) {
   MM_HANDLE(h);

@@ -700,13 +700,255 @@ void launch_average_m(const R* m, const R* m_lo, int64_t N, double* partials, do
   k_reduce_sum<<<1, 256, 0, st>>>(partials, nb, 3, out);
 }
 
+// ------------------------------------------------------------- adjoint ---
+// Reverse mode through one RK4 step.  The forward step is
+//   Y1 = y, Yi = y + c_i h k_{i-1} (c = 1/2, 1/2, 1), k_i = f(Y_i),
+//   z = y + h/6 (k1 + 2k2 + 2k3 + k4), y' = z / |z|,
+// with f the LLG right-hand side of the effective field.  Every field term
+// of the path is H_i = (1/mu0Ms_i) sum_j K_ij m_j + Zeeman with a symmetric
+// K (it is minus the gradient of a quadratic energy: exchange, both DMIs,
+// anisotropy, and demag = N * (Ms m) with a symmetric Newell tensor), so the
+// transpose of dH/dm applied to q is mu0Ms * H_lin(q / mu0Ms): the same
+// kernels (stencil and demag passes) evaluated on w = q / mu0Ms.
+
+template <typename R>
+__global__ void k_adj_stage_input(const R* __restrict__ y, const R* __restrict__ y_lo, const R* __restrict__ k,
+                                  R coef, R* __restrict__ out, int64_t n3) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n3;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (y_lo) out[i] = y[i] + (y_lo[i] + coef * k[i]);
+    else out[i] = y[i] + coef * k[i];
+  }
+}
+
+template <typename R>
+void launch_adj_stage_input(const R* y, const R* y_lo, const R* k, double coef, R* out, int64_t n3, cudaStream_t st) {
+  k_adj_stage_input<R><<<1184, 256, 0, st>>>(y, y_lo, k, static_cast<R>(coef), out, n3);
+}
+
+template <typename R>
+__global__ void k_adj_normalise(const R* __restrict__ y, const R* __restrict__ y_lo, const R* __restrict__ k1,
+                                const R* __restrict__ k2, const R* __restrict__ k3, const R* __restrict__ k4,
+                                double h6, double* __restrict__ lam, double* __restrict__ mu, double* __restrict__ g,
+                                int64_t N) {
+  const int64_t I = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (I >= N) return;
+  double z[3], l[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const int64_t p = c * N + I;
+    const double acc = ((double(k1[p]) + 2.0 * double(k2[p])) + 2.0 * double(k3[p])) + double(k4[p]);
+    z[c] = double(y[p]) + (y_lo ? double(y_lo[p]) : 0.0) + h6 * acc;
+    l[c] = lam[p];
+  }
+  const double n2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+  double u[3] = {0, 0, 0}, inv = 0.0;
+  if (n2 > 0) {
+    inv = 1.0 / sqrt(n2);
+    u[0] = z[0] * inv; u[1] = z[1] * inv; u[2] = z[2] * inv;
+  }
+  const double lu = l[0] * u[0] + l[1] * u[1] + l[2] * u[2];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double v = n2 > 0 ? (l[c] - lu * u[c]) * inv : 0.0;
+    lam[c * N + I] = v;
+    mu[c * N + I] = v;
+    g[c * N + I] = h6 * v;
+  }
+}
+
+template <typename R>
+void launch_adj_normalise(const R* y, const R* y_lo, const R* const k[4], double h, double* lam, double* mu,
+                          double* g, int64_t N, cudaStream_t st) {
+  k_adj_normalise<R><<<stage_blocks(N), kStageThreads, 0, st>>>(y, y_lo, k[0], k[1], k[2], k[3], h / 6.0, lam, mu,
+                                                                  g, N);
+}
+
+// VJP of f = C (m x p - alpha p), p = |m|^2 H - (m.H) m, C = c + c_lo, for
+// the upstream u:  v = C u, r = v x m - alpha v (no v x m without
+// precession), q = dL/dH = |m|^2 r - (r.m) m,
+// dL/dm = p x v + 2 (r.H) m - (r.m) H - (m.H) r.
+template <typename R>
+__global__ void __launch_bounds__(kStageThreads) k_adj_rhs(FieldArgs<R> a, int zeeman, const R* __restrict__ Y,
+                                                           const R* __restrict__ HdY, const double* __restrict__ g,
+                                                           R* __restrict__ q, R* __restrict__ w,
+                                                           double* __restrict__ aexp, AdjGrads gr) {
+  const int64_t N = a.N;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= a.nx || j >= a.ny) return;
+  const int I = (k * a.ny + j) * a.nx + i;
+  R mr[3], hl[3];
+  cell_heff<R, false>(a, Y, I, i, j, k, mr, hl, nullptr);  // local terms only
+  const double ms = double(a.Ms[I]);
+  const bool pinned = a.pins && a.pins[I];
+  if (ms == 0.0 || pinned) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      q[c * N + I] = R(0);
+      w[c * N + I] = R(0);
+      aexp[c * N + I] = 0.0;
+    }
+    return;
+  }
+  double m[3], h[3], hloc[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    m[c] = double(mr[c]);
+    hloc[c] = double(hl[c]);
+    h[c] = hloc[c];
+  }
+  if (HdY) {
+    h[0] += double(HdY[I]); h[1] += double(HdY[N + I]); h[2] += double(HdY[2 * N + I]);
+  }
+  if (zeeman) {
+    h[0] += double(a.hz_x); h[1] += double(a.hz_y); h[2] += double(a.hz_z);
+    if (a.Hz) {
+      h[0] += double(a.Hz[I]); h[1] += double(a.Hz[N + I]); h[2] += double(a.Hz[2 * N + I]);
+    }
+  }
+  const double C = double(a.llg_c) + double(a.llg_c_lo);
+  const double alpha = double(a.alpha);
+  const double v[3] = {C * g[I], C * g[N + I], C * g[2 * N + I]};
+  const double mm = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+  const double mh = m[0] * h[0] + m[1] * h[1] + m[2] * h[2];
+  const double p[3] = {mm * h[0] - mh * m[0], mm * h[1] - mh * m[1], mm * h[2] - mh * m[2]};
+  double r[3] = {-alpha * v[0], -alpha * v[1], -alpha * v[2]};
+  double ae[3] = {0, 0, 0};
+  if (a.precession) {
+    r[0] += v[1] * m[2] - v[2] * m[1];
+    r[1] += v[2] * m[0] - v[0] * m[2];
+    r[2] += v[0] * m[1] - v[1] * m[0];
+    ae[0] = p[1] * v[2] - p[2] * v[1];
+    ae[1] = p[2] * v[0] - p[0] * v[2];
+    ae[2] = p[0] * v[1] - p[1] * v[0];
+  }
+  const double rh = r[0] * h[0] + r[1] * h[1] + r[2] * h[2];
+  const double rm = r[0] * m[0] + r[1] * m[1] + r[2] * m[2];
+  double qq[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    ae[c] += 2.0 * rh * m[c] - rm * h[c] - mh * r[c];
+    qq[c] = mm * r[c] - rm * m[c];
+    q[c * N + I] = static_cast<R>(qq[c]);
+    w[c * N + I] = static_cast<R>(qq[c] / ms);
+    aexp[c * N + I] = ae[c];
+  }
+  // H_loc = G / mu0Ms: dH_loc/dMs = -H_loc / Ms (Ms in A/m = mu0Ms / mu0)
+  const double qh = qq[0] * hloc[0] + qq[1] * hloc[1] + qq[2] * hloc[2];
+  gr.Ms[I] += -kMu0 * qh / ms;
+  if (gr.Ku && (a.mask & TB_ANIS)) {
+    const double ux = double(a.ux), uy = double(a.uy), uz = double(a.uz);
+    const double sa = m[0] * ux + m[1] * uy + m[2] * uz;
+    gr.Ku[I] += 2.0 * sa * (qq[0] * ux + qq[1] * uy + qq[2] * uz) / ms;
+  }
+}
+
+template <typename R>
+void launch_adj_rhs(const FieldArgs<R>& fa_loc, bool zeeman, const R* Y, const R* HdY, const double* g, R* q, R* w,
+                    double* aexp, AdjGrads gr, cudaStream_t st) {
+  const StageGrid sg = stage_grid(fa_loc.nx, fa_loc.ny, fa_loc.nz);
+  k_adj_rhs<R><<<sg.grid, sg.block, 0, st>>>(fa_loc, zeeman ? 1 : 0, Y, HdY, g, q, w, aexp, gr);
+}
+
+// r_d x m for the interfacial DMI directions d = -x, +x, -y, +y
+// (r = +y, -y, -x, +x; the forward stencil of cell_heff)
+__device__ __forceinline__ void idmi_cross(int d, const double m[3], double out[3]) {
+  if (d == 0) { out[0] = m[2]; out[1] = 0.0; out[2] = -m[0]; }
+  else if (d == 1) { out[0] = -m[2]; out[1] = 0.0; out[2] = m[0]; }
+  else if (d == 2) { out[0] = 0.0; out[1] = m[2]; out[2] = -m[1]; }
+  else { out[0] = 0.0; out[1] = -m[2]; out[2] = m[1]; }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kStageThreads)
+    k_adj_field(FieldArgs<R> a, const R* __restrict__ w, const R* __restrict__ q, const R* __restrict__ Y,
+                const double* __restrict__ aexp, double* __restrict__ lam, const double* __restrict__ mu, double cm,
+                double ca, double* __restrict__ gnext, AdjGrads gr) {
+  const int64_t N = a.N;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= a.nx || j >= a.ny) return;
+  const int I = (k * a.ny + j) * a.nx + i;
+  R wr[3], hw[3];
+  cell_heff<R, false>(a, w, I, i, j, k, wr, hw, nullptr);  // linear local terms on w + demag(w)
+  const double ms = double(a.Ms[I]);
+  double av[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    av[c] = aexp[c * N + I] + ms * double(hw[c]);
+    lam[c * N + I] += av[c];
+    if (gnext) gnext[c * N + I] = cm * mu[c * N + I] + ca * av[c];
+  }
+  if (ms == 0.0) return;
+  const double y[3] = {double(Y[I]), double(Y[N + I]), double(Y[2 * N + I])};
+  if (a.mask & TB_DEMAG) {
+    // H_d = demag(Ms m): dL/dMs_j = m_j . demag(q)_j = mu0 m_j . demag(w)_j
+    const double hd[3] = {double(a.Hd[I]), double(a.Hd[N + I]), double(a.Hd[2 * N + I])};
+    gr.Ms[I] += kMu0 * (y[0] * hd[0] + y[1] * hd[1] + y[2] * hd[2]);
+  }
+  if (gr.D && (a.mask & TB_DMI_INTERFACIAL)) {
+    // pair (I, n) enters H at both cells with the coefficient
+    // hm(D_I, D_n) / d, hm(a, b) = 2ab / (a + b)
+    const int nx = a.nx, ny = a.ny;
+    const bool px = a.pbc & 1, py = a.pbc & 2;
+    const int nb[4] = {i > 0 ? I - 1 : (px ? I + nx - 1 : I), i < nx - 1 ? I + 1 : (px ? I - (nx - 1) : I),
+                       j > 0 ? I - nx : (py ? I + (ny - 1) * nx : I),
+                       j < ny - 1 ? I + nx : (py ? I - (ny - 1) * nx : I)};
+    const unsigned nbm = a.nbm[I];
+    const double dd[4] = {double(a.id_x), double(a.id_x), double(a.id_y), double(a.id_y)};
+    const double DI = a.D ? double(a.D[I]) : double(a.D_uni);
+    const double qI[3] = {double(q[I]), double(q[N + I]), double(q[2 * N + I])};
+    double acc = 0.0;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+      if (!((nbm >> d) & 1u)) continue;
+      const int n = nb[d];
+      double dc;  // d(coefficient)/dD_I
+      if (a.D) {
+        const double Dn = double(a.D[n]);
+        if (DI + Dn == 0.0) continue;
+        dc = 2.0 * Dn * Dn / ((DI + Dn) * (DI + Dn)) * dd[d];
+      } else {
+        dc = 0.5 * dd[d];
+      }
+      const double yn[3] = {double(Y[n]), double(Y[N + n]), double(Y[2 * N + n])};
+      const double qn[3] = {double(q[n]), double(q[N + n]), double(q[2 * N + n])};
+      double x1[3], x2[3];
+      idmi_cross(d, yn, x1);      // field at I from n
+      idmi_cross(d ^ 1, y, x2);   // field at n from I (opposite direction)
+      const double t1 = (qI[0] * x1[0] + qI[1] * x1[1] + qI[2] * x1[2]) / ms;
+      const double t2 = (qn[0] * x2[0] + qn[1] * x2[1] + qn[2] * x2[2]) / double(a.Ms[n]);
+      acc += dc * (t1 + t2);
+    }
+    gr.D[I] += acc;
+  }
+}
+
+template <typename R>
+void launch_adj_field(const FieldArgs<R>& fa_lin, const R* w, const R* q, const R* Y, const double* aexp,
+                      double* lam, const double* mu, double cm, double ca, double* gnext, AdjGrads gr,
+                      cudaStream_t st) {
+  const StageGrid sg = stage_grid(fa_lin.nx, fa_lin.ny, fa_lin.nz);
+  k_adj_field<R><<<sg.grid, sg.block, 0, st>>>(fa_lin, w, q, Y, aexp, lam, mu, cm, ca, gnext, gr);
+}
+
 #define MM_INST(R)                                                                                       \
   template void launch_stage<R>(int, const FieldArgs<R>&, const R*, const StageArgs<R>&, cudaStream_t); \
   template void launch_nbmask<R>(int, int, int, int, const R*, uint8_t*, cudaStream_t);                 \
   template void launch_aos_to_soa<R>(const double*, R*, R*, int64_t, int*, cudaStream_t);                     \
   template void launch_soa_to_aos<R>(const R*, const R*, double*, int64_t, cudaStream_t);               \
   template void launch_scalar_to_R<R>(const double*, R*, int64_t, double, cudaStream_t);                \
-  template void launch_average_m<R>(const R*, const R*, int64_t, double*, double*, cudaStream_t);
+  template void launch_average_m<R>(const R*, const R*, int64_t, double*, double*, cudaStream_t);      \
+  template void launch_adj_stage_input<R>(const R*, const R*, const R*, double, R*, int64_t, cudaStream_t); \
+  template void launch_adj_normalise<R>(const R*, const R*, const R* const[4], double, double*, double*,   \
+                                        double*, int64_t, cudaStream_t);                                   \
+  template void launch_adj_rhs<R>(const FieldArgs<R>&, bool, const R*, const R*, const double*, R*, R*,    \
+                                  double*, AdjGrads, cudaStream_t);                                        \
+  template void launch_adj_field<R>(const FieldArgs<R>&, const R*, const R*, const R*, const double*,      \
+                                    double*, const double*, double, double, double*, AdjGrads, cudaStream_t);
 MM_INST(float)
 MM_INST(double)
 

@@ -135,4 +135,42 @@ void launch_reduce_sum(const double* partials, int nblocks, int width, double* o
 template <typename R>
 void launch_average_m(const R* m, const R* m_lo, int64_t N, double* partials, double* out, cudaStream_t st);
 
+// ------------------------------------------------------------- adjoint ---
+// Discrete adjoint of one RK4 step (src/integrator/rk.jl:23-52 with the
+// field of src/micro/kernels.jl and the LLG right-hand side of
+// src/llg/llg.jl:6-40).  lam, mu, g and a are FP64 SoA arrays of 3N.
+struct AdjGrads {
+  double* Ms;   // dL/dMs (per A/m), N, accumulated
+  double* Ku;   // dL/dKu, N, accumulated (null: not wanted)
+  double* D;    // dL/dD of interfacial DMI, N, accumulated (null: not wanted)
+};
+
+// Y_next = y (+ y_lo) + coef * k, the RK4 stage input exactly as the forward
+// stage kernel forms it
+template <typename R>
+void launch_adj_stage_input(const R* y, const R* y_lo, const R* k, double coef, R* out, int64_t n3, cudaStream_t st);
+
+// Normalisation at the end of the step: z = y + h/6 (((k1 + 2k2) + 2k3) + k4),
+// m_{n+1} = z/|z|.  In: lam = dL/dm_{n+1}.  Out: mu = dL/dz (also in lam),
+// g = (h/6) mu, the upstream gradient of k4.
+template <typename R>
+void launch_adj_normalise(const R* y, const R* y_lo, const R* const k[4], double h, double* lam, double* mu,
+                          double* g, int64_t N, cudaStream_t st);
+
+// Stage VJP, part 1: with the field H(Y) (local terms of fa_loc, plus Hd and
+// Zeeman), dL/dH = q and the explicit dL/dY of the LLG right-hand side for
+// the upstream gradient g of k = f(Y).  Writes q, w = q / (mu0 Ms), aexp and
+// accumulates the Ms and Ku gradients of the local terms.
+template <typename R>
+void launch_adj_rhs(const FieldArgs<R>& fa_loc, bool zeeman, const R* Y, const R* HdY, const double* g, R* q, R* w,
+                    double* aexp, AdjGrads gr, cudaStream_t st);
+
+// Stage VJP, part 2: a = aexp + mu0 Ms * H_lin(w) (H_lin: the linear local
+// terms on w plus the demag field Hdw = demag(w)), lam += a, Ms gradient of
+// demag, interfacial-D gradient of the pairs; if gnext: gnext = cm*mu + ca*a.
+template <typename R>
+void launch_adj_field(const FieldArgs<R>& fa_lin, const R* w, const R* q, const R* Y, const double* aexp,
+                      double* lam, const double* mu, double cm, double ca, double* gnext, AdjGrads gr,
+                      cudaStream_t st);
+
 }  // namespace mm

@@ -42,7 +42,7 @@ EXPORTS = (
     "mm_advance_step", "mm_dopri_reset", "mm_relax", "mm_kernel_time", "mm_rk4_launches_per_step",
     "mm_energy_noalloc", "mm_batch_create", "mm_batch_rk4_run", "mm_batch_get_stream", "mm_batch_destroy",
     "mm_heun_run", "mm_set_adaptive_method", "mm_ovf_write", "mm_ovf_read_header", "mm_ovf_read",
-    "mm_save_ovf", "mm_load_ovf",
+    "mm_save_ovf", "mm_load_ovf", "mm_adjoint_record", "mm_adjoint_backward",
 )
 KERNELS = ("demag_fwd_x", "demag_fwd_y", "demag_conv", "demag_inv_y", "demag_inv_x", "rk4_stage", "rk4_step")
 
@@ -118,6 +118,8 @@ def load():
         "mm_ovf_read": ([ctypes.c_char_p, _dp, i64], i),
         "mm_save_ovf": ([_vp, ctypes.c_char_p, i, ctypes.c_char_p], i),
         "mm_load_ovf": ([_vp, ctypes.c_char_p], i),
+        "mm_adjoint_record": ([_vp, d, i64, i64], i),
+        "mm_adjoint_backward": ([_vp, _dp, _dp, _dp, _dp, _dp], i),
         "mm_dopri_set_tol": ([_vp, d], i),
         "mm_run_until": ([_vp, d, ctypes.POINTER(Stats)], i),
         "mm_advance_step": ([_vp, ctypes.POINTER(Stats)], i),

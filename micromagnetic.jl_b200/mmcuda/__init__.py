@@ -6,6 +6,7 @@ relax, ...) on top of libmmcuda.so's C ABI (include/mmcuda.h).
 """
 from ._lib import MMError, load as _load_library  # noqa: F401
 from .ovf import OVF2, mag2ovf, read_ovf, save_ovf  # noqa: F401
+from .adjoint import rk4_grad  # noqa: F401
 from .sim import (  # noqa: F401
     FDMesh,
     Sim,

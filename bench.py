@@ -61,6 +61,11 @@ BATCHES = {
     # 32 NEB images of one 128x128x1 film, m interpolated between two random states
     "c3neb": dict(kind="neb", count=32, seed=103, nx=128, ny=128),
 }
+# reverse-mode gradients through RK4: 128x128x4 cells at 2 nm, exchange +
+# interfacial DMI + anisotropy + demag, per-cell Ms ~ U[6,9]e5, random m0
+# (seed 104), 2000 RK4 steps of 5e-14 s with checkpoints every 100 steps
+ADJOINT = {"c4": dict(nx=128, ny=128, nz=4, dx=2e-9, A=1.3e-11, D=3e-3, Ku=4e5, alpha=0.1, gamma=2.211e5,
+                      dt=5e-14, nsteps=2000, ckpt=100, seed=104)}
 # the CPU baseline times a bounded block of the same physics
 CPU_SAMPLE = {"c2": (128, 128, 32), "c5": (256, 256, 16), "c1": (200, 50, 1), "fig9": (1000, 1000, 1),
               "fig9_4000": (1000, 1000, 1)}
@@ -236,6 +241,75 @@ def run_batch(args, rank, ws, device, dist):
         dist.destroy_process_group()
 
 
+def run_adjoint(args, rank, ws, device, dist):
+    """Gradient of L = sum |m_T - target|^2 through the workload's RK4 steps:
+    mm_adjoint_record (forward with checkpoints) + mm_adjoint_backward,
+    timed with CUDA events; value = cells x steps / (record + backward)."""
+    import torch
+    from mmcuda import _lib
+
+    w = ADJOINT[args.workload]
+    n = w["nx"] * w["ny"] * w["nz"]
+    rng = np.random.default_rng(w["seed"])
+    m0 = rng.standard_normal((n, 3))
+    m0 /= np.linalg.norm(m0, axis=1, keepdims=True)
+    target = rng.standard_normal((n, 3))
+    target /= np.linalg.norm(target, axis=1, keepdims=True)
+    Ms = rng.uniform(6e5, 9e5, n)
+    out = {}
+    for fname, form in (("fp32", _lib.MM_FP32), ("fp64", _lib.MM_FP64)):
+        if args.only and fname != args.only:
+            continue
+        h = _lib.Handle(w["nx"], w["ny"], w["nz"], w["dx"], w["dx"], w["dx"], 0, form, device)
+        h.call("mm_set_Ms", _lib.dptr(Ms), 0.0)
+        h.call("mm_set_llg", w["alpha"], w["gamma"], 1)
+        h.call("mm_add_exch", None, w["A"], w["A"], w["A"])
+        h.call("mm_add_dmi_interfacial", None, w["D"])
+        h.call("mm_add_anis", None, w["Ku"], 0.0, 0.0, 1.0)
+        h.call("mm_add_demag", 0, 0, 0)
+        stream = torch.cuda.ExternalStream(h.stream(), device=device)
+        gm0, gMs, gKu, gD = np.zeros(3 * n), np.zeros(n), np.zeros(n), np.zeros(n)
+        d = _lib.dptr
+        times = []
+        for rep in range(2):  # the first pass warms up (graphs, buffers)
+            h.set_m(m0.reshape(-1))
+            h.call("mm_synchronize")
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            h.call("mm_adjoint_record", w["dt"], w["nsteps"], w["ckpt"])
+            e1.record(stream)
+            mT = h.get_m()
+            gT = np.ascontiguousarray(2 * (mT - target.reshape(-1)))
+            e1b = torch.cuda.Event(enable_timing=True)
+            e1b.record(stream)
+            h.call("mm_adjoint_backward", d(gT), d(gm0), d(gMs), d(gKu), d(gD))
+            e2.record(stream)
+            e2.synchronize()
+            times.append((e0.elapsed_time(e1), e1b.elapsed_time(e2)))
+        t_rec, t_back = times[-1]
+        t = torch.tensor([t_rec + t_back], device=f"cuda:{device}")
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        out[fname] = {"value": ws * n * w["nsteps"] / (ms / 1e3), "ms_record": t_rec, "ms_backward": t_back,
+                      "backward_over_forward": t_back / t_rec, "dL_dD": float(gD.sum())}
+        h.close()
+        del stream
+    if rank == 0:
+        r = out.get("fp32") or out.get("fp64")
+        line = {"metric": "adjoint cell-steps/s (RK4 record + backward)", "value": r["value"],
+                "unit": "cell-steps/s", "n_gpus": ws, "steps": w["nsteps"], "warmup": 1,
+                "ms_per_step": (r["ms_record"] + r["ms_backward"]) / w["nsteps"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if "fp32" in out else "f64",
+                "data": "synthetic (seeded numpy PCG64)",
+                "config": {"workload": f"{args.workload}: {w['nx']}x{w['ny']}x{w['nz']} exch + interfacial DMI + anis "
+                                       f"+ demag, {w['nsteps']} RK4 steps, checkpoints every {w['ckpt']}"},
+                "forms": out}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def cpu_baseline(wname, steps=1):
     """FP64 oracle (CPU restatement of the reference path), all host threads,
     on a bounded block of the workload's physics."""
@@ -312,6 +386,10 @@ def run_reference(args):
             dist.destroy_process_group()
         return
     wname = args.workload
+    if wname not in WORKLOADS:
+        print(json.dumps({"impl": "reference", "unavailable": f"{wname}: the CPU port times single-mesh RK4 "
+                                                               "workloads only (c1, c2, c5, fig9)"}), flush=True)
+        return
     w = WORKLOADS[wname]
     vals = []
     for _ in range(max(1, args.warmup // 3)):
@@ -350,6 +428,8 @@ def run_native(args):
     wname = args.workload
     if wname in BATCHES:
         return run_batch(args, rank, ws, device, dist)
+    if wname in ADJOINT:
+        return run_adjoint(args, rank, ws, device, dist)
     w = WORKLOADS[wname]
     n = w["nx"] * w["ny"] * w["nz"]
     dt = w["dt"]
@@ -541,7 +621,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + sorted(BATCHES))
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(ADJOINT))
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", choices=["fp32", "fp64"], help="time one form only (profiling runs)")

@@ -82,6 +82,11 @@ function attach!(sim::MicroMagnetic.MicroSim; form::Symbol=:fp64, device::Intege
         check(ccall((:mm_set_llg, libmmcuda), Cint, (Ptr{Cvoid}, Float64, Float64, Cint),
                     h.ptr, drv.alpha, drv.gamma, drv.precession ? 1 : 0))
         if drv.integrator isa MicroMagnetic.AdaptiveRK
+            # method of Sim(mesh; integrator=...)  src/integrator/adaptive_rk.jl:248-266
+            meth = drv.integrator.method
+            code = meth isa MicroMagnetic.BS23Method ? 1 : meth isa MicroMagnetic.CashKarp54Method ? 2 :
+                   meth isa MicroMagnetic.Fehlberg54Method ? 3 : 0
+            check(ccall((:mm_set_adaptive_method, libmmcuda), Cint, (Ptr{Cvoid}, Cint), h.ptr, code))
             check(ccall((:mm_dopri_set_tol, libmmcuda), Cint, (Ptr{Cvoid}, Float64), h.ptr, drv.integrator.tol))
         end
     end
@@ -141,6 +146,26 @@ function advance_step(sim::MicroMagnetic.MicroSim, integ::MicroMagnetic.RungeKut
     integ.nsteps += 1
     integ.t = integ.nsteps * integ.step
     pull_spin!(sim, h)
+    return nothing
+end
+
+# advance_step(sim, ::ModifiedEuler)  src/integrator/heun.jl:28-49
+function advance_step(sim::MicroMagnetic.MicroSim, integ::MicroMagnetic.ModifiedEuler)
+    h = handle(sim)
+    h === nothing && return invoke(advance_step, Tuple{MicroMagnetic.AbstractSim,MicroMagnetic.ModifiedEuler}, sim, integ)
+    check(ccall((:mm_heun_run, libmmcuda), Cint, (Ptr{Cvoid}, Float64, Int64), h.ptr, integ.step, 1))
+    integ.nsteps += 1
+    integ.t = integ.nsteps * integ.step
+    pull_spin!(sim, h)
+    return nothing
+end
+
+# save_ovf(sim, fname; type) from the device state  src/ovf2.jl:44-62
+function save_ovf(sim::MicroMagnetic.MicroSim, fname::String; type::DataType=Float64)
+    h = handle(sim)
+    h === nothing && return MicroMagnetic.save_ovf(sim, fname; type=type)
+    code = type == Float32 ? 4 : type == String ? 0 : 8
+    check(ccall((:mm_save_ovf, libmmcuda), Cint, (Ptr{Cvoid}, Cstring, Cint, Cstring), h.ptr, fname, code, sim.name))
     return nothing
 end
 

@@ -552,8 +552,8 @@ def run_native(args):
                        "parallelism": f"replicas x{ws}", "l2": "working set > 126 MB L2 (inputs larger than L2)"},
             "e2e": r["e2e"],
             "gpu_launches": r["launches_per_step"] * args.steps,
-            "fp64": {"value": evals * results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
-                     "fp32_over_fp64": r["value"] / results["fp64"]["value"]},
+            "fp64": ({"value": evals * results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
+                      "fp32_over_fp64": r["value"] / results["fp64"]["value"]} if "fp64" in results else None),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "peak_kind": peak_kind,
                          "traffic": traffic},

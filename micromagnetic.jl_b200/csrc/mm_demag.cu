@@ -3,6 +3,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "mm_demag.cuh"
@@ -58,6 +59,10 @@ static int smem_budget_bytes() {
 
 
 // ============================================================== kernels ====
+template <typename R> struct Vec2;
+template <> struct Vec2<float> { using T = float2; };
+template <> struct Vec2<double> { using T = double2; };
+
 enum XMode { XM_MAGN = 0, XM_TENSOR = 1 };
 
 // Forward x pass: real rows (zero padded / mirrored to Px) -> half spectrum.
@@ -156,15 +161,31 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_inv_x(
   }
   __syncthreads();
   buf = line_fft_to_smem<true, NT>(SmemLines<C>{buf, LS}, buf2, buf, LS, nl, fnl, g.plx, twx, 2);
-  for (int e = threadIdx.x; e < nlh * Lc; e += NT) {
-    const int l = fdiv(e, g.fLc), t = e - l * Lc;
-    const int line = line0 + l;
-    const int c = fdiv(line, g.frows), row = line - c * rows;
-    const C z = buf[l * LS + t];
-    const int u = 2 * t;
-    R* out = H + c * N + static_cast<int64_t>(row) * nx;
-    if (u < nx) out[u] = z.x;
-    if (u + 1 < nx) out[u + 1] = z.y;
+  if (!(nx & 1) && N * 3 < (int64_t(1) << 31)) {
+    using V2 = typename Vec2<R>::T;
+    const int Ni = static_cast<int>(N);
+    for (int e = threadIdx.x; e < nlh * Lc; e += NT) {
+      const int l = fdiv(e, g.fLc), t = e - l * Lc;
+      const int line = line0 + l;
+      const int c = fdiv(line, g.frows), row = line - c * rows;
+      if (2 * t >= nx) continue;
+      const C z = buf[l * LS + t];
+      V2 o;
+      o.x = z.x;
+      o.y = z.y;
+      *reinterpret_cast<V2*>(H + c * Ni + row * nx + 2 * t) = o;
+    }
+  } else {
+    for (int e = threadIdx.x; e < nlh * Lc; e += NT) {
+      const int l = fdiv(e, g.fLc), t = e - l * Lc;
+      const int line = line0 + l;
+      const int c = fdiv(line, g.frows), row = line - c * rows;
+      const C z = buf[l * LS + t];
+      const int u = 2 * t;
+      R* out = H + c * N + static_cast<int64_t>(row) * nx;
+      if (u < nx) out[u] = z.x;
+      if (u + 1 < nx) out[u + 1] = z.y;
+    }
   }
 }
 
@@ -386,11 +407,12 @@ enum YLMode { YL_FWD = 0, YL_INV = 1, YL_CONV2D = 2 };
 //   YL_FWD:    X rows y < ny            -> Y rows 0..Py-1
 //   YL_INV:    Y rows 0..Py-1           -> X rows y < ny
 //   YL_CONV2D: X rows y < ny, forward y, tensor product (kz = 0), inverse y -> X
-template <typename R, int MODE, int NT>
+template <typename R, int MODE, int NT, bool I32>
 __global__ void __launch_bounds__(NT, 2) k_ylines(const cplx_t<R>* in, cplx_t<R>* out, const R* __restrict__ Nhat,
                                                   DemagGeom g, int lgW, int ncompc, FastDiv fnl,
                                                   const cplx_t<R>* __restrict__ twy, int half) {
   using C = cplx_t<R>;
+  using IX = std::conditional_t<I32, int, int64_t>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* a = reinterpret_cast<C*>(smem_raw);
   C* b = a + half;
@@ -400,10 +422,10 @@ __global__ void __launch_bounds__(NT, 2) k_ylines(const cplx_t<R>* in, cplx_t<R>
   const int kx0 = blockIdx.x * W, z = blockIdx.y, c0 = blockIdx.z * ncompc;
   const int nlines = ncompc * W;
   const int rin = MODE == YL_INV ? Py : ny, rout = MODE == YL_FWD ? Py : ny;
-  RowsIn<C> src{in + static_cast<int64_t>(c0 * nz + z) * rin * Hx, static_cast<int64_t>(nz) * rin * Hx, Hx, lgW, kx0,
-                Hx, rin};
-  RowsOut<C> dst{out + static_cast<int64_t>(c0 * nz + z) * rout * Hx, static_cast<int64_t>(nz) * rout * Hx, Hx, lgW,
-                 kx0, Hx, rout};
+  RowsIn<C, IX> src{in + static_cast<int64_t>(c0 * nz + z) * rin * Hx, static_cast<IX>(static_cast<int64_t>(nz) * rin * Hx),
+                    static_cast<IX>(Hx), lgW, kx0, Hx, rin};
+  RowsOut<C, IX> dst{out + static_cast<int64_t>(c0 * nz + z) * rout * Hx,
+                     static_cast<IX>(static_cast<int64_t>(nz) * rout * Hx), static_cast<IX>(Hx), lgW, kx0, Hx, rout};
   if (MODE == YL_CONV2D) {
     C* res = line_fft_to_smem<false, NT>(src, a, b, LS, nlines, fnl, g.ply, twy, 1);
     tensor_product<R, true, NT>(res, LS, lgW, Py, g.fPy, kx0, 0, Nhat, Hx, Py, g.Pz);
@@ -416,10 +438,11 @@ __global__ void __launch_bounds__(NT, 2) k_ylines(const cplx_t<R>* in, cplx_t<R>
 // z lines (forward z, tensor product, inverse z, in place on Y) of one ky row
 // over a W-wide kx tile.  grid: (tiles, Py); consecutive blockIdx.y take ky
 // and Py - ky so the two reads of each tensor entry are close in time (L2).
-template <typename R, int NT>
+template <typename R, int NT, bool I32>
 __global__ void __launch_bounds__(NT, 2) k_zconv(cplx_t<R>* Y, const R* __restrict__ Nhat, DemagGeom g, int lgW,
                                                  FastDiv fnl, const cplx_t<R>* __restrict__ twz, int half) {
   using C = cplx_t<R>;
+  using IX = std::conditional_t<I32, int, int64_t>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* a = reinterpret_cast<C*>(smem_raw);
   C* b = a + half;
@@ -431,9 +454,9 @@ __global__ void __launch_bounds__(NT, 2) k_zconv(cplx_t<R>* Y, const R* __restri
   const int q = (bq + 1) >> 1;
   const int ky = bq == 0 ? 0 : ((bq & 1) ? q : Py - q);
   const int nlines = 3 * W;
-  const int64_t cs = static_cast<int64_t>(nz) * Py * Hx, rs = static_cast<int64_t>(Py) * Hx;
-  RowsIn<C> src{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
-  RowsOut<C> dst{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
+  const IX cs = static_cast<IX>(static_cast<int64_t>(nz) * Py * Hx), rs = static_cast<IX>(static_cast<int64_t>(Py) * Hx);
+  RowsIn<C, IX> src{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
+  RowsOut<C, IX> dst{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
   C* res = line_fft_to_smem<false, NT>(src, a, b, LS, nlines, fnl, g.plz, twz, 1);
   tensor_product<R, false, NT>(res, LS, lgW, Pz, g.fPz, kx0, ky, Nhat, Hx, Py, Pz);
   line_fft_from_smem<true, NT>(res, res == a ? b : a, dst, LS, nlines, fnl, g.plz, twz, 1);
@@ -446,10 +469,11 @@ __global__ void __launch_bounds__(NT, 2) k_zconv(cplx_t<R>* Y, const R* __restri
 // inputs are the same positions), written back in place after a barrier;
 // finally the inverse radix-RA stage straight to the Y rows kz < nz.
 // One shared buffer; requires W * RA <= NT (one middle task per thread).
-template <typename R, int RA, int RB, int NT>
+template <typename R, int RA, int RB, int NT, bool I32>
 __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_zconv2(cplx_t<R>* Y, const R* __restrict__ Nhat, DemagGeom g, int lgW,
                                                   FastDiv fnl, const cplx_t<R>* __restrict__ twz) {
   using C = cplx_t<R>;
+  using IX = std::conditional_t<I32, int, int64_t>;
   constexpr int L = RA * RB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* a = reinterpret_cast<C*>(smem_raw);
@@ -461,9 +485,9 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_zconv2(cplx_t<R>
   const int q = (bq + 1) >> 1;
   const int ky = bq == 0 ? 0 : ((bq & 1) ? q : Py - q);
   const int nlines = 3 * W;
-  const int64_t cs = static_cast<int64_t>(nz) * Py * Hx, rs = static_cast<int64_t>(Py) * Hx;
-  RowsIn<C> src{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
-  RowsOut<C> dst{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
+  const IX cs = static_cast<IX>(static_cast<int64_t>(nz) * Py * Hx), rs = static_cast<IX>(static_cast<int64_t>(Py) * Hx);
+  RowsIn<C, IX> src{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
+  RowsOut<C, IX> dst{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
   SmemLines<C> A{a, LS};
   lstage<RA, false, true, NT>(src, A, L, nlines, fnl, 1, twz, 1);
   // fused middle: thread -> (w, i), w fastest
@@ -650,10 +674,14 @@ static void set_smem_attrs_nt() {
   cudaFuncSetAttribute(k_ypass<R, YM_TENSOR_Q, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_zpass<R, ZM_CONV, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_zpass<R, ZM_TENSOR_Q, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_FWD, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_INV, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_zconv<R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_FWD, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_INV, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_zconv<R, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_FWD, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_INV, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_zconv<R, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
 
 template <typename R>
@@ -773,6 +801,12 @@ static void launch_zpass(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, double
   k_zpass<R, MODE, NT><<<grid, NT, sm, st>>>(Y, Nhat, Tq, g, ilog2(W), ncompc, twz, tsign, tscale, half);
 }
 
+// every element offset of the X and Y spectra (3 * nz * max(Py, ny) * Hx
+// complex words) fits in a signed 32-bit int
+static bool offsets_fit_int(const DemagGeom& g) {
+  return 3LL * g.nz * std::max(g.Py, g.ny) * g.Hx < (1LL << 31);
+}
+
 template <typename R>
 static int lines_tile(int Hx, int L, int lines_per_col, int nbuf) {
   using C = cplx_t<R>;
@@ -793,8 +827,12 @@ static void launch_ylines(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* ou
   const int half = ncompc * W * (g.Py | 1);
   dim3 grid((g.Hx + W - 1) / W, g.nz, 3 / ncompc);
   const size_t sm = static_cast<size_t>(std::max(1, nbuf)) * sizeof(C) * half;
-  k_ylines<R, MODE, kHotNT><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc,
-                                                      make_fastdiv(ncompc * W), twy, half);
+  if (offsets_fit_int(g))
+    k_ylines<R, MODE, kHotNT, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc,
+                                                              make_fastdiv(ncompc * W), twy, half);
+  else
+    k_ylines<R, MODE, kHotNT, false><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc,
+                                                               make_fastdiv(ncompc * W), twy, half);
 }
 
 template <typename R, int RA, int RB>
@@ -808,11 +846,15 @@ static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const
   int dev = 0;
   cudaGetDevice(&dev);
   if (!((done >> dev) & 1ull)) {
-    cudaFuncSetAttribute(k_zconv2<R, RA, RB, kHotNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_zconv2<R, RA, RB, kHotNT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_zconv2<R, RA, RB, kHotNT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     done |= 1ull << dev;
   }
   dim3 grid((g.Hx + W - 1) / W, g.Py, 1);
-  k_zconv2<R, RA, RB, kHotNT><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz);
+  if (offsets_fit_int(g))
+    k_zconv2<R, RA, RB, kHotNT, true><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz);
+  else
+    k_zconv2<R, RA, RB, kHotNT, false><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz);
 }
 
 // Power-of-two z lengths with a fused-middle kernel: L = RA * RB
@@ -843,7 +885,10 @@ static void launch_zconv(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const 
   const int half = 3 * W * (g.Pz | 1);
   dim3 grid((g.Hx + W - 1) / W, g.Py, 1);
   const size_t sm = 2 * sizeof(C) * half;
-  k_zconv<R, kHotNT><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz, half);
+  if (offsets_fit_int(g))
+    k_zconv<R, kHotNT, true><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz, half);
+  else
+    k_zconv<R, kHotNT, false><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz, half);
 }
 
 template <typename R>

@@ -27,30 +27,33 @@ struct SmemLines {
 };
 
 // rows of a spectrum array: element (line, pos) at
-// base[comp * comp_stride + pos * row_stride + kx0 + w], comp = line >> lgW
-template <typename C>
+// base[comp * comp_stride + pos * row_stride + kx0 + w], comp = line >> lgW.
+// IX is the offset type: int where every offset of the array fits in 31 bits
+// (the launchers check), which keeps the per-element address arithmetic in
+// 32-bit integer instructions.
+template <typename C, typename IX = int64_t>
 struct RowsIn {
   const C* base;
-  int64_t comp_stride, row_stride;
+  IX comp_stride, row_stride;
   int lgW, kx0, Hx, nrows;  // pos >= nrows reads as zero
   __device__ __forceinline__ C load(int line, int pos) const {
     const int w = line & ((1 << lgW) - 1), comp = line >> lgW;
     const int kx = kx0 + w;
     if (pos >= nrows || kx >= Hx) return cmk<C>(0, 0);
-    return base[comp * comp_stride + pos * row_stride + kx];
+    return base[static_cast<IX>(comp) * comp_stride + static_cast<IX>(pos) * row_stride + kx];
   }
 };
 
-template <typename C>
+template <typename C, typename IX = int64_t>
 struct RowsOut {
   C* base;
-  int64_t comp_stride, row_stride;
+  IX comp_stride, row_stride;
   int lgW, kx0, Hx, nrows;  // pos >= nrows is not written
   __device__ __forceinline__ void store(int line, int pos, C v) const {
     const int w = line & ((1 << lgW) - 1), comp = line >> lgW;
     const int kx = kx0 + w;
     if (pos >= nrows || kx >= Hx) return;
-    base[comp * comp_stride + pos * row_stride + kx] = v;
+    base[static_cast<IX>(comp) * comp_stride + static_cast<IX>(pos) * row_stride + kx] = v;
   }
 };
 

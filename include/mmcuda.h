@@ -56,7 +56,12 @@ enum mm_term {
   MM_TERM_DMI_INTERFACIAL = 3,
   MM_TERM_ANIS = 4,
   MM_TERM_DEMAG = 5,
-  MM_NTERMS = 6
+  MM_NTERMS = 6, /* terms with an energy; mm_energy reports these */
+  /* field-only terms (mm_term_field; no energy) */
+  MM_TERM_SOT = 6,
+  MM_TERM_STT_ZHANG_LI = 7,
+  MM_TERM_STT_SLONCZEWSKI = 8,
+  MM_TERM_THERMAL = 9
 };
 
 enum mm_driver { MM_DRIVER_SD = 0, MM_DRIVER_LLG = 1 };
@@ -163,6 +168,39 @@ typedef enum {
 /* Select the method used by mm_run_until / mm_advance_step / mm_relax(LLG);
  * resets the adaptive state as a new Sim would (default MM_RK_DORMAND_PRINCE). */
 int mm_set_adaptive_method(mm_handle* h, int method);
+
+/* ---- Further terms --------------------------------------------------------
+ * Evaluated in the same fused per-cell kernel (a variant compiled with them,
+ * so handles without them keep the base kernel).  Array arguments are per
+ * cell (N) or NULL for the uniform value; one term of each kind per handle. */
+/* add_dmi(sim, (Dx, Dy, Dz), type="bulk") with spatial D: per-axis arrays,
+ * harmonic mean per pair, pairs with a zero D dropped
+ * (SpatialVectorBulkDMI, src/micro/add_field.jl:299-326, kernels.jl:347-422);
+ * takes the place of mm_add_dmi_bulk */
+int mm_add_dmi_bulk_spatial(mm_handle* h, const double* Dx, const double* Dy, const double* Dz);
+/* add_sot(sim, aj, bj, p): field H = (aj/gamma) m x p + (bj/gamma) p
+ * (DFTorqueField, src/micro/add_field.jl:951-966, kernels.jl:619-632) */
+int mm_add_sot(mm_handle* h, const double* aj, double aj_uniform, double bj, double px, double py, double pz);
+/* add_stt(sim; model=:zhang_li): bJ = b * J per cell (AoS 3N, with the
+ * 1/(1+xi^2) factor already applied when b came from (P, Ms)), xi per cell,
+ * ft = the current-scale value (the reference's ft(t), taken constant);
+ * H = m x f + xi f, f = (ft/gamma) (bJ . nabla) m (src/micro/add_field.jl:1150-1190,
+ * kernels.jl:680-739) */
+int mm_add_stt_zhang_li(mm_handle* h, const double* bJ, const double* xi, double xi_uniform, double ft);
+/* add_stt(sim; model=:slonczewski): J per cell, ft_beta = ft * beta with
+ * beta = hbar / (mu0 Ms e tf), Lambda, P, xi, polarisation p
+ * (src/micro/add_field.jl:1192-1226, slonczewski_torque_kernel!) */
+int mm_add_stt_slonczewski(mm_handle* h, const double* J, double J_uniform, double ft_beta, double Lambda, double P,
+                           double xi, double px, double py, double pz);
+/* add_thermal_noise(sim, Temp; T0, scaling, k_B): H = eta sqrt(2 alpha k_B
+ * scaling (T + T0) / (V gamma dt mu0Ms)) with eta ~ N(0,1) redrawn once per
+ * step (src/micro/add_field.jl:734-760, field.jl:244-280, kernels.jl:469-494).
+ * eta of step n in cell i is a counter-based draw (Philox-4x32-10 on
+ * (i, n) keyed by seed, Box-Muller), so runs are reproducible; dt is used for
+ * evaluations outside a step (fixed steps use their own dt, the adaptive
+ * stepper its current step). */
+int mm_add_thermal_noise(mm_handle* h, const double* T, double T_uniform, double T0, double scaling, double k_B,
+                         uint64_t seed, double dt);
 
 /* ---- Adjoint of fixed-step RK4 ------------------------------------------
  * The reference has no differentiation of this path; these give reverse-mode

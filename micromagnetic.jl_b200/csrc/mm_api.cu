@@ -76,6 +76,13 @@ class EngineBase {
   virtual int add_dmi_bulk(double dx, double dy, double dz) = 0;
   virtual int add_dmi_interfacial(const double* D, double uni) = 0;
   virtual int add_anis(const double* Ku, double uni, double ax, double ay, double az) = 0;
+  virtual int add_dmi_bulk_spatial(const double* Dx, const double* Dy, const double* Dz) = 0;
+  virtual int add_sot(const double* aj, double aj_uni, double bj, double px, double py, double pz) = 0;
+  virtual int add_stt_zhang_li(const double* bJ, const double* xi, double xi_uni, double ft) = 0;
+  virtual int add_stt_slonczewski(const double* J, double J_uni, double ft_beta, double Lambda, double P, double xi,
+                                  double px, double py, double pz) = 0;
+  virtual int add_thermal_noise(const double* T, double T_uni, double T0, double scaling, double kB, uint64_t seed,
+                                double dt) = 0;
   virtual int add_demag(int Nx, int Ny, int Nz, const double* T6N_host) = 0;
   virtual int effective_field(double* H) = 0;
   virtual int term_field(int term, double* f, double* e) = 0;
@@ -275,6 +282,112 @@ class Engine : public EngineBase {
     return MM_OK;
   }
 
+  // add_dmi(sim, (Dx, Dy, Dz) arrays / functions, type="bulk")  src/micro/add_field.jl:299-326
+  int add_dmi_bulk_spatial(const double* Dxh, const double* Dyh, const double* Dzh) override {
+    if (mask & TB_DMI_BULK) return fail(MM_ERR_UNSUPPORTED, "one bulk DMI term per handle");
+    if (!Dxh || !Dyh || !Dzh) return fail(MM_ERR_ARG, "spatial bulk DMI needs Dx, Dy and Dz arrays");
+    int rc;
+    if ((rc = upload_R(Dxh, bDx, N)) || (rc = upload_R(Dyh, bDy, N)) || (rc = upload_R(Dzh, bDz, N))) return rc;
+    bulk_spatial = true;
+    mask |= TB_DMI_BULK;
+    ++version;
+    return MM_OK;
+  }
+
+  // add_sot(sim, aj, bj, p)  src/micro/add_field.jl:951-966 (DFTorqueField)
+  int add_sot(const double* ajh, double aj_uni, double bj, double px, double py, double pz) override {
+    if (mask & TB_SOT) return fail(MM_ERR_UNSUPPORTED, "one SOT term per handle");
+    double v;
+    if (ajh && !uniform(ajh, N, v)) {
+      int rc;
+      if ((rc = upload_R(ajh, sot_aj, N))) return rc;
+      sot_spatial = true;
+    } else {
+      sot_aj_uni = ajh ? v : aj_uni;
+    }
+    sot_bj = bj;
+    sot_p[0] = px; sot_p[1] = py; sot_p[2] = pz;
+    mask |= TB_SOT;
+    ++version;
+    return MM_OK;
+  }
+
+  // add_stt(sim; model=:zhang_li, ...)  src/micro/add_field.jl:1150-1190: b*J (AoS 3N), xi
+  int add_stt_zhang_li(const double* bJh, const double* xih, double xi_uni, double ft) override {
+    if (mask & TB_STT_ZL) return fail(MM_ERR_UNSUPPORTED, "one Zhang-Li torque per handle");
+    if (!bJh) return fail(MM_ERR_ARG, "Zhang-Li torque needs the b*J array");
+    int rc;
+    if (!zl_bJ && (rc = alloc(zl_bJ, 3 * N))) return rc;
+    MM_CUDA(cudaMemcpyAsync(stage64, bJh, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st_));
+    launch_aos_to_soa<R>(stage64, zl_bJ, nullptr, N, nullptr, st_);
+    double v;
+    if (xih && !uniform(xih, N, v)) {
+      if ((rc = upload_R(xih, zl_xi, N))) return rc;
+      zl_spatial = true;
+    } else {
+      zl_xi_uni = xih ? v : xi_uni;
+    }
+    zl_ft = ft;
+    MM_CUDA(cudaStreamSynchronize(st_));
+    mask |= TB_STT_ZL;
+    ++version;
+    return MM_OK;
+  }
+
+  // add_stt(sim; model=:slonczewski, ...)  src/micro/add_field.jl:1192-1226
+  int add_stt_slonczewski(const double* Jh, double J_uni, double ft_beta, double Lambda, double P, double xi,
+                          double px, double py, double pz) override {
+    if (mask & TB_STT_SL) return fail(MM_ERR_UNSUPPORTED, "one Slonczewski torque per handle");
+    double v;
+    if (Jh && !uniform(Jh, N, v)) {
+      int rc;
+      if ((rc = upload_R(Jh, sl_J, N))) return rc;
+      sl_spatial = true;
+    } else {
+      sl_J_uni = Jh ? v : J_uni;
+    }
+    sl_ftb = ft_beta;
+    sl_L2 = Lambda * Lambda;
+    sl_P = P;
+    sl_xi = xi;
+    sl_p[0] = px; sl_p[1] = py; sl_p[2] = pz;
+    mask |= TB_STT_SL;
+    ++version;
+    return MM_OK;
+  }
+
+  // add_thermal_noise(sim, Temp; T0, scaling, k_B)  src/micro/add_field.jl:734-760
+  int add_thermal_noise(const double* Th, double T_uni, double T0, double scaling, double kB, uint64_t seed,
+                        double dt) override {
+    if (mask & TB_THERMAL) return fail(MM_ERR_UNSUPPORTED, "one thermal term per handle");
+    if (!(dt > 0)) return fail(MM_ERR_ARG, "thermal noise needs dt > 0 for evaluations outside a step");
+    int rc;
+    double v;
+    if (Th && !uniform(Th, N, v)) {
+      if ((rc = upload_R(Th, th_T, N))) return rc;
+    } else {
+      th_T_uni = Th ? v : T_uni;
+    }
+    if ((rc = alloc(Hth, 3 * N)) || (rc = alloc(th_step, 1))) return rc;
+    th_T0 = T0;
+    th_scaling = scaling;
+    th_kB = kB;
+    th_seed = seed;
+    th_dt = dt;
+    mask |= TB_THERMAL;
+    ++version;
+    MM_CUDA(cudaStreamSynchronize(st_));
+    return MM_OK;
+  }
+
+  // the thermal field of the step whose index is *step (fixed-step counter or
+  // the adaptive stepper's accepted-step count)
+  void enqueue_thermal(const long long* step, const double* dt_dev, double dt, const int* gate) {
+    if (!(mask & TB_THERMAL)) return;
+    const double c = 2.0 * alpha * th_kB * th_scaling / (dx * dy * dz * gamma);
+    launch_thermal<R>(th_seed, step, dt_dev, dt, c, th_T, th_T_uni, th_T0, Ms, Hth, N, gate, st_);
+  }
+
   int add_dmi_interfacial(const double* Dh, double uni) override {
     if (mask & TB_DMI_INTERFACIAL) return fail(MM_ERR_UNSUPPORTED, "one interfacial DMI term per handle");
     double v;
@@ -369,11 +482,36 @@ class Engine : public EngineBase {
     a.llg_c_lo = static_cast<R>(c - static_cast<double>(a.llg_c));
     a.precession = precession;
     a.pins = pins_on ? pins : nullptr;
+    ExtraTerms<R>& x = a.x;
+    x.bD[0] = bulk_spatial ? bDx : nullptr;
+    x.bD[1] = bulk_spatial ? bDy : nullptr;
+    x.bD[2] = bulk_spatial ? bDz : nullptr;
+    x.inv_d[0] = static_cast<R>(1.0 / dx); x.inv_d[1] = static_cast<R>(1.0 / dy); x.inv_d[2] = static_cast<R>(1.0 / dz);
+    x.sot_aj = sot_spatial ? sot_aj : nullptr;
+    x.sot_aj_uni = static_cast<R>(sot_aj_uni);
+    x.sot_b = static_cast<R>(sot_bj / gamma);
+    x.sot_inv_g = static_cast<R>(1.0 / gamma);
+    for (int c3 = 0; c3 < 3; ++c3) {
+      x.sot_p[c3] = static_cast<R>(sot_p[c3]);
+      x.sl_p[c3] = static_cast<R>(sl_p[c3]);
+    }
+    x.zl_bJ = zl_bJ;
+    x.zl_xi = zl_spatial ? zl_xi : nullptr;
+    x.zl_xi_uni = static_cast<R>(zl_xi_uni);
+    x.zl_ut = static_cast<R>(zl_ft / gamma);
+    x.sl_J = sl_spatial ? sl_J : nullptr;
+    x.sl_J_uni = static_cast<R>(sl_J_uni);
+    x.sl_ftb = static_cast<R>(sl_ftb);
+    x.sl_L2 = static_cast<R>(sl_L2);
+    x.sl_P = static_cast<R>(sl_P);
+    x.sl_xi = static_cast<R>(sl_xi);
+    x.Hth = Hth;
     return a;
   }
 
   // ------------------------------------------------------ evaluation --
   void enqueue_field(const R* y, R* out, unsigned msk, R* ecell) {
+    if (msk & mask & TB_THERMAL) enqueue_thermal(th_step, nullptr, th_dt, nullptr);
     if ((msk & mask & TB_DEMAG) && demag) demag->apply(y, Ms, Hd, st_);
     StageArgs<R> s{};
     s.out = out;
@@ -381,7 +519,8 @@ class Engine : public EngineBase {
     launch_stage<R>(SM_FIELD, fargs(msk), y, s, st_);
   }
 
-  void enqueue_rhs(const R* y, R* out) {
+  void enqueue_rhs(const R* y, R* out, bool thermal_draw = true) {
+    if (thermal_draw) enqueue_thermal(th_step, nullptr, th_dt, nullptr);
     if ((mask & TB_DEMAG) && demag) demag->apply(y, Ms, Hd, st_);
     StageArgs<R> s{};
     s.out = out;
@@ -407,7 +546,7 @@ class Engine : public EngineBase {
 
   int term_field(int term, double* f, double* e) override {
     if (int rc = need_ms()) return rc;
-    if (term < 0 || term >= kNTerms) return fail(MM_ERR_ARG, "bad term index %d", term);
+    if (term < 0 || term >= kNTermIds) return fail(MM_ERR_ARG, "bad term index %d", term);
     if (!(mask & (1u << term))) return fail(MM_ERR_ARG, "term %d was not added", term);
     int rc;
     if (!ecell && (rc = alloc(ecell, N))) return rc;
@@ -424,6 +563,7 @@ class Engine : public EngineBase {
 
   int energy(double* per, double* total) override {
     if (int rc = need_ms()) return rc;
+    enqueue_thermal(th_step, nullptr, th_dt, nullptr);
     if ((mask & TB_DEMAG) && demag) demag->apply(m, Ms, Hd, st_);
     StageArgs<R> s{};
     s.partials = partials;
@@ -461,6 +601,7 @@ class Engine : public EngineBase {
   // -------------------------------------------------------------- RK4 --
   void enqueue_rk4_step(double h) {
     const FieldArgs<R> fa = fargs(~0u);
+    enqueue_thermal(th_step, nullptr, h, nullptr);
     for (int s = 1; s <= 4; ++s) {
       // stage inputs ping-pong so that no kernel overwrites a field it reads
       const R* yin = s == 1 ? m : (s == 3 ? yB : yA);
@@ -475,11 +616,13 @@ class Engine : public EngineBase {
       sa.stage = s;
       launch_stage<R>(SM_RK4, fa, yin, sa, st_);
     }
+    if (mask & TB_THERMAL) launch_count_step(th_step, st_);
   }
 
   // advance_step(sim, ::ModifiedEuler) x nsteps  src/integrator/heun.jl:28-49
   void enqueue_heun_step(double h) {
     const FieldArgs<R> fa = fargs(~0u);
+    enqueue_thermal(th_step, nullptr, h, nullptr);
     for (int st = 1; st <= 2; ++st) {
       const R* yin = st == 1 ? m : yA;
       if ((mask & TB_DEMAG) && demag) demag->apply(yin, Ms, Hd, st_);
@@ -493,11 +636,13 @@ class Engine : public EngineBase {
       sa.scheme = 1;
       launch_stage<R>(SM_RK4, fa, yin, sa, st_);
     }
+    if (mask & TB_THERMAL) launch_count_step(th_step, st_);
   }
 
   int heun_run(double dt, int64_t n) override {
     if (int rc = need_ms()) return rc;
     if (n < 0 || !(dt > 0)) return fail(MM_ERR_ARG, "heun: need dt > 0 and nsteps >= 0");
+    th_dt = dt;
     int rc;
     if (!acc && (rc = alloc(acc, 3 * N))) return rc;
     if (!he_graph || he_dt != dt || he_version != version) {
@@ -525,6 +670,7 @@ class Engine : public EngineBase {
   int rk4_run(double dt, int64_t n) override {
     if (int rc = need_ms()) return rc;
     if (n < 0 || !(dt > 0)) return fail(MM_ERR_ARG, "rk4: need dt > 0 and nsteps >= 0");
+    th_dt = dt;
     int rc;
     if (!acc && (rc = alloc(acc, 3 * N))) return rc;
     if (!yB && (rc = alloc(yB, 3 * N))) return rc;
@@ -705,6 +851,9 @@ class Engine : public EngineBase {
     const FieldArgs<R> fa = fargs(~0u);
     const RkTableau& tb = rk_tableau(method);
     auto target_of = [&](int s) { return s == tb.sol ? yn : (s % 2 == 1 ? yA : yB); };
+    // the thermal field of the accepted-step count, as the reference redraws
+    // it when integrator.nsteps advances (src/micro/field.jl:250-253)
+    enqueue_thermal(&ctrl->nsteps, &ctrl->step, 0.0, &ctrl->active);
     for (int s = 1; s <= tb.nstage; ++s) {
       const R* yin = s == 1 ? m : target_of(s - 1);
       R* target = s <= tb.sol ? target_of(s) : nullptr;
@@ -737,7 +886,9 @@ class Engine : public EngineBase {
 
   // compute_initial_step(sim, integrator, 1e-12)  adaptive_rk.jl:151-165
   int initial_step(double& out) {
-    enqueue_rhs(m, work);
+    // the right-hand side sees integrator.step = 1e-15 (adaptive_rk.jl:154)
+    enqueue_thermal(&ctrl->nsteps, nullptr, 1e-15, nullptr);
+    enqueue_rhs(m, work, false);
     launch_absmax<R>(work, 3 * N, partials, scal, st_);
     double mx = 0.0;
     MM_CUDA(cudaMemcpyAsync(&mx, scal, sizeof(double), cudaMemcpyDeviceToHost, st_));
@@ -928,6 +1079,8 @@ class Engine : public EngineBase {
   int adjoint_record(double dt, int64_t n, int64_t ck) override {
     if (int rc = need_ms()) return rc;
     if (n < 1 || !(dt > 0) || ck < 1) return fail(MM_ERR_ARG, "adjoint: need dt > 0, nsteps >= 1, ckpt_every >= 1");
+    if (mask & kExtraBits)
+      return fail(MM_ERR_UNSUPPORTED, "adjoint: torque and thermal terms are not differentiated");
     const int64_t nck = (n + ck - 1) / ck;
     MM_CUDA(cudaStreamSynchronize(st_));
     adj_release();
@@ -1086,6 +1239,23 @@ class Engine : public EngineBase {
   int64_t adj_n = 0, adj_every = 0, adj_nck = 0, adj_seg_cap = 0;
   double adj_dt = 0.0;
   uint64_t adj_version = 0;
+
+  // extra terms
+  R *bDx = nullptr, *bDy = nullptr, *bDz = nullptr;
+  bool bulk_spatial = false;
+  R* sot_aj = nullptr;
+  bool sot_spatial = false;
+  double sot_aj_uni = 0.0, sot_bj = 0.0, sot_p[3] = {0, 0, 0};
+  R *zl_bJ = nullptr, *zl_xi = nullptr;
+  bool zl_spatial = false;
+  double zl_xi_uni = 0.0, zl_ft = 1.0;
+  R* sl_J = nullptr;
+  bool sl_spatial = false;
+  double sl_J_uni = 0.0, sl_ftb = 0.0, sl_L2 = 4.0, sl_P = 0.0, sl_xi = 0.0, sl_p[3] = {0, 0, 0};
+  R *th_T = nullptr, *Hth = nullptr;
+  long long* th_step = nullptr;
+  double th_T_uni = 0.0, th_T0 = 0.0, th_scaling = 1.0, th_kB = 1.3806505e-23, th_dt = 1e-14;
+  uint64_t th_seed = 0;
 
   // ------------------------------------------------------------ state --
   int nx = 1, ny = 1, nz = 1, pbc = 0;
@@ -1322,6 +1492,29 @@ int mm_run_until(mm_handle* h, double t, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h
 int mm_advance_step(mm_handle* h, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h->eng->advance_step(s)); }
 int mm_dopri_reset(mm_handle* h) { MM_HANDLE(h); MM_GUARD(h->eng->dopri_reset()); }
 int mm_set_adaptive_method(mm_handle* h, int method) { MM_HANDLE(h); MM_GUARD(h->eng->set_method(method)); }
+
+int mm_add_dmi_bulk_spatial(mm_handle* h, const double* Dx, const double* Dy, const double* Dz) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->add_dmi_bulk_spatial(Dx, Dy, Dz));
+}
+int mm_add_sot(mm_handle* h, const double* aj, double aj_uniform, double bj, double px, double py, double pz) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->add_sot(aj, aj_uniform, bj, px, py, pz));
+}
+int mm_add_stt_zhang_li(mm_handle* h, const double* bJ, const double* xi, double xi_uniform, double ft) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->add_stt_zhang_li(bJ, xi, xi_uniform, ft));
+}
+int mm_add_stt_slonczewski(mm_handle* h, const double* J, double J_uniform, double ft_beta, double Lambda, double P,
+                           double xi, double px, double py, double pz) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->add_stt_slonczewski(J, J_uniform, ft_beta, Lambda, P, xi, px, py, pz));
+}
+int mm_add_thermal_noise(mm_handle* h, const double* T, double T_uniform, double T0, double scaling, double k_B,
+                         uint64_t seed, double dt) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->add_thermal_noise(T, T_uniform, T0, scaling, k_B, seed, dt));
+}
 
 int mm_adjoint_record(mm_handle* h, double dt, int64_t nsteps, int64_t ckpt_every) {
   MM_HANDLE(h);

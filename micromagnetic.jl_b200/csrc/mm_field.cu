@@ -125,14 +125,15 @@ void launch_nbmask(int nx, int ny, int nz, int pbc, const R* Ms, uint8_t* nbm, c
 // kernels of src/micro/kernels.jl (zeeman 14-20, anisotropy 54-75, exchange
 // 226-304, bulk DMI 306-344, interfacial DMI 426-466) and the demag energy of
 // src/micro/demag.jl:435-456; terms with Ms == 0 contribute nothing.
-template <typename R, bool ENERGY>
+template <typename R, bool ENERGY, bool EXTRA = false>
 __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __restrict__ y, int I, int i, int j,
                                           int k, R m[3], R h[3], double* e) {
   const int64_t N = a.N;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int nxy = nx * ny;
   const unsigned mask = a.mask;
-  const bool local = (mask & (TB_EXCH | TB_DMI_BULK | TB_DMI_INTERFACIAL | TB_ANIS)) != 0;
+  const bool local = (mask & (TB_EXCH | TB_DMI_BULK | TB_DMI_INTERFACIAL | TB_ANIS)) != 0 ||
+                     (EXTRA && (mask & TB_STT_ZL));
   // Every load is issued before any use: neighbour indices are clamped to the
   // cell itself where a neighbour does not exist (the mask bit then drops the
   // term), so no load waits on another.
@@ -218,6 +219,27 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
         h[2] += fz * Ms_inv;
       }
     }
+    // spatial bulk DMI (spatial_vector_bulkdmi_kernel!, kernels.jl:347-422):
+    // per axis the harmonic mean of the two cells' D, pairs with a zero D dropped
+    if (EXTRA && (mask & TB_DMI_BULK) && a.x.bD[0]) {
+      R fx = 0, fy = 0, fz = 0;
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        if (!((nbm >> d) & 1u)) continue;
+        const int ax = d >> 1;
+        const R Di = a.x.bD[ax][I], Dn = a.x.bD[ax][nb[d]];
+        if (Di == R(0) || Dn == R(0)) continue;
+        const R Deff = 2 * Di * Dn / (Di + Dn);
+        const R s = (d & 1) ? -a.x.inv_d[ax] : a.x.inv_d[ax];
+        if (ax == 0) { fy += Deff * (-s * mn[d][2]); fz += Deff * (s * mn[d][1]); }
+        else if (ax == 1) { fx += Deff * (s * mn[d][2]); fz += Deff * (-s * mn[d][0]); }
+        else { fx += Deff * (-s * mn[d][1]); fy += Deff * (s * mn[d][0]); }
+      }
+      if (ENERGY) e[2] = -0.5 * (double(fx) * m[0] + double(fy) * m[1] + double(fz) * m[2]) * double(a.V);
+      h[0] += fx * Ms_inv;
+      h[1] += fy * Ms_inv;
+      h[2] += fz * Ms_inv;
+    } else
     // bulk DMI: sum_d (D/d) a_d x m_d, a = +x,-x,+y,-y,+z,-z for d = -x,+x,-y,+y,-z,+z
     if (mask & TB_DMI_BULK) {
       R fx = 0, fy = 0, fz = 0;
@@ -279,6 +301,56 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
     h[1] += zy;
     h[2] += zz;
     if (ENERGY) e[0] = -double(a.V) * double(Ms) * (double(m[0]) * zx + double(m[1]) * zy + double(m[2]) * zz);
+  }
+  if constexpr (EXTRA) {
+    const ExtraTerms<R>& x = a.x;
+    // df_torque_kernel! (kernels.jl:619-632): h = (aj/gamma) m x p + (bj/gamma) p
+    if (mask & TB_SOT) {
+      const R aa = (x.sot_aj ? x.sot_aj[I] : x.sot_aj_uni) * x.sot_inv_g;
+      h[0] += aa * (m[1] * x.sot_p[2] - m[2] * x.sot_p[1]) + x.sot_b * x.sot_p[0];
+      h[1] += aa * (m[2] * x.sot_p[0] - m[0] * x.sot_p[2]) + x.sot_b * x.sot_p[1];
+      h[2] += aa * (m[0] * x.sot_p[1] - m[1] * x.sot_p[0]) + x.sot_b * x.sot_p[2];
+    }
+    // zhangli_torque_kernel! (kernels.jl:680-739): f = ut sum_axis bJ_axis (m_+ - m_-)
+    // / (2d or d), neighbours by existence in the mesh; h = m x f + xi f
+    if (mask & TB_STT_ZL) {
+      const bool px = a.pbc & 1, py = a.pbc & 2, pz = a.pbc & 4;
+      const bool ex[6] = {i > 0 || px, i < nx - 1 || px, j > 0 || py, j < ny - 1 || py, k > 0 || pz, k < nz - 1 || pz};
+      R f[3] = {R(0), R(0), R(0)};
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        const R dd = ax == 0 ? x.inv_d[0] : (ax == 1 ? x.inv_d[1] : x.inv_d[2]);
+        const R fac = (ex[2 * ax] && ex[2 * ax + 1]) ? R(0.5) * dd : dd;
+        const R u = x.zl_bJ[ax * N + I] * fac;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const R mp = ex[2 * ax + 1] ? mn[2 * ax + 1][c] : m[c];
+          const R mm = ex[2 * ax] ? mn[2 * ax][c] : m[c];
+          f[c] += u * (mp - mm);
+        }
+      }
+      const R xi = x.zl_xi ? x.zl_xi[I] : x.zl_xi_uni;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) f[c] *= x.zl_ut;
+      h[0] += (m[1] * f[2] - m[2] * f[1]) + xi * f[0];
+      h[1] += (m[2] * f[0] - m[0] * f[2]) + xi * f[1];
+      h[2] += (m[0] * f[1] - m[1] * f[0]) + xi * f[2];
+    }
+    // slonczewski_torque_kernel!: eps = P L^2 / (L^2 + 1 + (L^2 - 1) m.p),
+    // h = J ft beta (eps m x p + xi p)
+    if (mask & TB_STT_SL) {
+      const R mp = m[0] * x.sl_p[0] + m[1] * x.sl_p[1] + m[2] * x.sl_p[2];
+      const R eps = x.sl_P * x.sl_L2 / (x.sl_L2 + R(1) + (x.sl_L2 - R(1)) * mp);
+      const R aa = (x.sl_J ? x.sl_J[I] : x.sl_J_uni) * x.sl_ftb;
+      h[0] += aa * (eps * (m[1] * x.sl_p[2] - m[2] * x.sl_p[1]) + x.sl_xi * x.sl_p[0]);
+      h[1] += aa * (eps * (m[2] * x.sl_p[0] - m[0] * x.sl_p[2]) + x.sl_xi * x.sl_p[1]);
+      h[2] += aa * (eps * (m[0] * x.sl_p[1] - m[1] * x.sl_p[0]) + x.sl_xi * x.sl_p[2]);
+    }
+    if (mask & TB_THERMAL) {
+      h[0] += x.Hth[I];
+      h[1] += x.Hth[N + I];
+      h[2] += x.Hth[2 * N + I];
+    }
   }
 }
 
@@ -347,7 +419,7 @@ __constant__ RkTableau c_rk[RK_NMETHODS] = MM_RK_TABLES;
 static const RkTableau h_rk[RK_NMETHODS] = MM_RK_TABLES;
 const RkTableau& rk_tableau(int method) { return h_rk[method]; }
 
-template <typename R, int MODE>
+template <typename R, int MODE, bool EXTRA>
 __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage(FieldArgs<R> a, const R* __restrict__ y, StageArgs<R> s) {
   constexpr bool kF32 = sizeof(R) == 4;
   if (MODE == SM_DOPRI && !s.ctrl->active) return;
@@ -375,7 +447,7 @@ __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage
   // FSAL: stage 1 takes k1 from the last stage of the accepted attempt
   const bool reuse = MODE == SM_DOPRI && s.stage == 1 && !s.ctrl->eval1;
   if (live) {
-    if (!reuse) cell_heff<R, MODE == SM_ENERGY || MODE == SM_FIELD>(a, y, I, i, j, k, m, h, e);
+    if (!reuse) cell_heff<R, MODE == SM_ENERGY || MODE == SM_FIELD, EXTRA>(a, y, I, i, j, k, m, h, e);
     if (MODE == SM_FIELD) {
       s.out[I] = h[0];
       s.out[N + I] = h[1];
@@ -593,12 +665,23 @@ __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage
 template <typename R>
 void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<R>& sa, cudaStream_t st) {
   const StageGrid g = stage_grid(fa.nx, fa.ny, fa.nz);
+  // handles without the extra terms run the kernel compiled without them
+  if ((fa.mask & kExtraBits) || ((fa.mask & TB_DMI_BULK) && fa.x.bD[0])) {
+    switch (mode) {
+      case SM_FIELD: k_stage<R, SM_FIELD, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+      case SM_RHS: k_stage<R, SM_RHS, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+      case SM_RK4: k_stage<R, SM_RK4, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+      case SM_ENERGY: k_stage<R, SM_ENERGY, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+      default: k_stage<R, SM_DOPRI, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+    }
+    return;
+  }
   switch (mode) {
-    case SM_FIELD: k_stage<R, SM_FIELD><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-    case SM_RHS: k_stage<R, SM_RHS><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-    case SM_RK4: k_stage<R, SM_RK4><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-    case SM_ENERGY: k_stage<R, SM_ENERGY><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-    default: k_stage<R, SM_DOPRI><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+    case SM_FIELD: k_stage<R, SM_FIELD, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+    case SM_RHS: k_stage<R, SM_RHS, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+    case SM_RK4: k_stage<R, SM_RK4, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+    case SM_ENERGY: k_stage<R, SM_ENERGY, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+    default: k_stage<R, SM_DOPRI, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
   }
 }
 
@@ -700,6 +783,50 @@ void launch_average_m(const R* m, const R* m_lo, int64_t N, double* partials, do
   k_reduce_sum<<<1, 256, 0, st>>>(partials, nb, 3, out);
 }
 
+// ------------------------------------------------------------- thermal ---
+template <typename R>
+__global__ void k_thermal(uint32_t k0, uint32_t k1, const long long* __restrict__ step,
+                          const double* __restrict__ dt_dev, double dt, double c, const R* __restrict__ T,
+                          double T_uni, double T0, const R* __restrict__ mu0Ms, R* __restrict__ H, int64_t N,
+                          const int* __restrict__ gate) {
+  if (gate && !*gate) return;
+  const int64_t I = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (I >= N) return;
+  const uint64_t n = static_cast<uint64_t>(*step);
+  const double ms = double(mu0Ms[I]);
+  double v[3] = {0.0, 0.0, 0.0};
+  if (ms > 0) {
+    uint32_t ctr[4] = {static_cast<uint32_t>(I), static_cast<uint32_t>(static_cast<uint64_t>(I) >> 32),
+                       static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32)};
+    philox4x32_10(ctr, k0, k1);
+    const double s32 = 2.3283064365386963e-10;  // 2^-32
+    const double r0 = sqrt(-2.0 * log((double(ctr[0]) + 1.0) * s32));
+    const double r1 = sqrt(-2.0 * log((double(ctr[2]) + 1.0) * s32));
+    const double t0 = 6.283185307179586 * (double(ctr[1]) * s32);
+    const double t1 = 6.283185307179586 * (double(ctr[3]) * s32);
+    const double h = dt_dev ? *dt_dev : dt;
+    const double Tl = (T ? double(T[I]) : T_uni) + T0;
+    const double scale = sqrt(c / h * Tl / ms);
+    v[0] = r0 * cos(t0) * scale;
+    v[1] = r0 * sin(t0) * scale;
+    v[2] = r1 * cos(t1) * scale;
+  }
+  H[I] = static_cast<R>(v[0]);
+  H[N + I] = static_cast<R>(v[1]);
+  H[2 * N + I] = static_cast<R>(v[2]);
+}
+
+template <typename R>
+void launch_thermal(uint64_t seed, const long long* step, const double* dt_dev, double dt, double c, const R* T,
+                    double T_uni, double T0, const R* mu0Ms, R* Hth, int64_t N, const int* gate, cudaStream_t st) {
+  k_thermal<R><<<stage_blocks(N), kStageThreads, 0, st>>>(static_cast<uint32_t>(seed),
+                                                          static_cast<uint32_t>(seed >> 32), step, dt_dev, dt, c, T,
+                                                          T_uni, T0, mu0Ms, Hth, N, gate);
+}
+
+__global__ void k_count_step(long long* step) { *step += 1; }
+void launch_count_step(long long* step, cudaStream_t st) { k_count_step<<<1, 1, 0, st>>>(step); }
+
 // ------------------------------------------------------------- adjoint ---
 // Reverse mode through one RK4 step.  The forward step is
 //   Y1 = y, Yi = y + c_i h k_{i-1} (c = 1/2, 1/2, 1), k_i = f(Y_i),
@@ -780,7 +907,7 @@ __global__ void __launch_bounds__(kStageThreads) k_adj_rhs(FieldArgs<R> a, int z
   if (i >= a.nx || j >= a.ny) return;
   const int I = (k * a.ny + j) * a.nx + i;
   R mr[3], hl[3];
-  cell_heff<R, false>(a, Y, I, i, j, k, mr, hl, nullptr);  // local terms only
+  cell_heff<R, false, true>(a, Y, I, i, j, k, mr, hl, nullptr);  // local terms only
   const double ms = double(a.Ms[I]);
   const bool pinned = a.pins && a.pins[I];
   if (ms == 0.0 || pinned) {
@@ -873,7 +1000,7 @@ __global__ void __launch_bounds__(kStageThreads)
   if (i >= a.nx || j >= a.ny) return;
   const int I = (k * a.ny + j) * a.nx + i;
   R wr[3], hw[3];
-  cell_heff<R, false>(a, w, I, i, j, k, wr, hw, nullptr);  // linear local terms on w + demag(w)
+  cell_heff<R, false, true>(a, w, I, i, j, k, wr, hw, nullptr);  // linear local terms on w + demag(w)
   const double ms = double(a.Ms[I]);
   double av[3];
 #pragma unroll
@@ -942,6 +1069,8 @@ void launch_adj_field(const FieldArgs<R>& fa_lin, const R* w, const R* q, const 
   template void launch_soa_to_aos<R>(const R*, const R*, double*, int64_t, cudaStream_t);               \
   template void launch_scalar_to_R<R>(const double*, R*, int64_t, double, cudaStream_t);                \
   template void launch_average_m<R>(const R*, const R*, int64_t, double*, double*, cudaStream_t);      \
+  template void launch_thermal<R>(uint64_t, const long long*, const double*, double, double, const R*, double,   \
+                                  double, const R*, R*, int64_t, const int*, cudaStream_t);                     \
   template void launch_adj_stage_input<R>(const R*, const R*, const R*, double, R*, int64_t, cudaStream_t); \
   template void launch_adj_normalise<R>(const R*, const R*, const R* const[4], double, double*, double*,   \
                                         double*, int64_t, cudaStream_t);                                   \

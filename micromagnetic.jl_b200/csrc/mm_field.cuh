@@ -18,8 +18,34 @@ enum TermBit : unsigned {
   TB_DMI_INTERFACIAL = 1u << 3,
   TB_ANIS = 1u << 4,
   TB_DEMAG = 1u << 5,
+  TB_SOT = 1u << 6,        // add_sot: field-like / damping-like torque field
+  TB_STT_ZL = 1u << 7,     // add_stt(model=:zhang_li)
+  TB_STT_SL = 1u << 8,     // add_stt(model=:slonczewski)
+  TB_THERMAL = 1u << 9,    // add_thermal_noise
 };
-constexpr int kNTerms = 6;
+constexpr int kNTerms = 6;  // terms with an energy (Zeeman .. demag)
+constexpr int kNTermIds = 10;
+constexpr unsigned kExtraBits = TB_SOT | TB_STT_ZL | TB_STT_SL | TB_THERMAL;
+
+// Terms outside the base set, evaluated in the same per-cell kernel when a
+// handle has them (src/micro/kernels.jl: spatial_vector_bulkdmi 347-422,
+// df_torque 619-632, zhangli_torque 680-739, slonczewski_torque;
+// stochastic_field 469-494).  Torque terms enter as equivalent fields, as the
+// reference adds them to the effective field.
+template <typename R> struct ExtraTerms {
+  const R* bD[3];          // spatial bulk DMI: per-cell Dx, Dy, Dz (null: uniform bd_*)
+  R inv_d[3];              // 1/dx, 1/dy, 1/dz
+  const R* sot_aj;         // SOT: h = (aj/gamma)(m x p) + (bj/gamma) p
+  R sot_aj_uni, sot_b, sot_inv_g;
+  R sot_p[3];
+  const R* zl_bJ;          // Zhang-Li: b*J per cell, SoA 3N
+  const R* zl_xi;
+  R zl_xi_uni, zl_ut;      // ut = ft / gamma
+  const R* sl_J;           // Slonczewski: J per cell
+  R sl_J_uni, sl_ftb, sl_L2, sl_P, sl_xi;
+  R sl_p[3];
+  const R* Hth;            // thermal field of the current step, SoA 3N
+};
 
 template <typename R> struct FieldArgs {
   int nx, ny, nz, pbc;
@@ -52,6 +78,7 @@ template <typename R> struct FieldArgs {
   R alpha, llg_c, llg_c_lo;
   int precession;
   const uint8_t* pins;
+  ExtraTerms<R> x;
 };
 
 enum StageMode { SM_FIELD = 0, SM_RHS = 1, SM_RK4 = 2, SM_ENERGY = 3, SM_DOPRI = 4 };
@@ -134,6 +161,37 @@ void launch_reduce_sum(const double* partials, int nblocks, int width, double* o
 
 template <typename R>
 void launch_average_m(const R* m, const R* m_lo, int64_t N, double* partials, double* out, cudaStream_t st);
+
+// ------------------------------------------------------------- thermal ---
+// Counter-based normal deviates: Philox-4x32-10 (Salmon, Moraes, Dror, Shaw,
+// SC'11) on the counter (cell, step) with the seed as key, Box-Muller on the
+// four 32-bit outputs.  Identical on host and device, so the thermal field of
+// step n is a function of (seed, n, cell) only.
+__host__ __device__ inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * c[0];
+    const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c[2];
+    const uint32_t hi0 = static_cast<uint32_t>(p0 >> 32), lo0 = static_cast<uint32_t>(p0);
+    const uint32_t hi1 = static_cast<uint32_t>(p1 >> 32), lo1 = static_cast<uint32_t>(p1);
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0;
+    c[1] = lo1;
+    c[2] = n2;
+    c[3] = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+// add_thermal_noise: H = eta sqrt(factor (T + T0) / mu0Ms), factor =
+// 2 alpha k_B scaling / (V gamma dt)  (stochastic_field_kernel!,
+// src/micro/kernels.jl:469-494; src/micro/field.jl:244-280).  The step index
+// is read from step (device); dt from dt_dev when non-null, else dt.
+template <typename R>
+void launch_thermal(uint64_t seed, const long long* step, const double* dt_dev, double dt, double alpha_kB_s_over_Vg,
+                    const R* T, double T_uni, double T0, const R* mu0Ms, R* Hth, int64_t N, const int* gate,
+                    cudaStream_t st);
+void launch_count_step(long long* step, cudaStream_t st);
 
 // ------------------------------------------------------------- adjoint ---
 // Discrete adjoint of one RK4 step (src/integrator/rk.jl:23-52 with the

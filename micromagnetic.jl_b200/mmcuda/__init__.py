@@ -15,6 +15,9 @@ from .sim import (  # noqa: F401
     add_demag,
     add_dmi,
     add_exch,
+    add_sot,
+    add_stt,
+    add_thermal_noise,
     add_zeeman,
     advance_step,
     average_m,

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "libmmcuda.so")
 
 MM_OK = 0
 MM_ERR_ARG, MM_ERR_CUDA, MM_ERR_NAN, MM_ERR_NOCONVERGE = -1, -2, -3, -4
+MM_ERR_TIMEOUT, MM_ERR_STATE, MM_ERR_UNSUPPORTED = -5, -6, -7
 STATUS = {
     -1: "MM_ERR_ARG",
     -2: "MM_ERR_CUDA",
@@ -29,6 +30,7 @@ MM_RK_DORMAND_PRINCE, MM_RK_BS23, MM_RK_CASH_KARP54, MM_RK_FEHLBERG54 = 0, 1, 2,
 MM_OVF_TEXT, MM_OVF_BINARY4, MM_OVF_BINARY8 = 0, 4, 8
 RK_METHODS = {"DormandPrince": 0, "DOPRI54": 0, "BS23": 1, "CashKarp54": 2, "Fehlberg54": 3, "RKF54": 3}
 TERM_ZEEMAN, TERM_EXCH, TERM_DMI_BULK, TERM_DMI_INTERFACIAL, TERM_ANIS, TERM_DEMAG = range(6)
+TERM_SOT, TERM_STT_ZHANG_LI, TERM_STT_SLONCZEWSKI, TERM_THERMAL = 6, 7, 8, 9
 NTERMS = 6
 DRIVER_SD, DRIVER_LLG = 0, 1
 
@@ -42,7 +44,8 @@ EXPORTS = (
     "mm_advance_step", "mm_dopri_reset", "mm_relax", "mm_kernel_time", "mm_rk4_launches_per_step",
     "mm_energy_noalloc", "mm_batch_create", "mm_batch_rk4_run", "mm_batch_get_stream", "mm_batch_destroy",
     "mm_heun_run", "mm_set_adaptive_method", "mm_ovf_write", "mm_ovf_read_header", "mm_ovf_read",
-    "mm_save_ovf", "mm_load_ovf", "mm_adjoint_record", "mm_adjoint_backward",
+    "mm_save_ovf", "mm_load_ovf", "mm_adjoint_record", "mm_adjoint_backward", "mm_add_dmi_bulk_spatial",
+    "mm_add_sot", "mm_add_stt_zhang_li", "mm_add_stt_slonczewski", "mm_add_thermal_noise",
 )
 KERNELS = ("demag_fwd_x", "demag_fwd_y", "demag_conv", "demag_inv_y", "demag_inv_x", "rk4_stage", "rk4_step")
 
@@ -119,6 +122,11 @@ def load():
         "mm_save_ovf": ([_vp, ctypes.c_char_p, i, ctypes.c_char_p], i),
         "mm_load_ovf": ([_vp, ctypes.c_char_p], i),
         "mm_adjoint_record": ([_vp, d, i64, i64], i),
+        "mm_add_dmi_bulk_spatial": ([_vp, _dp, _dp, _dp], i),
+        "mm_add_sot": ([_vp, _dp, d, d, d, d, d], i),
+        "mm_add_stt_zhang_li": ([_vp, _dp, _dp, d, d], i),
+        "mm_add_stt_slonczewski": ([_vp, _dp, d, d, d, d, d, d, d, d], i),
+        "mm_add_thermal_noise": ([_vp, _dp, d, d, d, d, ctypes.c_uint64, d], i),
         "mm_adjoint_backward": ([_vp, _dp, _dp, _dp, _dp, _dp], i),
         "mm_dopri_set_tol": ([_vp, d], i),
         "mm_run_until": ([_vp, d, ctypes.POINTER(Stats)], i),

@@ -18,6 +18,10 @@ from . import _lib
 from ._lib import Handle, check, dptr
 
 mu_0 = 4 * math.pi * 1e-7  # src/const.jl:1
+mu_B = 9.27400949e-24      # src/const.jl:2
+k_B = 1.3806505e-23        # src/const.jl:3
+c_e = 1.602176565e-19      # src/const.jl:4
+h_bar = 1.05457172647e-34  # src/const.jl:9
 mT = 0.001 / mu_0          # src/const.jl:13
 
 _precision = [np.float64]  # global Float[] of src/MicroMagnetic.jl
@@ -365,7 +369,11 @@ def add_dmi(sim: Sim, D, name="dmi", type="bulk"):
             sim._h.call("mm_add_dmi_bulk", *(float(x) for x in D))
             kind = _lib.TERM_DMI_BULK
         else:
-            raise NotImplementedError("spatially varying bulk DMI is outside the accelerated path")
+            # SpatialVectorBulkDMI: a tuple of per-axis fields, or one field for all axes
+            parts = D if (isinstance(D, tuple) and len(D) == 3) else (D, D, D)
+            arrs = [np.ascontiguousarray(_scalar_field(sim.mesh, x)) for x in parts]
+            sim._h.call("mm_add_dmi_bulk_spatial", *(dptr(a) for a in arrs))
+            kind = _lib.TERM_DMI_BULK
     elif type == "interfacial":
         a = _scalar_field(sim.mesh, D)
         sim._h.call("mm_add_dmi_interfacial", dptr(np.ascontiguousarray(a)), 0.0)
@@ -390,6 +398,76 @@ def add_anis(sim: Sim, Ku, axis=(0, 0, 1), name="anis"):
     ax = [float(x) for x in axis]
     sim._h.call("mm_add_anis", dptr(np.ascontiguousarray(a)), 0.0, *ax)
     t = Term(sim, _lib.TERM_ANIS, name)
+    sim.interactions.append(t)
+    return t
+
+
+def _const_scale(f, name):
+    if callable(f):
+        v = float(f(0.0))
+        warnings.warn(f"{name}: a time-dependent scale is taken at t = 0 ({v}) on this path")
+        return v
+    return float(f)
+
+
+def add_sot(sim: Sim, aj, bj, p, name="sot"):
+    """add_sot(sim, aj, bj, p; name)  src/micro/add_field.jl:951-966:
+    H = (aj/gamma) m x p + (bj/gamma) p."""
+    a = _scalar_field(sim.mesh, aj)
+    sim._h.call("mm_add_sot", dptr(np.ascontiguousarray(a)), 0.0, float(bj), *(float(x) for x in p))
+    t = Term(sim, _lib.TERM_SOT, name)
+    sim.interactions.append(t)
+    return t
+
+
+def add_stt(sim: Sim, model="slonczewski", **params):
+    """add_stt(sim; model=:slonczewski | :zhang_li, kwargs...)  src/micro/add_field.jl:1134-1226."""
+    model = str(model).lstrip(":")
+    if "J" not in params:
+        raise ValueError("Current density parameter `J` is required.")
+    ft = _const_scale(params.get("ft", 1.0), "add_stt ft")
+    if model == "zhang_li":
+        has_b = "b" in params
+        has_P = "P" in params and "Ms" in params
+        if has_b:
+            b = float(params["b"])
+        elif has_P:
+            b = params["P"] * mu_B / (c_e * params["Ms"])
+        else:
+            raise ValueError("Zhang-Li model requires either `b` or `(P, Ms)` parameters")
+        xi = _scalar_field(sim.mesh, params.get("xi", 0.0))
+        bJ = _vector_field(sim.mesh, params["J"]) * b
+        if has_P and not has_b:
+            bJ = (bJ.reshape(-1, 3) / (1 + xi ** 2)[:, None]).reshape(-1)
+        sim._h.call("mm_add_stt_zhang_li", dptr(np.ascontiguousarray(bJ)), dptr(np.ascontiguousarray(xi)), 0.0, ft)
+        t = Term(sim, _lib.TERM_STT_ZHANG_LI, params.get("name", "zhangli"))
+    elif model == "slonczewski":
+        for k in ("tf", "Ms", "p", "P"):
+            if k not in params:
+                raise ValueError(f"Parameter {k} is not provided")
+        beta = h_bar / (mu_0 * params["Ms"] * c_e * params["tf"])
+        J = _scalar_field(sim.mesh, params["J"])
+        p = params["p"]
+        sim._h.call("mm_add_stt_slonczewski", dptr(np.ascontiguousarray(J)), 0.0, ft * beta,
+                    float(params.get("Lambda", 2.0)), float(params["P"]), float(params.get("xi", 0.0)),
+                    *(float(x) for x in p))
+        t = Term(sim, _lib.TERM_STT_SLONCZEWSKI, params.get("name", "slonczewski"))
+    else:
+        raise ValueError(f"Unsupported STT model: {model}. Supported models are: zhang_li, slonczewski")
+    sim.interactions.append(t)
+    return t
+
+
+def add_thermal_noise(sim: Sim, Temp, name="thermal", T0=0.0, scaling=1.0, k_B=k_B, seed=0):
+    """add_thermal_noise(sim, Temp; name, T0, scaling, k_B)  src/micro/add_field.jl:734-760.
+    The noise of step n in cell i is a counter-based draw from `seed`."""
+    if callable(Temp) and _nargs(Temp) == 4:
+        raise NotImplementedError("space-time temperature profiles are outside the accelerated path")
+    T = _scalar_field(sim.mesh, Temp)
+    dt = float(sim.driver.integrator._step) if sim.driver.integrator is not None and sim.driver.integrator._step else 1e-14
+    sim._h.call("mm_add_thermal_noise", dptr(np.ascontiguousarray(T)), 0.0, float(T0),
+                _const_scale(scaling, "add_thermal_noise scaling"), float(k_B), int(seed), dt)
+    t = Term(sim, _lib.TERM_THERMAL, name)
     sim.interactions.append(t)
     return t
 
@@ -562,13 +640,13 @@ def write_data(sim: Sim):
     E = compute_system_energy(sim)
     m = average_m(sim)
     fname = f"{sim.name}_{sim.driver_name.lower()}.txt"
-    names = [t.name for t in sim.interactions]
+    names = [t.name for t in sim.interactions if t.kind < _lib.NTERMS]  # torque fields carry no energy
     if not sim._header_saved:
         with open(fname, "w") as f:
             cols = ["step", "time", "E_total", "m_x", "m_y", "m_z"] + [f"E_{n}" for n in names]
             f.write("#" + "".join(f"{c:>18s}" for c in cols) + "\n")
         sim._header_saved = True
-    per = [sim.energies[t.kind] for t in sim.interactions]
+    per = [sim.energies[t.kind] for t in sim.interactions if t.kind < _lib.NTERMS]
     with open(fname, "a") as f:
         vals = [sim.saver_nsteps, sim.saver_t, E, *m, *per]
         f.write(" " + "".join(f"{v:18.10e}" if isinstance(v, float) else f"{v:18d}" for v in vals) + "\n")

@@ -246,7 +246,10 @@ double tensor_comp(int c, double x, double y, double z, double dx, double dy, do
 // Terms (src/head.jl:150-310).  Each keeps its own field (3N) and energy (N)
 // buffers, exactly like the reference's interaction structs.
 // ---------------------------------------------------------------------------
-enum TermKind { T_ZEEMAN = 0, T_EXCH = 1, T_DMI_BULK = 2, T_DMI_INTERFACIAL = 3, T_ANIS = 4, T_DEMAG = 5 };
+enum TermKind {
+  T_ZEEMAN = 0, T_EXCH = 1, T_DMI_BULK = 2, T_DMI_INTERFACIAL = 3, T_ANIS = 4, T_DEMAG = 5,
+  T_DMI_BULK_SPATIAL = 6, T_SOT = 7, T_STT_ZL = 8, T_STT_SL = 9, T_THERMAL = 10
+};
 
 struct Term {
   TermKind kind;
@@ -265,6 +268,18 @@ struct Term {
   // demag
   int Px = 1, Py = 1, Pz = 1;
   std::vector<double> Nhat[6];  // real spectra, full (Pz,Py,Px) grid
+  // spatial bulk DMI (per-axis arrays)
+  std::vector<double> bD[3];
+  // SOT (DFTorqueField): aj per cell, bj, p
+  std::vector<double> aj;
+  double bj = 0, p[3] = {0, 0, 0};
+  // Zhang-Li: b*J (AoS 3N), xi per cell, ft;  Slonczewski: J per cell, ft*beta, Lambda, P, xi, p
+  std::vector<double> bJ, xi, J;
+  double ft = 1.0, ftb = 0.0, Lambda = 2.0, P = 0.0, xi_s = 0.0;
+  // thermal: T per cell, T0, scaling, k_B, seed, dt outside a step
+  std::vector<double> T;
+  double T0 = 0.0, scaling = 1.0, kB = 1.3806505e-23, dt = 1e-14;
+  uint64_t seed = 0;
   std::vector<double> field, energy;
 };
 
@@ -287,6 +302,11 @@ struct Sim {
   int64_t nsteps = 0, nfevals = 0;
   bool succeed = false;
   int method = 0;  // 0 DOPRI54, 1 BS23, 2 CashKarp54, 3 Fehlberg54
+  // thermal noise: fixed-step counter; the (step, dt) the current evaluation draws for
+  int64_t th_step = 0;
+  int64_t th_cur_step = 0;
+  double th_cur_dt = 0.0;
+  double th_dt = 1e-14;  // dt of evaluations outside a step: the add-time value, then the last fixed step
   std::vector<double> y_current, y_next, y_temp;
   std::vector<double> ks[7];
   // SD driver (src/sd.jl; src/driver.jl:95-102)
@@ -542,6 +562,135 @@ void demag_field(const Sim& s, const Term& tm, const double* m, double* h, doubl
       }
 }
 
+// spatial_vector_bulkdmi_kernel!  src/micro/kernels.jl:347-422
+void dmi_bulk_spatial(const Sim& s, const Term& tm, const double* m, double* h, double* e) {
+  const Mesh& g = s.mesh;
+  const double axes[6] = {1 / g.dx, -1 / g.dx, 1 / g.dy, -1 / g.dy, 1 / g.dz, -1 / g.dz};
+#pragma omp parallel for schedule(static)
+  for (int64_t I = 0; I < g.n; ++I) {
+    const int64_t i = 3 * I;
+    const double Ms = s.mu0Ms[I];
+    if (Ms == 0.0) { e[I] = 0; h[i] = h[i + 1] = h[i + 2] = 0; continue; }
+    double fx = 0, fy = 0, fz = 0;
+    for (int d = 0; d < 6; ++d) {
+      const int64_t id = g.ngb[6 * I + d];
+      if (id < 0 || !(s.mu0Ms[id] > 0)) continue;
+      const int ax = d / 2;
+      const double Di = tm.bD[ax][I], Dn = tm.bD[ax][id];
+      if (Di == 0 || Dn == 0) continue;
+      const double Deff = 2 * Di * Dn / (Di + Dn), a = axes[d];
+      const int64_t k = 3 * id;
+      if (ax == 0) { fy += Deff * (-a * m[k + 2]); fz += Deff * (a * m[k + 1]); }
+      else if (ax == 1) { fx += Deff * (a * m[k + 2]); fz += Deff * (-a * m[k]); }
+      else { fx += Deff * (-a * m[k + 1]); fy += Deff * (a * m[k]); }
+    }
+    const double Ms_inv = 1.0 / Ms;
+    e[I] = -0.5 * (fx * m[i] + fy * m[i + 1] + fz * m[i + 2]) * g.volume;
+    h[i] = fx * Ms_inv; h[i + 1] = fy * Ms_inv; h[i + 2] = fz * Ms_inv;
+  }
+}
+
+// df_torque_kernel!  src/micro/kernels.jl:619-632
+void sot_field(const Sim& s, const Term& tm, const double* m, double* h, double* e) {
+  const Mesh& g = s.mesh;
+  for (int64_t I = 0; I < g.n; ++I) {
+    const int64_t j = 3 * I;
+    const double a = tm.aj[I] / s.gamma, b = tm.bj / s.gamma;
+    double cx, cy, cz;
+    cross3(m[j], m[j + 1], m[j + 2], tm.p[0], tm.p[1], tm.p[2], cx, cy, cz);
+    h[j] = a * cx + b * tm.p[0]; h[j + 1] = a * cy + b * tm.p[1]; h[j + 2] = a * cz + b * tm.p[2];
+    e[I] = 0;
+  }
+}
+
+// zhangli_torque_kernel!  src/micro/kernels.jl:680-739 (ut = ft / gamma)
+void zhangli_field(const Sim& s, const Term& tm, const double* m, double* h, double* e) {
+  const Mesh& g = s.mesh;
+  const double ds[3] = {g.dx, g.dy, g.dz};
+  const double ut = tm.ft / s.gamma;
+  for (int64_t I = 0; I < g.n; ++I) {
+    const int64_t j = 3 * I;
+    double f[3] = {0, 0, 0};
+    for (int ax = 0; ax < 3; ++ax) {
+      int64_t i1 = g.ngb[6 * I + 2 * ax], i2 = g.ngb[6 * I + 2 * ax + 1];
+      const double factor = (i1 >= 0 && i2 >= 0) ? 1 / (2 * ds[ax]) : 1 / ds[ax];
+      if (i1 < 0) i1 = I;
+      if (i2 < 0) i2 = I;
+      const double u = tm.bJ[j + ax] * factor;
+      for (int c = 0; c < 3; ++c) f[c] += u * (m[3 * i2 + c] - m[3 * i1 + c]);
+    }
+    for (int c = 0; c < 3; ++c) f[c] *= ut;
+    double cx, cy, cz;
+    cross3(m[j], m[j + 1], m[j + 2], f[0], f[1], f[2], cx, cy, cz);
+    h[j] = cx + tm.xi[I] * f[0]; h[j + 1] = cy + tm.xi[I] * f[1]; h[j + 2] = cz + tm.xi[I] * f[2];
+    e[I] = 0;
+  }
+}
+
+// slonczewski_torque_kernel!  src/micro/kernels.jl (ft multiplied by beta)
+void slonczewski_field(const Sim& s, const Term& tm, const double* m, double* h, double* e) {
+  const Mesh& g = s.mesh;
+  const double L2 = tm.Lambda * tm.Lambda;
+  for (int64_t I = 0; I < g.n; ++I) {
+    const int64_t j = 3 * I;
+    const double mp = m[j] * tm.p[0] + m[j + 1] * tm.p[1] + m[j + 2] * tm.p[2];
+    const double eps = tm.P * L2 / (L2 + 1 + (L2 - 1) * mp);
+    const double a = tm.J[I] * tm.ftb;
+    double cx, cy, cz;
+    cross3(m[j], m[j + 1], m[j + 2], tm.p[0], tm.p[1], tm.p[2], cx, cy, cz);
+    h[j] = a * (eps * cx + tm.xi_s * tm.p[0]);
+    h[j + 1] = a * (eps * cy + tm.xi_s * tm.p[1]);
+    h[j + 2] = a * (eps * cz + tm.xi_s * tm.p[2]);
+    e[I] = 0;
+  }
+}
+
+// Philox-4x32-10 (Salmon et al., SC'11), ten rounds with the Weyl key bumps
+void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * c[0];
+    const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c[2];
+    const uint32_t n0 = static_cast<uint32_t>(p1 >> 32) ^ c[1] ^ k0;
+    const uint32_t n2 = static_cast<uint32_t>(p0 >> 32) ^ c[3] ^ k1;
+    c[1] = static_cast<uint32_t>(p1);
+    c[3] = static_cast<uint32_t>(p0);
+    c[0] = n0;
+    c[2] = n2;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+// stochastic_field_kernel!  src/micro/kernels.jl:469-494 with eta of step
+// th_cur_step drawn per cell from Philox((cell, step), seed) + Box-Muller;
+// factor = 2 alpha k_B scaling / (V gamma dt)  (src/micro/field.jl:244-280)
+void thermal_field(const Sim& s, const Term& tm, const double* m, double* h, double* e) {
+  const Mesh& g = s.mesh;
+  const double factor = 2 * s.alpha * tm.kB * tm.scaling / (g.volume * s.gamma * s.th_cur_dt);
+  const uint64_t n = static_cast<uint64_t>(s.th_cur_step);
+  const double s32 = 2.3283064365386963e-10;
+  for (int64_t I = 0; I < g.n; ++I) {
+    const int64_t j = 3 * I;
+    const double Ms = s.mu0Ms[I];
+    if (Ms > 0) {
+      uint32_t c[4] = {static_cast<uint32_t>(I), static_cast<uint32_t>(static_cast<uint64_t>(I) >> 32),
+                       static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32)};
+      philox4x32_10(c, static_cast<uint32_t>(tm.seed), static_cast<uint32_t>(tm.seed >> 32));
+      const double r0 = std::sqrt(-2.0 * std::log((double(c[0]) + 1.0) * s32));
+      const double r1 = std::sqrt(-2.0 * std::log((double(c[2]) + 1.0) * s32));
+      const double t0 = 6.283185307179586 * (double(c[1]) * s32), t1 = 6.283185307179586 * (double(c[3]) * s32);
+      const double scale = std::sqrt(factor * (tm.T[I] + tm.T0) / Ms);
+      h[j] = r0 * std::cos(t0) * scale;
+      h[j + 1] = r0 * std::sin(t0) * scale;
+      h[j + 2] = r1 * std::cos(t1) * scale;
+      e[I] = -Ms * g.volume * (m[j] * h[j] + m[j + 1] * h[j + 1] + m[j + 2] * h[j + 2]);
+    } else {
+      h[j] = h[j + 1] = h[j + 2] = 0;
+      e[I] = 0;
+    }
+  }
+}
+
 void term_eval(const Sim& s, Term& tm, const double* m) {
   double* h = tm.field.data();
   double* e = tm.energy.data();
@@ -552,6 +701,11 @@ void term_eval(const Sim& s, Term& tm, const double* m) {
     case T_DMI_INTERFACIAL: dmi_interfacial(s, tm, m, h, e); break;
     case T_ANIS: anis_uniaxial(s, tm, m, h, e); break;
     case T_DEMAG: demag_field(s, tm, m, h, e); break;
+    case T_DMI_BULK_SPATIAL: dmi_bulk_spatial(s, tm, m, h, e); break;
+    case T_SOT: sot_field(s, tm, m, h, e); break;
+    case T_STT_ZL: zhangli_field(s, tm, m, h, e); break;
+    case T_STT_SL: slonczewski_field(s, tm, m, h, e); break;
+    case T_THERMAL: thermal_field(s, tm, m, h, e); break;
   }
 }
 
@@ -606,7 +760,16 @@ void normalise(double* a, int64_t n) {
 }
 
 // advance_step(sim, ::RungeKutta)  src/integrator/rk.jl:23-52
+// evaluations outside a step draw the thermal field of the fixed-step
+// counter with the last fixed step (or the add-time dt)
+void standalone_context(Sim& s) {
+  s.th_cur_step = s.th_step;
+  s.th_cur_dt = s.th_dt;
+}
+
 void rk4_step(Sim& s, double h) {
+  s.th_cur_step = s.th_step;
+  s.th_cur_dt = h;
   const int64_t n3 = 3 * s.mesh.n;
   std::vector<double>& k1 = s.ks[0];
   std::vector<double>& k2 = s.ks[1];
@@ -627,11 +790,14 @@ void rk4_step(Sim& s, double h) {
   normalise(m, s.mesh.n);
   s.rk_nsteps += 1;
   s.rk_t = s.rk_nsteps * h;
+  s.th_step += 1;
 }
 
 // advance_step(sim, ::ModifiedEuler)  src/integrator/heun.jl:28-49
 // (vector_add2 / vector_add3 of src/util.jl)
 void heun_step(Sim& s, double h) {
+  s.th_cur_step = s.th_step;
+  s.th_cur_dt = h;
   const int64_t n3 = 3 * s.mesh.n;
   std::vector<double>& k1 = s.ks[0];
   std::vector<double>& k2 = s.ks[1];
@@ -644,6 +810,7 @@ void heun_step(Sim& s, double h) {
   normalise(m, s.mesh.n);
   s.rk_nsteps += 1;
   s.rk_t = s.rk_nsteps * h;
+  s.th_step += 1;
 }
 
 // rk_step_dopri54!  src/integrator/adaptive_rk_steps.jl:49-... (vector_add2..6b
@@ -806,6 +973,9 @@ double six_stage_attempt(Sim& s, double step, const SixStage& tb) {
 
 // method-specific step function  src/integrator/adaptive_rk.jl:67-89
 double rk_attempt(Sim& s, double step, double t) {
+  // the thermal field is redrawn when integrator.nsteps advances (src/micro/field.jl:250-253)
+  s.th_cur_step = s.nsteps;
+  s.th_cur_dt = step;
   switch (s.method) {
     case 1: return bs23_attempt(s, step, t);
     case 2: return six_stage_attempt(s, step, kCashKarp54);
@@ -822,6 +992,8 @@ int order_embedded(const Sim& s) { return s.method == 1 ? 2 : 4; }
 double compute_initial_step(Sim& s, double dt) {
   double abs_step = dt, abs_step_tmp = dt;
   s.step = 1e-15;
+  s.th_cur_step = s.nsteps;  // the rhs sees integrator.step = 1e-15
+  s.th_cur_dt = s.step;
   llg_rhs(s, s.y_temp.data(), s.y_current.data());
   double mx = 0.0;
   for (double v : s.y_temp) mx = std::max(mx, std::fabs(v));
@@ -1053,6 +1225,57 @@ int orc_add_dmi_interfacial(void* h, const double* D) {
   return static_cast<int>(s->terms.size()) - 1;
 }
 
+int orc_add_dmi_bulk_spatial(void* h, const double* Dx, const double* Dy, const double* Dz) {
+  Sim* s = static_cast<Sim*>(h);
+  Term* t = new_term(s, T_DMI_BULK_SPATIAL);
+  const int64_t n = s->mesh.n;
+  t->bD[0].assign(Dx, Dx + n); t->bD[1].assign(Dy, Dy + n); t->bD[2].assign(Dz, Dz + n);
+  return static_cast<int>(s->terms.size()) - 1;
+}
+
+int orc_add_sot(void* h, const double* aj, double bj, double px, double py, double pz) {
+  Sim* s = static_cast<Sim*>(h);
+  Term* t = new_term(s, T_SOT);
+  t->aj.assign(aj, aj + s->mesh.n);
+  t->bj = bj; t->p[0] = px; t->p[1] = py; t->p[2] = pz;
+  return static_cast<int>(s->terms.size()) - 1;
+}
+
+int orc_add_stt_zhang_li(void* h, const double* bJ, const double* xi, double ft) {
+  Sim* s = static_cast<Sim*>(h);
+  Term* t = new_term(s, T_STT_ZL);
+  t->bJ.assign(bJ, bJ + 3 * s->mesh.n);
+  t->xi.assign(xi, xi + s->mesh.n);
+  t->ft = ft;
+  return static_cast<int>(s->terms.size()) - 1;
+}
+
+int orc_add_stt_slonczewski(void* h, const double* J, double ftb, double Lambda, double P, double xi, double px,
+                            double py, double pz) {
+  Sim* s = static_cast<Sim*>(h);
+  Term* t = new_term(s, T_STT_SL);
+  t->J.assign(J, J + s->mesh.n);
+  t->ftb = ftb; t->Lambda = Lambda; t->P = P; t->xi_s = xi;
+  t->p[0] = px; t->p[1] = py; t->p[2] = pz;
+  return static_cast<int>(s->terms.size()) - 1;
+}
+
+int orc_add_thermal_noise(void* h, const double* T, double T0, double scaling, double kB, uint64_t seed, double dt) {
+  Sim* s = static_cast<Sim*>(h);
+  Term* t = new_term(s, T_THERMAL);
+  t->T.assign(T, T + s->mesh.n);
+  t->T0 = T0; t->scaling = scaling; t->kB = kB; t->seed = seed; t->dt = dt;
+  s->th_dt = dt;
+  return static_cast<int>(s->terms.size()) - 1;
+}
+
+// Philox-4x32-10 of one counter block (test access)
+void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+  philox4x32_10(c, key[0], key[1]);
+  for (int i = 0; i < 4; ++i) out[i] = c[i];
+}
+
 // add_anis  src/micro/add_field.jl:430-465 (axis normalised at add time)
 int orc_add_anis(void* h, const double* Ku, double ux, double uy, double uz) {
   Sim* s = static_cast<Sim*>(h);
@@ -1101,6 +1324,7 @@ void orc_demag_tensor(int nx, int ny, int nz, double dx, double dy, double dz, i
 
 // Evaluate one term on m (or on the stored m if m == null); field 3N, energy N.
 int orc_term_field(void* h, int idx, const double* m, double* field, double* energy) {
+  standalone_context(*static_cast<Sim*>(h));
   Sim* s = static_cast<Sim*>(h);
   if (idx < 0 || idx >= static_cast<int>(s->terms.size())) { g_err = "bad term"; return -1; }
   Term& t = *s->terms[idx];
@@ -1112,6 +1336,7 @@ int orc_term_field(void* h, int idx, const double* m, double* field, double* ene
 
 // Aggregated H_eff (field.jl:496-505) on m (or stored m).
 void orc_effective_field(void* h, const double* m, double* field) {
+  standalone_context(*static_cast<Sim*>(h));
   Sim* s = static_cast<Sim*>(h);
   effective_field(*s, m ? m : s->m.data());
   if (field) std::copy(s->field.begin(), s->field.end(), field);
@@ -1119,12 +1344,14 @@ void orc_effective_field(void* h, const double* m, double* field) {
 
 // dm/dt = llg_call_back(sim, dm_dt, m, t)
 void orc_llg_rhs(void* h, const double* m, double* dmdt) {
+  standalone_context(*static_cast<Sim*>(h));
   Sim* s = static_cast<Sim*>(h);
   llg_rhs(*s, dmdt, m ? m : s->m.data());
 }
 
 // compute_system_energy  field.jl:520-536: total and per-term energies
 double orc_energy(void* h, double* per_term) {
+  standalone_context(*static_cast<Sim*>(h));
   Sim* s = static_cast<Sim*>(h);
   double total = 0.0;
   for (size_t i = 0; i < s->terms.size(); ++i) {
@@ -1140,6 +1367,7 @@ double orc_energy(void* h, double* per_term) {
 
 void orc_rk4(void* h, double dt, int64_t nsteps) {
   Sim* s = static_cast<Sim*>(h);
+  s->th_dt = dt;
   for (int64_t i = 0; i < nsteps; ++i) rk4_step(*s, dt);
 }
 
@@ -1147,6 +1375,7 @@ double orc_rk4_time(void* h) { return static_cast<Sim*>(h)->rk_t; }
 
 void orc_heun(void* h, double dt, int64_t nsteps) {
   Sim* s = static_cast<Sim*>(h);
+  s->th_dt = dt;
   for (int64_t i = 0; i < nsteps; ++i) heun_step(*s, dt);
 }
 
@@ -1203,6 +1432,7 @@ int orc_dopri_advance(void* h, double* stats) {
 // with Dormand-Prince (driver=1).  Returns the number of steps run; *max_dmdt
 // receives the last max_dmdt / dmdt_factor.
 int64_t orc_relax(void* h, int driver, int64_t max_steps, double stopping_dmdt, double* max_dmdt_out) {
+  standalone_context(*static_cast<Sim*>(h));
   Sim* s = static_cast<Sim*>(h);
   const double time_factor = 2.21e5 / 2;
   const double dmdt_factor = (2 * kPi / 360) * 1e9;

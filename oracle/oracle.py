@@ -67,6 +67,14 @@ def lib():
         L.orc_dopri_advance.argtypes = [vp, _dp]
         L.orc_relax.argtypes = [vp, ctypes.c_int, ctypes.c_int64, ctypes.c_double, _dp]
         L.orc_relax.restype = ctypes.c_int64
+        d = ctypes.c_double
+        L.orc_add_dmi_bulk_spatial.argtypes = [vp, _dp, _dp, _dp]
+        L.orc_add_sot.argtypes = [vp, _dp, d, d, d, d]
+        L.orc_add_stt_zhang_li.argtypes = [vp, _dp, _dp, d]
+        L.orc_add_stt_slonczewski.argtypes = [vp, _dp, d, d, d, d, d, d, d]
+        L.orc_add_thermal_noise.argtypes = [vp, _dp, d, d, d, ctypes.c_uint64, d]
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        L.orc_philox.argtypes = [u32p, u32p, u32p]
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_max_threads.restype = ctypes.c_int
         L.orc_last_error.restype = ctypes.c_char_p
@@ -163,6 +171,24 @@ class OracleSim:
         t = None if tensor is None else np.ascontiguousarray(np.asarray(tensor, dtype=np.float64).reshape(-1))
         return lib().orc_add_demag(self.h, Nx, Ny, Nz, _ptr(t))
 
+    def add_dmi_bulk_spatial(self, Dx, Dy, Dz):
+        return lib().orc_add_dmi_bulk_spatial(self.h, _ptr(self._vec(Dx, 1)), _ptr(self._vec(Dy, 1)),
+                                              _ptr(self._vec(Dz, 1)))
+
+    def add_sot(self, aj, bj, p):
+        return lib().orc_add_sot(self.h, _ptr(self._vec(aj, 1)), float(bj), *map(float, p))
+
+    def add_stt_zhang_li(self, bJ, xi, ft=1.0):
+        return lib().orc_add_stt_zhang_li(self.h, _ptr(self._vec(bJ, 3)), _ptr(self._vec(xi, 1)), float(ft))
+
+    def add_stt_slonczewski(self, J, ft_beta, Lambda, P, xi, p):
+        return lib().orc_add_stt_slonczewski(self.h, _ptr(self._vec(J, 1)), float(ft_beta), float(Lambda), float(P),
+                                             float(xi), *map(float, p))
+
+    def add_thermal_noise(self, T, T0=0.0, scaling=1.0, k_B=1.3806505e-23, seed=0, dt=1e-14):
+        return lib().orc_add_thermal_noise(self.h, _ptr(self._vec(T, 1)), float(T0), float(scaling), float(k_B),
+                                           int(seed), float(dt))
+
     def term_field(self, idx, m=None):
         f = np.zeros(3 * self.n)
         e = np.zeros(self.n)
@@ -219,3 +245,12 @@ class OracleSim:
         out = np.zeros(1)
         steps = lib().orc_relax(self.h, 0 if driver == "SD" else 1, int(max_steps), float(stopping_dmdt), _ptr(out))
         return int(steps), float(out[0])
+
+
+def philox(counter, key):
+    """Philox-4x32-10 of one 4-word counter block with a 2-word key."""
+    c = (ctypes.c_uint32 * 4)(*counter)
+    k = (ctypes.c_uint32 * 2)(*key)
+    o = (ctypes.c_uint32 * 4)()
+    lib().orc_philox(c, k, o)
+    return list(o)

@@ -65,11 +65,42 @@ def build_oracle(cfg, tensor=None):
             idx[t] = s.add_zeeman(cfg["H"])
         elif t == "demag":
             idx[t] = s.add_demag(*cfg.get("macro", (0, 0, 0)), tensor=tensor)
+        elif t == "dmi_bulk_sp":
+            idx[t] = s.add_dmi_bulk_spatial(*cfg["bD"])
+        elif t == "sot":
+            idx[t] = s.add_sot(cfg["aj"], cfg["bj"], cfg["p"])
+        elif t == "stt_zl":
+            idx[t] = s.add_stt_zhang_li(cfg["bJ"], cfg["xi"], cfg["ft"])
+        elif t == "stt_sl":
+            idx[t] = s.add_stt_slonczewski(cfg["J"], cfg["ftb"], cfg["Lambda"], cfg["P"], cfg["xi_s"], cfg["p_sl"])
+        elif t == "thermal":
+            idx[t] = s.add_thermal_noise(cfg["T"], cfg["T0"], cfg["scaling"], seed=cfg["seed"], dt=cfg["th_dt"])
     assert len(idx) == len(cfg["terms"]) and n > 0
     return s, idx
 
 
-TERM_ID = {"zeeman": 0, "exch": 1, "dmi_bulk": 2, "dmi_int": 3, "anis": 4, "demag": 5}
+def extra_config(seed, nx, ny, nz, pbc="", terms=("exch", "dmi_bulk_sp", "sot", "stt_zl", "stt_sl", "thermal")):
+    """random_config plus the parameters of the further terms."""
+    cfg = random_config(seed, nx, ny, nz, pbc, terms=terms)
+    rng = np.random.default_rng(seed + 1000)
+    n = nx * ny * nz
+    cfg["bD"] = tuple(rng.uniform(1e-3, 4e-3, n) for _ in range(3))
+    cfg["bD"][1][rng.random(n) < 0.1] = 0.0
+    cfg["aj"] = rng.uniform(5e8, 2e9, n)
+    cfg["bj"] = 3e8
+    cfg["p"] = (0.1, 0.2, 0.3)
+    cfg["bJ"] = rng.uniform(-50, 50, 3 * n)
+    cfg["xi"] = rng.uniform(0.0, 0.2, n)
+    cfg["ft"] = 0.7
+    cfg["J"] = rng.uniform(5e10, 2e11, n)
+    cfg["ftb"], cfg["Lambda"], cfg["P"], cfg["xi_s"], cfg["p_sl"] = 2.5e-12, 2.0, 0.4, 0.05, (0.0, 0.6, 0.8)
+    cfg["T"] = rng.uniform(100, 400, n)
+    cfg["T0"], cfg["scaling"], cfg["seed"], cfg["th_dt"] = 20.0, 0.8, 987654321, 2e-14
+    return cfg
+
+
+TERM_ID = {"zeeman": 0, "exch": 1, "dmi_bulk": 2, "dmi_int": 3, "anis": 4, "demag": 5, "dmi_bulk_sp": 2, "sot": 6,
+           "stt_zl": 7, "stt_sl": 8, "thermal": 9}
 
 
 class GpuSim:
@@ -109,6 +140,19 @@ class GpuSim:
                     c("mm_add_demag_tensor", dp(np.ascontiguousarray(tensor, dtype=np.float64).reshape(-1)))
                 else:
                     c("mm_add_demag", *cfg.get("macro", (0, 0, 0)))
+            elif t == "dmi_bulk_sp":
+                c("mm_add_dmi_bulk_spatial", *(dp(np.ascontiguousarray(x, dtype=np.float64)) for x in cfg["bD"]))
+            elif t == "sot":
+                c("mm_add_sot", dp(np.ascontiguousarray(cfg["aj"], dtype=np.float64)), 0.0, cfg["bj"], *cfg["p"])
+            elif t == "stt_zl":
+                c("mm_add_stt_zhang_li", dp(np.ascontiguousarray(cfg["bJ"], dtype=np.float64)),
+                  dp(np.ascontiguousarray(cfg["xi"], dtype=np.float64)), 0.0, cfg["ft"])
+            elif t == "stt_sl":
+                c("mm_add_stt_slonczewski", dp(np.ascontiguousarray(cfg["J"], dtype=np.float64)), 0.0, cfg["ftb"],
+                  cfg["Lambda"], cfg["P"], cfg["xi_s"], *cfg["p_sl"])
+            elif t == "thermal":
+                c("mm_add_thermal_noise", dp(np.ascontiguousarray(cfg["T"], dtype=np.float64)), 0.0, cfg["T0"],
+                  cfg["scaling"], 1.3806505e-23, cfg["seed"], cfg["th_dt"])
 
     def term_field(self, name):
         f = np.empty(3 * self.n)

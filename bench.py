@@ -477,6 +477,10 @@ def run_native(args):
         lps = h.rk4_launches() // 2 if heun else h.rk4_launches()
         res = {"ms_per_step": ms_max / args.steps, "value": ws * n * args.steps / (ms_max / 1e3),
                "launches_per_step": lps, "device_bytes": h.device_bytes()}
+        if w["demag"]:
+            tiles = (ctypes.c_int * 5)()
+            h.call("mm_demag_tiles", tiles, None)
+            res["tiles"] = list(tiles)
         if sampler:
             res["clocks"] = sampler.summary()
         if args.quick:
@@ -555,6 +559,7 @@ def run_native(args):
                                    + (" + zeeman" if w["zeeman"] else "") + " + demag, "
                                    + ("Heun" if heun else "RK4") + " dt=%g" % dt,
                        "form": "fp32 (compensated RK state; fp64 tensor/energies)",
+                       "demag_tiles_autotuned": r.get("tiles"),
                        "parallelism": f"replicas x{ws}", "l2": "working set > 126 MB L2 (inputs larger than L2)"},
             "e2e": r["e2e"],
             "gpu_launches": r["launches_per_step"] * args.steps,

@@ -169,6 +169,12 @@ typedef enum {
  * resets the adaptive state as a new Sim would (default MM_RK_DORMAND_PRINCE). */
 int mm_set_adaptive_method(mm_handle* h, int method);
 
+/* Tile widths (kx columns per block) the autotuner chose for the demag
+ * passes 0..4 (0: not tuned / static rule) and their timed milliseconds per
+ * launch; measurement hook, no reference counterpart.  Set MMCUDA_AUTOTUNE=0
+ * to keep the static rule. */
+int mm_demag_tiles(mm_handle* h, int* tiles5, float* ms5);
+
 /* ---- Further terms --------------------------------------------------------
  * Evaluated in the same fused per-cell kernel (a variant compiled with them,
  * so handles without them keep the base kernel).  Array arguments are per

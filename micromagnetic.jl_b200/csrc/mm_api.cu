@@ -77,6 +77,7 @@ class EngineBase {
   virtual int add_dmi_interfacial(const double* D, double uni) = 0;
   virtual int add_anis(const double* Ku, double uni, double ax, double ay, double az) = 0;
   virtual int add_dmi_bulk_spatial(const double* Dx, const double* Dy, const double* Dz) = 0;
+  virtual int demag_tiles(int* tiles, float* ms) = 0;
   virtual int add_sot(const double* aj, double aj_uni, double bj, double px, double py, double pz) = 0;
   virtual int add_stt_zhang_li(const double* bJ, const double* xi, double xi_uni, double ft) = 0;
   virtual int add_stt_slonczewski(const double* J, double J_uni, double ft_beta, double Lambda, double P, double xi,
@@ -294,6 +295,15 @@ class Engine : public EngineBase {
     return MM_OK;
   }
 
+  int demag_tiles(int* tiles, float* ms) override {
+    if (!demag) return fail(MM_ERR_STATE, "no demag term");
+    for (int i = 0; i < 5; ++i) {
+      if (tiles) tiles[i] = demag->tile[i];
+      if (ms) ms[i] = demag->tile_ms[i];
+    }
+    return MM_OK;
+  }
+
   // add_sot(sim, aj, bj, p)  src/micro/add_field.jl:951-966 (DFTorqueField)
   int add_sot(const double* ajh, double aj_uni, double bj, double px, double py, double pz) override {
     if (mask & TB_SOT) return fail(MM_ERR_UNSUPPORTED, "one SOT term per handle");
@@ -444,6 +454,8 @@ class Engine : public EngineBase {
     cudaFree(T);
     if (rc) return fail(MM_ERR_CUDA, "demag tensor assembly failed: %s", cudaGetErrorString(static_cast<cudaError_t>(rc)));
     if (!Hd && (rc = alloc(Hd, 3 * N))) return rc;
+    // tile widths of the strided passes, timed on this plan's own buffers
+    if ((rc = plan->autotune(m, Ms, Hd, st_))) return fail(MM_ERR_CUDA, "demag tile autotuning failed (%d)", rc);
     demag = std::move(plan);
     mask |= TB_DEMAG;
     ++version;
@@ -1492,6 +1504,11 @@ int mm_run_until(mm_handle* h, double t, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h
 int mm_advance_step(mm_handle* h, mm_stats* s) { MM_HANDLE(h); MM_GUARD(h->eng->advance_step(s)); }
 int mm_dopri_reset(mm_handle* h) { MM_HANDLE(h); MM_GUARD(h->eng->dopri_reset()); }
 int mm_set_adaptive_method(mm_handle* h, int method) { MM_HANDLE(h); MM_GUARD(h->eng->set_method(method)); }
+
+int mm_demag_tiles(mm_handle* h, int* tiles, float* ms) {
+  MM_HANDLE(h);
+  MM_GUARD(h->eng->demag_tiles(tiles, ms));
+}
 
 int mm_add_dmi_bulk_spatial(mm_handle* h, const double* Dx, const double* Dy, const double* Dz) {
   MM_HANDLE(h);

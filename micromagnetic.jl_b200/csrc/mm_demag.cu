@@ -1,5 +1,9 @@
 // mm_demag.cu -- demag tensor assembly (FP64) and FFT convolution passes.
 #include <algorithm>
+#include <tuple>
+#include <mutex>
+#include <map>
+#include <array>
 #include <cstdlib>
 #include <cmath>
 #include <cstring>
@@ -817,13 +821,37 @@ static int lines_tile(int Hx, int L, int lines_per_col, int nbuf) {
   return W;
 }
 
+// shared memory of one block of a strided pass with tile width W (bytes)
+template <typename R>
+static size_t pass_smem(const DemagGeom& g, int which, bool fused2d, int W) {
+  using C = cplx_t<R>;
+  if (which == 1 || which == 3) return static_cast<size_t>(std::max(1, line_fft_buffers(g.ply))) * sizeof(C) * W * (g.Py | 1);
+  if (fused2d) return 2 * sizeof(C) * 3 * W * (g.Py | 1);
+  const bool zc2 = (g.Pz & (g.Pz - 1)) == 0 && g.Pz >= 4 && (g.Pz <= 128 || (sizeof(R) == 4 && g.Pz == 256));
+  return (zc2 ? 1 : 2) * sizeof(C) * 3 * W * (g.Pz | 1);
+}
+
+// first radix of the fused-middle z kernel (W * RA threads carry the middle)
+static int zconv2_ra(int Pz) {
+  switch (Pz) {
+    case 4: return 2;
+    case 8: return 4;
+    case 16: return 4;
+    case 32: return 8;
+    case 64: return 8;
+    case 128: return 16;
+    case 256: return 32;
+    default: return 0;
+  }
+}
+
 template <typename R, int MODE>
 static void launch_ylines(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* out, const R* Nhat,
-                          const cplx_t<R>* twy, cudaStream_t st) {
+                          const cplx_t<R>* twy, cudaStream_t st, int Wforce = 0) {
   using C = cplx_t<R>;
   const int ncompc = MODE == YL_CONV2D ? 3 : 1;
   const int nbuf = MODE == YL_CONV2D ? 2 : line_fft_buffers(g.ply);
-  const int W = lines_tile<R>(g.Hx, g.Py, ncompc, nbuf);
+  const int W = Wforce > 0 ? Wforce : lines_tile<R>(g.Hx, g.Py, ncompc, nbuf);
   const int half = ncompc * W * (g.Py | 1);
   dim3 grid((g.Hx + W - 1) / W, g.nz, 3 / ncompc);
   const size_t sm = static_cast<size_t>(std::max(1, nbuf)) * sizeof(C) * half;
@@ -836,10 +864,11 @@ static void launch_ylines(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* ou
 }
 
 template <typename R, int RA, int RB>
-static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st) {
+static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st,
+                          int Wforce) {
   using C = cplx_t<R>;
   constexpr int L = RA * RB;
-  int W = lines_tile<R>(g.Hx, L, 3, 1);
+  int W = Wforce > 0 ? Wforce : lines_tile<R>(g.Hx, L, 3, 1);
   while (W * RA > kHotNT) W /= 2;
   const size_t sm = sizeof(C) * 3 * W * (L | 1);
   static uint64_t done = 0;
@@ -859,17 +888,18 @@ static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const
 
 // Power-of-two z lengths with a fused-middle kernel: L = RA * RB
 template <typename R>
-static bool try_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st) {
+static bool try_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st,
+                       int Wf) {
   switch (g.Pz) {
-    case 4: launch_zconv2<R, 2, 2>(g, Y, Nhat, twz, st); return true;
-    case 8: launch_zconv2<R, 4, 2>(g, Y, Nhat, twz, st); return true;
-    case 16: launch_zconv2<R, 4, 4>(g, Y, Nhat, twz, st); return true;
-    case 32: launch_zconv2<R, 8, 4>(g, Y, Nhat, twz, st); return true;
-    case 64: launch_zconv2<R, 8, 8>(g, Y, Nhat, twz, st); return true;
-    case 128: launch_zconv2<R, 16, 8>(g, Y, Nhat, twz, st); return true;
+    case 4: launch_zconv2<R, 2, 2>(g, Y, Nhat, twz, st, Wf); return true;
+    case 8: launch_zconv2<R, 4, 2>(g, Y, Nhat, twz, st, Wf); return true;
+    case 16: launch_zconv2<R, 4, 4>(g, Y, Nhat, twz, st, Wf); return true;
+    case 32: launch_zconv2<R, 8, 4>(g, Y, Nhat, twz, st, Wf); return true;
+    case 64: launch_zconv2<R, 8, 8>(g, Y, Nhat, twz, st, Wf); return true;
+    case 128: launch_zconv2<R, 16, 8>(g, Y, Nhat, twz, st, Wf); return true;
     case 256:
       if constexpr (sizeof(R) == 4) {
-        launch_zconv2<R, 32, 8>(g, Y, Nhat, twz, st);
+        launch_zconv2<R, 32, 8>(g, Y, Nhat, twz, st, Wf);
         return true;
       }
       return false;
@@ -878,10 +908,11 @@ static bool try_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cp
 }
 
 template <typename R>
-static void launch_zconv(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st) {
+static void launch_zconv(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st,
+                         int Wforce = 0) {
   using C = cplx_t<R>;
-  if (try_zconv2<R>(g, Y, Nhat, twz, st)) return;
-  const int W = lines_tile<R>(g.Hx, g.Pz, 3, 2);
+  if (try_zconv2<R>(g, Y, Nhat, twz, st, Wforce)) return;
+  const int W = Wforce > 0 ? Wforce : lines_tile<R>(g.Hx, g.Pz, 3, 2);
   const int half = 3 * W * (g.Pz | 1);
   dim3 grid((g.Hx + W - 1) / W, g.Py, 1);
   const size_t sm = 2 * sizeof(C) * half;
@@ -902,15 +933,15 @@ static bool run_pass(const DemagPlan<R>& p, DemagGeom g, int which, const R* m, 
       return true;
     case 1:
       if (p.fused2d) return false;
-      launch_ylines<R, YL_FWD>(g, p.X, p.Y, p.Nhat, p.twy, st);
+      launch_ylines<R, YL_FWD>(g, p.X, p.Y, p.Nhat, p.twy, st, p.tile[1]);
       return true;
     case 2:
-      if (p.fused2d) launch_ylines<R, YL_CONV2D>(g, p.X, p.X, p.Nhat, p.twy, st);
-      else launch_zconv<R>(g, p.Y, p.Nhat, p.twz, st);
+      if (p.fused2d) launch_ylines<R, YL_CONV2D>(g, p.X, p.X, p.Nhat, p.twy, st, p.tile[2]);
+      else launch_zconv<R>(g, p.Y, p.Nhat, p.twz, st, p.tile[2]);
       return true;
     case 3:
       if (p.fused2d) return false;
-      launch_ylines<R, YL_INV>(g, p.Y, p.X, p.Nhat, p.twy, st);
+      launch_ylines<R, YL_INV>(g, p.Y, p.X, p.Nhat, p.twy, st, p.tile[3]);
       return true;
     case 4: {
       const int lines = 3 * g.ny * g.nz;
@@ -939,6 +970,74 @@ void DemagPlan<R>::apply(const R* m, const R* mu0Ms, R* Hd, cudaStream_t st, con
 template <typename R>
 bool DemagPlan<R>::launch_pass(int which, const R* m, const R* mu0Ms, R* Hd, cudaStream_t st) {
   return run_pass(*this, this->g, which, m, mu0Ms, Hd, st);
+}
+
+// ---- tile autotuner ---------------------------------------------------------
+// For each strided pass the plan uses, time every valid tile width W (powers
+// of two up to a 128-byte row segment, within the 200 KB shared-memory limit
+// and, for the fused-middle z kernel, W * RA <= threads) on the plan's own
+// buffers and keep the fastest.  Results are cached per (form, mesh shape),
+// so a batch of equal meshes tunes once.  MMCUDA_AUTOTUNE=0 keeps the static
+// rule.
+struct TileKey {
+  int w, nx, ny, nz;
+  bool operator<(const TileKey& o) const {
+    return std::tie(w, nx, ny, nz) < std::tie(o.w, o.nx, o.ny, o.nz);
+  }
+};
+static std::mutex g_tile_mu;
+static std::map<TileKey, std::array<int, 5>> g_tile_cache;
+
+template <typename R>
+int DemagPlan<R>::autotune(const R* m, const R* mu0Ms, R* Hd, cudaStream_t st) {
+  using C = cplx_t<R>;
+  const char* env = getenv("MMCUDA_AUTOTUNE");
+  if (env && env[0] == '0') return 0;
+  const TileKey key{static_cast<int>(sizeof(R)), g.nx, g.ny, g.nz};
+  {
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    auto it = g_tile_cache.find(key);
+    if (it != g_tile_cache.end()) {
+      for (int i = 0; i < 5; ++i) tile[i] = it->second[i];
+      return 0;
+    }
+  }
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -1;
+  const int wmax = 128 / static_cast<int>(sizeof(C));
+  const int ra = zconv2_ra(g.Pz);
+  const bool zc2 = !fused2d && pass_smem<R>(g, 2, false, 1) == sizeof(C) * 3 * (g.Pz | 1);
+  for (int which = 1; which <= 3; ++which) {
+    if (fused2d && which != 2) continue;
+    float best = 1e30f;
+    int bestW = 0;
+    for (int W = 1; W <= wmax; W *= 2) {
+      if (W / 2 >= g.Hx) break;
+      if (pass_smem<R>(g, which, fused2d, W) > 200 * 1024) break;
+      if (which == 2 && zc2 && W * ra > kHotNT) break;
+      tile[which] = W;
+      for (int r = 0; r < 2; ++r) run_pass(*this, g, which, m, mu0Ms, Hd, st);
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < 5; ++r) run_pass(*this, g, which, m, mu0Ms, Hd, st);
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms <= best) {
+        best = ms;
+        bestW = W;
+      }
+    }
+    tile[which] = bestW;
+    tile_ms[which] = best / 5;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return static_cast<int>(err);
+  std::lock_guard<std::mutex> lk(g_tile_mu);
+  g_tile_cache[key] = {tile[0], tile[1], tile[2], tile[3], tile[4]};
+  return 0;
 }
 
 template <typename R>

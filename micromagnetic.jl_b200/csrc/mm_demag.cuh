@@ -53,6 +53,14 @@ class DemagPlan {
   double pass_bytes(int which) const;
   size_t device_bytes() const { return bytes_; }
 
+  // Tile widths (kx columns per block) of the strided passes 1..3, chosen by
+  // autotune(); 0 keeps the static rule (largest W whose tile fits the
+  // shared-memory budget).  Any W gives bit-identical results: each line is
+  // transformed by the same arithmetic whatever block it lands in.
+  int autotune(const R* m, const R* mu0Ms, R* Hd, cudaStream_t st);
+  int tile[5] = {0, 0, 0, 0, 0};
+  float tile_ms[5] = {0, 0, 0, 0, 0};
+
   DemagGeom g{};
   bool fused2d = false;
   C* X = nullptr;

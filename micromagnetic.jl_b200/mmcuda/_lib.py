@@ -45,7 +45,7 @@ EXPORTS = (
     "mm_energy_noalloc", "mm_batch_create", "mm_batch_rk4_run", "mm_batch_get_stream", "mm_batch_destroy",
     "mm_heun_run", "mm_set_adaptive_method", "mm_ovf_write", "mm_ovf_read_header", "mm_ovf_read",
     "mm_save_ovf", "mm_load_ovf", "mm_adjoint_record", "mm_adjoint_backward", "mm_add_dmi_bulk_spatial",
-    "mm_add_sot", "mm_add_stt_zhang_li", "mm_add_stt_slonczewski", "mm_add_thermal_noise",
+    "mm_add_sot", "mm_add_stt_zhang_li", "mm_add_stt_slonczewski", "mm_add_thermal_noise", "mm_demag_tiles",
 )
 KERNELS = ("demag_fwd_x", "demag_fwd_y", "demag_conv", "demag_inv_y", "demag_inv_x", "rk4_stage", "rk4_step")
 
@@ -123,6 +123,7 @@ def load():
         "mm_load_ovf": ([_vp, ctypes.c_char_p], i),
         "mm_adjoint_record": ([_vp, d, i64, i64], i),
         "mm_add_dmi_bulk_spatial": ([_vp, _dp, _dp, _dp], i),
+        "mm_demag_tiles": ([_vp, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_float)], i),
         "mm_add_sot": ([_vp, _dp, d, d, d, d, d], i),
         "mm_add_stt_zhang_li": ([_vp, _dp, _dp, d, d], i),
         "mm_add_stt_slonczewski": ([_vp, _dp, d, d, d, d, d, d, d, d], i),

@@ -27,6 +27,7 @@ template <typename R, int NT> struct PassCfg {
   static constexpr int minb = NT == 256 ? 3 : 1;
 };
 constexpr int kHotNT = 256;
+constexpr size_t kMaxSmem = 227 * 1024;  // dynamic shared memory per block (opt-in maximum)
 constexpr int kTensorNT = 512;
 template <typename R> constexpr int hot_cap() { return PassCfg<R, kHotNT>::cap; }
 constexpr int tensor_cap() { return PassCfg<double, kTensorNT>::cap; }
@@ -667,7 +668,7 @@ static C* upload_twiddles(int L, size_t& bytes, cudaStream_t st) {
 
 template <typename R, int NT>
 static void set_smem_attrs_nt() {
-  const int mx = 200 * 1024;
+  const int mx = static_cast<int>(kMaxSmem);
   cudaFuncSetAttribute(k_fwd_x<R, XM_MAGN, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_fwd_x<R, XM_TENSOR, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_inv_x<R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
@@ -720,12 +721,18 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
   g.Hx = g.Px > 1 ? g.Lc + 1 : 1;
   g.Tyq = g.Py / 2 + 1;
   g.Tzq = g.Pz / 2 + 1;
-  // every hot pass (single-component lines; 3-component z lines) and every
-  // FP64 tensor pass must fit one block
-  const int cap = std::min(hot_cap<R>(), tensor_cap());
-  if (g.Lc > cap || g.Py > cap || 3 * g.Pz > cap) {
-    snprintf(err, nerr, "demag: mesh %dx%dx%d exceeds the FFT pass limits (padded x/2 <= %d, padded y <= %d, padded z <= %d)",
-             nx, ny, nz, cap, cap, cap / 3);
+  // one line (x, y; the three components of a z line) with its ping-pong
+  // buffer must fit one block's shared memory, in the FP64 tensor passes too
+  const size_t c64 = sizeof(double2), cR = sizeof(C);
+  const bool fit_x = 2 * c64 * static_cast<size_t>(g.Lc | 1) <= kMaxSmem;
+  const bool fit_y = 2 * c64 * static_cast<size_t>(g.Py | 1) <= kMaxSmem;
+  const bool fit_z = 2 * c64 * static_cast<size_t>(g.Pz | 1) <= kMaxSmem &&
+                     2 * 3 * cR * static_cast<size_t>(g.Pz | 1) <= kMaxSmem;
+  if (!fit_x || !fit_y || !fit_z) {
+    const int lmax = static_cast<int>(kMaxSmem / (2 * c64)) - 1;
+    snprintf(err, nerr,
+             "demag: mesh %dx%dx%d exceeds the FFT pass limits (padded x/2 <= %d, padded y <= %d, padded z <= %d)",
+             nx, ny, nz, lmax, lmax, static_cast<int>(kMaxSmem / (6 * cR)) - 1);
     return -1;
   }
   const int maxr = sizeof(R) == 4 ? 32 : 8;
@@ -875,8 +882,8 @@ static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const
   int dev = 0;
   cudaGetDevice(&dev);
   if (!((done >> dev) & 1ull)) {
-    cudaFuncSetAttribute(k_zconv2<R, RA, RB, kHotNT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_zconv2<R, RA, RB, kHotNT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_zconv2<R, RA, RB, kHotNT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
+    cudaFuncSetAttribute(k_zconv2<R, RA, RB, kHotNT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
     done |= 1ull << dev;
   }
   dim3 grid((g.Hx + W - 1) / W, g.Py, 1);
@@ -1013,7 +1020,7 @@ int DemagPlan<R>::autotune(const R* m, const R* mu0Ms, R* Hd, cudaStream_t st) {
     int bestW = 0;
     for (int W = 1; W <= wmax; W *= 2) {
       if (W / 2 >= g.Hx) break;
-      if (pass_smem<R>(g, which, fused2d, W) > 200 * 1024) break;
+      if (pass_smem<R>(g, which, fused2d, W) > kMaxSmem) break;
       if (which == 2 && zc2 && W * ra > kHotNT) break;
       tile[which] = W;
       for (int r = 0; r < 2; ++r) run_pass(*this, g, which, m, mu0Ms, Hd, st);

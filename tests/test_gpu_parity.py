@@ -86,6 +86,27 @@ def test_demag_newell_fp64(mesh):
     assert rel_maxnorm(fg, fo) <= TENSOR_TOL, rel_maxnorm(fg, fo)
 
 
+@pytest.mark.parametrize("form", [0, 1])
+@pytest.mark.parametrize("mesh", [(3000, 2, 1), (4, 1800, 1), (2, 3, 700), (6, 1100, 3)])
+def test_demag_long_lines(mesh, form):
+    """Padded lines beyond the multi-line tiles (one line per block): x/2 = 3000,
+    y = 3600, z = 1400 and y = 2200 with z = 6 (the FP64 tensor passes and the
+    FP64 hot passes at their largest), FP64 to 1e-12 with the oracle's tensor,
+    the FP32 form to 1e-5."""
+    from oracle.oracle import demag_tensor
+
+    nx, ny, nz = mesh
+    cfg = random_config(17 + nx + ny + nz, nx, ny, nz, "", terms=("demag",))
+    T = demag_tensor(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, idx = build_oracle(cfg, tensor=T)
+    fo, _ = o.term_field(idx["demag"])
+    fg, _ = GpuSim(cfg, form=form, tensor=T).term_field("demag")
+    assert rel_maxnorm(fg, fo) <= (TOL64 if form == 0 else TOL32)
+    if form == 0:
+        fn, _ = GpuSim(cfg, form=0).term_field("demag")  # tensor assembled on the GPU
+        assert rel_maxnorm(fn, fo) <= TENSOR_TOL
+
+
 def test_demag_macro_pbc_fp64():
     cfg = random_config(5, 6, 5, 1, "", terms=("demag",))
     cfg["macro"] = (3, 2, 0)

@@ -52,6 +52,12 @@ WORKLOADS = {
     "fig9_4000": dict(nx=4000, ny=4000, nz=1, dx=4e-9, dy=4e-9, dz=4e-9, Ms=8e5, A=1e-13, Dbulk=None, Ku=None,
                       axis=(0, 0, 1), demag=True, alpha=0.01, gamma=2.211e5, dt=1e-14, seed=109, zeeman="y100mT",
                       integrator="heun", published=1.045e9),
+    "fig9_8000": dict(nx=8000, ny=8000, nz=1, dx=4e-9, dy=4e-9, dz=4e-9, Ms=8e5, A=1e-13, Dbulk=None, Ku=None,
+                      axis=(0, 0, 1), demag=True, alpha=0.01, gamma=2.211e5, dt=1e-14, seed=109, zeeman="y100mT",
+                      integrator="heun", published=1.069e9),
+    "fig9_10000": dict(nx=10000, ny=10000, nz=1, dx=4e-9, dy=4e-9, dz=4e-9, Ms=8e5, A=1e-13, Dbulk=None, Ku=None,
+                       axis=(0, 0, 1), demag=True, alpha=0.01, gamma=2.211e5, dt=1e-14, seed=109, zeeman="y100mT",
+                       integrator="heun", published=1.008e9),
 }
 # batched workloads: many meshes advanced by one graph launch per RK4 step
 BATCHES = {
@@ -68,7 +74,7 @@ ADJOINT = {"c4": dict(nx=128, ny=128, nz=4, dx=2e-9, A=1.3e-11, D=3e-3, Ku=4e5, 
                       dt=5e-14, nsteps=2000, ckpt=100, seed=104)}
 # the CPU baseline times a bounded block of the same physics
 CPU_SAMPLE = {"c2": (128, 128, 32), "c5": (256, 256, 16), "c1": (200, 50, 1), "fig9": (1000, 1000, 1),
-              "fig9_4000": (1000, 1000, 1)}
+              "fig9_4000": (1000, 1000, 1), "fig9_8000": (1000, 1000, 1), "fig9_10000": (1000, 1000, 1)}
 
 
 def synth_inputs(w, shape=None):

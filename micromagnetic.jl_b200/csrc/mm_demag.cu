@@ -704,6 +704,9 @@ template <typename R>
 DemagPlan<R>::~DemagPlan() {
   cudaFree(X);
   cudaFree(Y);
+  cudaFree(S);
+  cudaFree(Zx);
+  cudaFree(Zx2);
   cudaFree(Nhat);
   cudaFree(twx);
   cudaFree(twy);
@@ -723,16 +726,20 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
   g.Tzq = g.Pz / 2 + 1;
   // one line (x, y; the three components of a z line) with its ping-pong
   // buffer must fit one block's shared memory, in the FP64 tensor passes too
+  // x and y lines longer than one block holds (FP64 tensor passes included)
+  // run as global-memory stages; z lines must fit
   const size_t c64 = sizeof(double2), cR = sizeof(C);
-  const bool fit_x = 2 * c64 * static_cast<size_t>(g.Lc | 1) <= kMaxSmem;
-  const bool fit_y = 2 * c64 * static_cast<size_t>(g.Py | 1) <= kMaxSmem;
+  long_x = 2 * c64 * static_cast<size_t>(g.Lc | 1) > kMaxSmem;
+  long_y = 2 * c64 * static_cast<size_t>(g.Py | 1) > kMaxSmem;
   const bool fit_z = 2 * c64 * static_cast<size_t>(g.Pz | 1) <= kMaxSmem &&
                      2 * 3 * cR * static_cast<size_t>(g.Pz | 1) <= kMaxSmem;
-  if (!fit_x || !fit_y || !fit_z) {
-    const int lmax = static_cast<int>(kMaxSmem / (2 * c64)) - 1;
-    snprintf(err, nerr,
-             "demag: mesh %dx%dx%d exceeds the FFT pass limits (padded x/2 <= %d, padded y <= %d, padded z <= %d)",
-             nx, ny, nz, lmax, lmax, static_cast<int>(kMaxSmem / (6 * cR)) - 1);
+  if (!fit_z) {
+    snprintf(err, nerr, "demag: mesh %dx%dx%d exceeds the FFT pass limit (padded z <= %d)", nx, ny, nz,
+             static_cast<int>(kMaxSmem / (6 * cR)) - 1);
+    return -1;
+  }
+  if ((long_x && !make_fft_plan(g.Lc, gplx, 8)) || (long_y && !make_fft_plan(g.Py, gply, 8))) {
+    snprintf(err, nerr, "demag: no radix plan");
     return -1;
   }
   const int maxr = sizeof(R) == 4 ? 32 : 8;
@@ -750,7 +757,7 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
   g.frows = make_fastdiv(ny * nz);
   g.fpady = make_fastdiv(std::max(1, g.Py - ny));
   g.fpadz = make_fastdiv(std::max(1, g.Pz - nz));
-  fused2d = (g.Pz == 1) && (2 * 3 * (g.Py | 1) * sizeof(C) <= static_cast<size_t>(smem_budget_bytes()));
+  fused2d = !long_y && (g.Pz == 1) && (2 * 3 * (g.Py | 1) * sizeof(C) <= static_cast<size_t>(smem_budget_bytes()));
   set_smem_attrs<R>();
   set_smem_attrs<double>();
   const int64_t nX = 3LL * nz * ny * g.Hx;
@@ -760,6 +767,15 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
     const int64_t nY = 3LL * nz * g.Py * g.Hx;
     if (cudaMalloc(&Y, sizeof(C) * nY) != cudaSuccess) return 2;
     bytes_ += sizeof(C) * nY;
+    if (long_y) {
+      if (cudaMalloc(&S, sizeof(C) * nY) != cudaSuccess) return 2;
+      bytes_ += sizeof(C) * nY;
+    }
+  }
+  if (long_x) {
+    const int64_t nZ = 3LL * ny * nz * g.Lc;
+    if (cudaMalloc(&Zx, sizeof(C) * nZ) != cudaSuccess || cudaMalloc(&Zx2, sizeof(C) * nZ) != cudaSuccess) return 2;
+    bytes_ += 2 * sizeof(C) * nZ;
   }
   const int64_t nT = 6LL * g.Tzq * g.Tyq * g.Hx;
   if (cudaMalloc(&Nhat, sizeof(R) * nT) != cudaSuccess) return 2;
@@ -769,6 +785,255 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
   if (!(twy = upload_twiddles<C>(g.Py, bytes_, st))) return 2;
   if (!(twz = upload_twiddles<C>(g.Pz, bytes_, st))) return 2;
   return static_cast<int>(cudaGetLastError());
+}
+
+// ---- long lines: self-sorting Stockham stages through global memory -------
+// For lines longer than one block's shared memory holds (two buffers), each
+// radix stage is one launch that reads a whole spectrum array and writes the
+// other of a ping-pong pair: y lines of [cz][Py][Hx] arrays (element stride
+// Hx, the kx column fastest across threads) and x lines of [line][Lc] arrays
+// (element stride 1, the butterfly fastest).  Same butterflies, twiddles and
+// stage order as the shared-memory passes.
+template <typename R, int RADIX, bool INV, bool ROWS>
+__global__ void __launch_bounds__(256) k_gstage(const cplx_t<R>* __restrict__ src, cplx_t<R>* __restrict__ dst,
+                                                int L, int64_t outer, int inner, int64_t los, int64_t es, int p,
+                                                const cplx_t<R>* __restrict__ tw, int tw_mul, const int* __restrict__ gate) {
+  using C = cplx_t<R>;
+  if (gate && !*gate) return;
+  const int T = L / RADIX;
+  const int64_t total = outer * inner * static_cast<int64_t>(T);
+  const int twstep = L / (p * RADIX) * tw_mul;
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int64_t o;
+    int w, i;
+    if (ROWS) {  // x lines: butterfly fastest
+      i = static_cast<int>(idx % T);
+      const int64_t r = idx / T;
+      w = static_cast<int>(r % inner);
+      o = r / inner;
+    } else {  // y lines: kx column fastest
+      w = static_cast<int>(idx % inner);
+      const int64_t r = idx / inner;
+      i = static_cast<int>(r % T);
+      o = r / T;
+    }
+    const int64_t base = o * los + w;
+    const int k = i % p;
+    C v[RADIX];
+#pragma unroll
+    for (int r = 0; r < RADIX; ++r) v[r] = src[base + static_cast<int64_t>(i + r * T) * es];
+    if (p > 1) {
+#pragma unroll
+      for (int r = 1; r < RADIX; ++r) {
+        C t = __ldg(tw + r * k * twstep);
+        if (INV) t.y = -t.y;
+        v[r] = cmul(v[r], t);
+      }
+    }
+    dftR<RADIX, INV>(v);
+    const int oo = (i - k) * RADIX + k;
+#pragma unroll
+    for (int r = 0; r < RADIX; ++r) dst[base + static_cast<int64_t>(oo + r * p) * es] = v[r];
+  }
+}
+
+template <typename R, bool INV, bool ROWS>
+static void launch_gstage(int radix, const cplx_t<R>* src, cplx_t<R>* dst, int L, int64_t outer, int inner,
+                          int64_t los, int64_t es, int p, const cplx_t<R>* tw, int tw_mul, const int* gate,
+                          cudaStream_t st) {
+  const int64_t total = outer * inner * static_cast<int64_t>(L / radix);
+  const int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 16));
+  switch (radix) {
+    case 8: k_gstage<R, 8, INV, ROWS><<<blocks, 256, 0, st>>>(src, dst, L, outer, inner, los, es, p, tw, tw_mul, gate); break;
+    case 7: k_gstage<R, 7, INV, ROWS><<<blocks, 256, 0, st>>>(src, dst, L, outer, inner, los, es, p, tw, tw_mul, gate); break;
+    case 5: k_gstage<R, 5, INV, ROWS><<<blocks, 256, 0, st>>>(src, dst, L, outer, inner, los, es, p, tw, tw_mul, gate); break;
+    case 4: k_gstage<R, 4, INV, ROWS><<<blocks, 256, 0, st>>>(src, dst, L, outer, inner, los, es, p, tw, tw_mul, gate); break;
+    case 3: k_gstage<R, 3, INV, ROWS><<<blocks, 256, 0, st>>>(src, dst, L, outer, inner, los, es, p, tw, tw_mul, gate); break;
+    default: k_gstage<R, 2, INV, ROWS><<<blocks, 256, 0, st>>>(src, dst, L, outer, inner, los, es, p, tw, tw_mul, gate); break;
+  }
+}
+
+// all stages of plan pl (radix <= 8) over the lines of buffer `a`, with `b`
+// as the other buffer of the pair; returns the buffer holding the result
+template <typename R, bool INV, bool ROWS>
+static cplx_t<R>* glines_fft(const FftPlan1& pl, cplx_t<R>* a, cplx_t<R>* b, int64_t outer, int inner, int64_t los,
+                             int64_t es, const cplx_t<R>* tw, int tw_mul, cudaStream_t st,
+                             const int* gate = nullptr) {
+  int p = 1;
+  for (int s = 0; s < pl.nst; ++s) {
+    const int R_ = plan_radix(pl, s);
+    launch_gstage<R, INV, ROWS>(R_, a, b, pl.L, outer, inner, los, es, p, tw, tw_mul, gate, st);
+    p *= R_;
+    std::swap(a, b);
+  }
+  return a;
+}
+
+// y lines of the rows y < ny of X[cz][ny][Hx] into Y[cz][Py][Hx]: zero padded,
+// or (tensor) mirrored with sign tsign (rows j >= Py - ny + 1 take row Py - j)
+template <typename R>
+__global__ void k_gy_expand(const cplx_t<R>* __restrict__ X, cplx_t<R>* __restrict__ Y, int ny, int Py, int Hx,
+                            int64_t ncz, int tensor_sign, const int* __restrict__ gate = nullptr) {
+  using C = cplx_t<R>;
+  if (gate && !*gate) return;
+  const int64_t total = ncz * Py * static_cast<int64_t>(Hx);
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int kx = static_cast<int>(e % Hx);
+    const int64_t r = e / Hx;
+    const int j = static_cast<int>(r % Py);
+    const int64_t cz = r / Py;
+    C v = cmk<C>(R(0), R(0));
+    if (j < ny) {
+      v = X[(cz * ny + j) * Hx + kx];
+    } else if (tensor_sign != 0 && j >= Py - ny + 1) {
+      v = X[(cz * ny + (Py - j)) * Hx + kx];
+      if (tensor_sign < 0) v = cmk<C>(-v.x, -v.y);
+    }
+    Y[e] = v;
+  }
+}
+
+// rows y < ny of Y[cz][Py][Hx] back into X[cz][ny][Hx]
+template <typename R>
+__global__ void k_gy_extract(const cplx_t<R>* __restrict__ Y, cplx_t<R>* __restrict__ X, int ny, int Py, int Hx,
+                             int64_t ncz, const int* __restrict__ gate) {
+  if (gate && !*gate) return;
+  const int64_t total = ncz * ny * static_cast<int64_t>(Hx);
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int kx = static_cast<int>(e % Hx);
+    const int64_t r = e / Hx;
+    const int j = static_cast<int>(r % ny);
+    const int64_t cz = r / ny;
+    X[e] = Y[(cz * Py + j) * Hx + kx];
+  }
+}
+
+// real part of ky <= Py/2 of Y[Py][Hx] times scale into Tq[Tyq][Hx] (films)
+__global__ void k_gy_quadrant(const double2* __restrict__ Y, double* __restrict__ Tq, int Tyq, int Hx, double scale) {
+  const int64_t total = static_cast<int64_t>(Tyq) * Hx;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    Tq[e] = Y[e].x * scale;
+}
+
+// film convolution in the y spectrum: H(kx, ky) = Nhat(kx, ky, kz = 0) M(kx, ky)
+// for the three components of Y[c][Py][Hx] (nz = 1), tensor quadrant unfolded
+template <typename R>
+__global__ void k_gproduct_film(cplx_t<R>* __restrict__ Y, const R* __restrict__ Nhat, int Py, int Hx, int Tyq,
+                                const int* __restrict__ gate) {
+  using C = cplx_t<R>;
+  if (gate && !*gate) return;
+  const int64_t total = static_cast<int64_t>(Py) * Hx;
+  const int64_t Ts = static_cast<int64_t>(Tyq) * Hx;  // Tzq = 1
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int kx = static_cast<int>(e % Hx);
+    const int ky = static_cast<int>(e / Hx);
+    const bool fy = ky > Py / 2;
+    const int kyq = fy ? Py - ky : ky;
+    const R sy = fy ? R(-1) : R(1);
+    const int64_t b = static_cast<int64_t>(kyq) * Hx + kx;
+    const R xx = Nhat[b], yy = Nhat[Ts + b], zz = Nhat[2 * Ts + b];
+    const R xy = sy * Nhat[3 * Ts + b], xz = Nhat[4 * Ts + b], yz = sy * Nhat[5 * Ts + b];
+    const C p0 = Y[e], p1 = Y[total + e], p2 = Y[2 * total + e];
+    Y[e] = cmk<C>(xx * p0.x + xy * p1.x + xz * p2.x, xx * p0.y + xy * p1.y + xz * p2.y);
+    Y[total + e] = cmk<C>(xy * p0.x + yy * p1.x + yz * p2.x, xy * p0.y + yy * p1.y + yz * p2.y);
+    Y[2 * total + e] = cmk<C>(xz * p0.x + yz * p1.x + zz * p2.x, xz * p0.y + yz * p1.y + zz * p2.y);
+  }
+}
+
+static int gblocks(int64_t n) { return static_cast<int>(std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+
+// x lines longer than a block holds: pack the real rows (Ms*m, or the
+// mirrored tensor row) as Lc complex pairs, transform, then the even/odd
+// split of k_fwd_x; the inverse undoes it as k_inv_x does
+template <typename R, int MODE>
+__global__ void k_gx_pack(const R* __restrict__ m, const R* __restrict__ Ms, const double* __restrict__ Tr, int tsign,
+                          cplx_t<R>* __restrict__ Z, int rows, int nx, int Lc, int Px, int64_t lines,
+                          const int* __restrict__ gate = nullptr) {
+  using C = cplx_t<R>;
+  if (gate && !*gate) return;
+  const int64_t N = static_cast<int64_t>(rows) * nx, total = lines * Lc;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int t = static_cast<int>(e % Lc);
+    const int64_t line = e / Lc;
+    const int64_t c = line / rows, row = line - c * rows;
+    R v[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int u = 2 * t + h;
+      R x = R(0);
+      const int64_t I = row * nx;
+      if (MODE == XM_MAGN) {
+        if (u < nx) x = m[c * N + I + u] * Ms[I + u];
+      } else {
+        if (u < nx) x = static_cast<R>(Tr[I + u]);
+        else if (u >= Px - nx + 1) x = static_cast<R>(tsign * Tr[I + (Px - u)]);
+      }
+      v[h] = x;
+    }
+    Z[e] = cmk<C>(v[0], v[1]);
+  }
+}
+
+template <typename R>
+__global__ void k_gx_post(const cplx_t<R>* __restrict__ Z, cplx_t<R>* __restrict__ X, int Lc, int Hx, int64_t lines,
+                          const cplx_t<R>* __restrict__ twx, const int* __restrict__ gate = nullptr) {
+  using C = cplx_t<R>;
+  if (gate && !*gate) return;
+  const int64_t total = lines * Hx;
+  const R one_half = R(0.5);
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int k = static_cast<int>(e % Hx);
+    const int64_t l = e / Hx;
+    const C* z = Z + l * Lc;
+    const C zk = z[k == Lc ? 0 : k];
+    const C zc = cconj(z[k == 0 ? 0 : Lc - k]);
+    const C ev = cscale(cadd(zk, zc), one_half);
+    const C od = crot<false>(cscale(csub(zk, zc), one_half));
+    X[e] = cadd(ev, cmul(__ldg(twx + k), od));
+  }
+}
+
+template <typename R>
+__global__ void k_gx_pre(const cplx_t<R>* __restrict__ X, cplx_t<R>* __restrict__ Z, int Lc, int Hx, int64_t lines,
+                         const cplx_t<R>* __restrict__ twx, const int* __restrict__ gate) {
+  using C = cplx_t<R>;
+  if (gate && !*gate) return;
+  const int64_t total = lines * Lc;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int k = static_cast<int>(e % Lc);
+    const int64_t l = e / Lc;
+    const C* xr = X + l * Hx;
+    const C a = xr[k];
+    const C b = cconj(xr[Lc - k]);
+    const C w = cconj(__ldg(twx + k));
+    Z[e] = cadd(cadd(a, b), crot<true>(cmul(csub(a, b), w)));
+  }
+}
+
+template <typename R>
+__global__ void k_gx_unpack(const cplx_t<R>* __restrict__ Z, R* __restrict__ H, int rows, int nx, int Lc,
+                            int64_t lines, const int* __restrict__ gate) {
+  if (gate && !*gate) return;
+  const int64_t N = static_cast<int64_t>(rows) * nx, total = lines * Lc;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int t = static_cast<int>(e % Lc);
+    const int64_t line = e / Lc;
+    const int64_t c = line / rows, row = line - c * rows;
+    const auto z = Z[e];
+    const int u = 2 * t;
+    R* out = H + c * N + row * nx;
+    if (u < nx) out[u] = z.x;
+    if (u + 1 < nx) out[u + 1] = z.y;
+  }
 }
 
 // ---- launch helpers shared by apply() and the tensor assembly ------------
@@ -934,24 +1199,55 @@ static bool run_pass(const DemagPlan<R>& p, DemagGeom g, int which, const R* m, 
                      cudaStream_t st) {
   using C = cplx_t<R>;
   constexpr int NT = kHotNT;
+  const int64_t xlines = 3LL * g.ny * g.nz, ncz = 3LL * g.nz;
   switch (which) {
     case 0:
+      if (p.long_x) {
+        k_gx_pack<R, XM_MAGN><<<gblocks(xlines * g.Lc), 256, 0, st>>>(m, mu0Ms, nullptr, 1, p.Zx, g.ny * g.nz, g.nx,
+                                                                     g.Lc, g.Px, xlines, g.gate);
+        C* z = glines_fft<R, false, true>(p.gplx, p.Zx, p.Zx2, xlines, 1, g.Lc, 1, p.twx, 2, st, g.gate);
+        k_gx_post<R><<<gblocks(xlines * g.Hx), 256, 0, st>>>(z, p.X, g.Lc, g.Hx, xlines, p.twx, g.gate);
+        return true;
+      }
       launch_fwd_x<R, XM_MAGN, NT>(g, m, mu0Ms, nullptr, 1, p.X, 3, p.twx, st);
       return true;
     case 1:
       if (p.fused2d) return false;
+      if (p.long_y) {
+        // start in the buffer that leaves the result in Y after nst stages
+        C* a = (p.gply.nst & 1) ? p.S : p.Y;
+        k_gy_expand<R><<<gblocks(ncz * g.Py * g.Hx), 256, 0, st>>>(p.X, a, g.ny, g.Py, g.Hx, ncz, 0, g.gate);
+        glines_fft<R, false, false>(p.gply, a, a == p.Y ? p.S : p.Y, ncz, g.Hx, static_cast<int64_t>(g.Py) * g.Hx,
+                                    g.Hx, p.twy, 1, st, g.gate);
+        return true;
+      }
       launch_ylines<R, YL_FWD>(g, p.X, p.Y, p.Nhat, p.twy, st, p.tile[1]);
       return true;
     case 2:
       if (p.fused2d) launch_ylines<R, YL_CONV2D>(g, p.X, p.X, p.Nhat, p.twy, st, p.tile[2]);
+      else if (p.long_y && g.Pz == 1)
+        k_gproduct_film<R><<<gblocks(static_cast<int64_t>(g.Py) * g.Hx), 256, 0, st>>>(p.Y, p.Nhat, g.Py, g.Hx, g.Tyq,
+                                                                                    g.gate);
       else launch_zconv<R>(g, p.Y, p.Nhat, p.twz, st, p.tile[2]);
       return true;
     case 3:
       if (p.fused2d) return false;
+      if (p.long_y) {
+        C* r = glines_fft<R, true, false>(p.gply, p.Y, p.S, ncz, g.Hx, static_cast<int64_t>(g.Py) * g.Hx, g.Hx,
+                                          p.twy, 1, st, g.gate);
+        k_gy_extract<R><<<gblocks(ncz * g.ny * g.Hx), 256, 0, st>>>(r, p.X, g.ny, g.Py, g.Hx, ncz, g.gate);
+        return true;
+      }
       launch_ylines<R, YL_INV>(g, p.Y, p.X, p.Nhat, p.twy, st, p.tile[3]);
       return true;
     case 4: {
       const int lines = 3 * g.ny * g.nz;
+      if (p.long_x) {
+        k_gx_pre<R><<<gblocks(xlines * g.Lc), 256, 0, st>>>(p.X, p.Zx, g.Lc, g.Hx, xlines, p.twx, g.gate);
+        C* z = glines_fft<R, true, true>(p.gplx, p.Zx, p.Zx2, xlines, 1, g.Lc, 1, p.twx, 2, st, g.gate);
+        k_gx_unpack<R><<<gblocks(xlines * g.Lc), 256, 0, st>>>(z, Hd, g.ny * g.nz, g.nx, g.Lc, xlines, g.gate);
+        return true;
+      }
       if (g.Px == 1) {
         k_inv_x1<R><<<(lines + 255) / 256, 256, 0, st>>>(p.X, Hd, lines, g.gate);
       } else {
@@ -1016,6 +1312,7 @@ int DemagPlan<R>::autotune(const R* m, const R* mu0Ms, R* Hd, cudaStream_t st) {
   const bool zc2 = !fused2d && pass_smem<R>(g, 2, false, 1) == sizeof(C) * 3 * (g.Pz | 1);
   for (int which = 1; which <= 3; ++which) {
     if (fused2d && which != 2) continue;
+    if (long_y && (which != 2 || g.Pz == 1)) continue;  // global-memory stages have no tile
     // the static rule's W is the incumbent; another W must be 3 % faster
     // (timing noise, e.g. under a profiler, then cannot move the choice)
     tile[which] = 0;
@@ -1080,7 +1377,11 @@ double DemagPlan<R>::pass_bytes(int which) const {
 
 template <typename R>
 int DemagPlan<R>::launches_per_apply() const {
-  return fused2d ? 3 : 5;
+  if (fused2d) return 3;
+  int n = 1;                                          // conv
+  n += long_x ? 2 * (gplx.nst + 2) : 2;               // x forward / inverse
+  n += long_y ? 2 * (gply.nst + 1) : 2;               // y forward / inverse
+  return n;
 }
 
 // Tensor spectrum: for each component, forward r2c-x / y / z transforms of
@@ -1106,15 +1407,41 @@ int DemagPlan<R>::set_tensor(const double* T6N, cudaStream_t st) {
   if (g.Px > 1 && !(tx = upload_twiddles<C64>(g.Px, b64, st))) rc = 2;
   if (!rc && !(ty = upload_twiddles<C64>(g.Py, b64, st))) rc = 2;
   if (!rc && !(tz = upload_twiddles<C64>(g.Pz, b64, st))) rc = 2;
+  C64 *Z64 = nullptr, *Z64b = nullptr, *S64 = nullptr;
+  const int64_t nZ = static_cast<int64_t>(g.ny) * g.nz * g.Lc;
   if (!rc && cudaMalloc(&X64, sizeof(C64) * nX) != cudaSuccess) rc = 2;
-  if (!rc && g.Pz > 1 && cudaMalloc(&Y64, sizeof(C64) * nY) != cudaSuccess) rc = 2;
+  if (!rc && (g.Pz > 1 || long_y) && cudaMalloc(&Y64, sizeof(C64) * nY) != cudaSuccess) rc = 2;
+  if (!rc && long_y && cudaMalloc(&S64, sizeof(C64) * nY) != cudaSuccess) rc = 2;
+  if (!rc && long_x && (cudaMalloc(&Z64, sizeof(C64) * nZ) != cudaSuccess || cudaMalloc(&Z64b, sizeof(C64) * nZ) != cudaSuccess))
+    rc = 2;
   if (!rc && cudaMalloc(&Tq, sizeof(double) * 6 * Ts) != cudaSuccess) rc = 2;
   if (!rc) {
     const double scale = -1.0 / (kMu0 * static_cast<double>(g.Px) * g.Py * g.Pz);
+    const int64_t rows = static_cast<int64_t>(g.ny) * g.nz;
     for (int c = 0; c < 6; ++c) {
       const int sx = odd_axis(c, 0) ? -1 : 1, sy = odd_axis(c, 1) ? -1 : 1, sz = odd_axis(c, 2) ? -1 : 1;
-      launch_fwd_x<double, XM_TENSOR, NT>(g64, nullptr, nullptr, T6N + c * N, sx, X64, 1, tx, st);
-      if (g.Pz == 1) {
+      if (long_x) {
+        k_gx_pack<double, XM_TENSOR><<<gblocks(rows * g.Lc), 256, 0, st>>>(nullptr, nullptr, T6N + c * N, sx, Z64,
+                                                                          static_cast<int>(rows), g.nx, g.Lc, g.Px,
+                                                                          rows);
+        C64* z = glines_fft<double, false, true>(gplx, Z64, Z64b, rows, 1, g.Lc, 1, tx, 2, st);
+        k_gx_post<double><<<gblocks(rows * g.Hx), 256, 0, st>>>(z, X64, g.Lc, g.Hx, rows, tx);
+      } else {
+        launch_fwd_x<double, XM_TENSOR, NT>(g64, nullptr, nullptr, T6N + c * N, sx, X64, 1, tx, st);
+      }
+      if (long_y) {
+        // mirrored y lines in global memory; the result lands in Y64
+        C64* a = (gply.nst & 1) ? S64 : Y64;
+        k_gy_expand<double><<<gblocks(static_cast<int64_t>(g.nz) * g.Py * g.Hx), 256, 0, st>>>(
+            X64, a, g.ny, g.Py, g.Hx, g.nz, sy);
+        glines_fft<double, false, false>(gply, a, a == Y64 ? S64 : Y64, g.nz, g.Hx,
+                                         static_cast<int64_t>(g.Py) * g.Hx, g.Hx, ty, 1, st);
+        if (g.Pz == 1)
+          k_gy_quadrant<<<gblocks(static_cast<int64_t>(g.Tyq) * g.Hx), 256, 0, st>>>(Y64, Tq + c * Ts, g.Tyq, g.Hx,
+                                                                                      scale);
+        else
+          launch_zpass<double, ZM_TENSOR_Q, NT>(g64, Y64, nullptr, Tq + c * Ts, 1, g.Tyq, tz, sz, scale, st);
+      } else if (g.Pz == 1) {
         launch_ypass<double, YM_TENSOR_Q, NT>(g64, X64, nullptr, nullptr, Tq + c * Ts, 1, 1, ty, sy, scale, st);
       } else {
         launch_ypass<double, YM_TENSOR, NT>(g64, X64, Y64, nullptr, nullptr, 1, 1, ty, sy, 0.0, st);
@@ -1126,6 +1453,7 @@ int DemagPlan<R>::set_tensor(const double* T6N, cudaStream_t st) {
     cudaStreamSynchronize(st);
   }
   cudaFree(tx); cudaFree(ty); cudaFree(tz); cudaFree(X64); cudaFree(Y64); cudaFree(Tq);
+  cudaFree(S64); cudaFree(Z64); cudaFree(Z64b);
   return rc;
 }
 

@@ -63,6 +63,14 @@ class DemagPlan {
 
   DemagGeom g{};
   bool fused2d = false;
+  // x / y lines longer than one block holds run as global-memory radix
+  // stages (plans gplx / gply, radix <= 8) through ping-pong buffers:
+  // S (same shape as Y) for y, Zx / Zx2 ([3 ny nz][Lc]) for x
+  bool long_x = false, long_y = false;
+  FftPlan1 gplx{}, gply{};
+  C* S = nullptr;
+  C* Zx = nullptr;
+  C* Zx2 = nullptr;
   C* X = nullptr;
   C* Y = nullptr;
   R* Nhat = nullptr;

@@ -87,12 +87,13 @@ def test_demag_newell_fp64(mesh):
 
 
 @pytest.mark.parametrize("form", [0, 1])
-@pytest.mark.parametrize("mesh", [(3000, 2, 1), (4, 1800, 1), (2, 3, 700), (6, 1100, 3)])
+@pytest.mark.parametrize("mesh", [(3000, 2, 1), (4, 1800, 1), (2, 3, 700), (6, 1100, 3), (7300, 2, 1),
+                                  (2, 3700, 1), (2, 3700, 3), (7300, 2, 2)])
 def test_demag_long_lines(mesh, form):
-    """Padded lines beyond the multi-line tiles (one line per block): x/2 = 3000,
-    y = 3600, z = 1400 and y = 2200 with z = 6 (the FP64 tensor passes and the
-    FP64 hot passes at their largest), FP64 to 1e-12 with the oracle's tensor,
-    the FP32 form to 1e-5."""
+    """Padded lines beyond the multi-line tiles: one line per block (x/2 = 3000,
+    y = 3600, z = 1400, y = 2200 with z = 6) and lines beyond one block, run as
+    global-memory radix stages (x/2 = 7350, y = 7500, films and 3-D), FP64 to
+    1e-12 with the oracle's tensor (and 1e-9 with the GPU's), FP32 to 1e-5."""
     from oracle.oracle import demag_tensor
 
     nx, ny, nz = mesh
@@ -105,6 +106,28 @@ def test_demag_long_lines(mesh, form):
     if form == 0:
         fn, _ = GpuSim(cfg, form=0).term_field("demag")  # tensor assembled on the GPU
         assert rel_maxnorm(fn, fo) <= TENSOR_TOL
+
+
+def test_long_lines_rk4_and_dopri_fp64():
+    """Stepping through the global-memory line stages, gated in the adaptive
+    stepper's graph (y = 7500 film with exchange, anisotropy and Zeeman)."""
+    from oracle.oracle import demag_tensor
+
+    cfg = random_config(23, 2, 3700, 1, "", terms=("exch", "anis", "zeeman", "demag"), spatial=False)
+    T = demag_tensor(2, 3700, 1, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, _ = build_oracle(cfg, tensor=T)
+    g = GpuSim(cfg, form=0, tensor=T)
+    o.rk4(2e-14, 3)
+    g.rk4(2e-14, 3)
+    assert rel_maxnorm(g.m(), o.get_m()) <= 1e-11
+    o, _ = build_oracle(cfg, tensor=T)  # a fresh Sim for the adaptive stepper (its y_current is m0)
+    g = GpuSim(cfg, form=0, tensor=T)
+    o.set_tol(1e-6)
+    g.set_tol(1e-6)
+    ok, so = o.run_until(1e-13)
+    rc, sg = g.run_until(1e-13)
+    assert ok and rc == 0 and sg["nsteps"] == so["nsteps"]
+    assert rel_maxnorm(g.m(), o.get_m()) <= 1e-11
 
 
 def test_demag_macro_pbc_fp64():

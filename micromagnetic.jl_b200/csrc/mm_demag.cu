@@ -27,6 +27,9 @@ template <typename R, int NT> struct PassCfg {
   static constexpr int minb = NT == 256 ? 3 : 1;
 };
 constexpr int kHotNT = 256;
+// threads of the fused-middle z kernel (384 in FP32, so that the first stage
+// of a 16-column tile takes one round, measured 17 % slower: register cap)
+template <typename R> constexpr int zconv2_nt() { return 256; }
 constexpr size_t kMaxSmem = 227 * 1024;  // dynamic shared memory per block (opt-in maximum)
 constexpr int kTensorNT = 512;
 template <typename R> constexpr int hot_cap() { return PassCfg<R, kHotNT>::cap; }
@@ -475,7 +478,7 @@ __global__ void __launch_bounds__(NT, 2) k_zconv(cplx_t<R>* Y, const R* __restri
 // finally the inverse radix-RA stage straight to the Y rows kz < nz.
 // One shared buffer; requires W * RA <= NT (one middle task per thread).
 template <typename R, int RA, int RB, int NT, bool I32>
-__global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_zconv2(cplx_t<R>* Y, const R* __restrict__ Nhat, DemagGeom g, int lgW,
+__global__ void __launch_bounds__(NT, NT > 256 ? 2 : (sizeof(R) == 4 ? 3 : 2)) k_zconv2(cplx_t<R>* Y, const R* __restrict__ Nhat, DemagGeom g, int lgW,
                                                   FastDiv fnl, const cplx_t<R>* __restrict__ twz) {
   using C = cplx_t<R>;
   using IX = std::conditional_t<I32, int, int64_t>;
@@ -1140,22 +1143,23 @@ static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const
                           int Wforce) {
   using C = cplx_t<R>;
   constexpr int L = RA * RB;
+  constexpr int NTZ = zconv2_nt<R>();
   int W = Wforce > 0 ? Wforce : lines_tile<R>(g.Hx, L, 3, 1);
-  while (W * RA > kHotNT) W /= 2;
+  while (W * RA > NTZ) W /= 2;
   const size_t sm = sizeof(C) * 3 * W * (L | 1);
   static uint64_t done = 0;
   int dev = 0;
   cudaGetDevice(&dev);
   if (!((done >> dev) & 1ull)) {
-    cudaFuncSetAttribute(k_zconv2<R, RA, RB, kHotNT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
-    cudaFuncSetAttribute(k_zconv2<R, RA, RB, kHotNT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
+    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
+    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
     done |= 1ull << dev;
   }
   dim3 grid((g.Hx + W - 1) / W, g.Py, 1);
   if (offsets_fit_int(g))
-    k_zconv2<R, RA, RB, kHotNT, true><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz);
+    k_zconv2<R, RA, RB, NTZ, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz);
   else
-    k_zconv2<R, RA, RB, kHotNT, false><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz);
+    k_zconv2<R, RA, RB, NTZ, false><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz);
 }
 
 // Power-of-two z lengths with a fused-middle kernel: L = RA * RB
@@ -1321,14 +1325,14 @@ int DemagPlan<R>::autotune(const R* m, const R* mu0Ms, R* Hd, cudaStream_t st) {
       const int nb = which == 2 ? (fused2d ? 2 : (zc2 ? 1 : 2)) : std::max(1, line_fft_buffers(g.ply));
       W0 = which == 2 && !fused2d ? lines_tile<R>(g.Hx, g.Pz, 3, nb) : lines_tile<R>(g.Hx, g.Py, which == 2 ? 3 : 1, nb);
       if (which == 2 && zc2)
-        while (W0 * ra > kHotNT) W0 /= 2;
+        while (W0 * ra > zconv2_nt<R>()) W0 /= 2;
     }
     float ms0 = 0.f, best = 1e30f;
     int bestW = W0;
     for (int W = 1; W <= wmax; W *= 2) {
       if (W / 2 >= g.Hx) break;
       if (pass_smem<R>(g, which, fused2d, W) > kMaxSmem) break;
-      if (which == 2 && zc2 && W * ra > kHotNT) break;
+      if (which == 2 && zc2 && W * ra > zconv2_nt<R>()) break;
       tile[which] = W;
       for (int r = 0; r < 2; ++r) run_pass(*this, g, which, m, mu0Ms, Hd, st);
       cudaEventRecord(e0, st);

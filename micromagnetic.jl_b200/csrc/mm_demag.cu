@@ -416,7 +416,7 @@ enum YLMode { YL_FWD = 0, YL_INV = 1, YL_CONV2D = 2 };
 //   YL_INV:    Y rows 0..Py-1           -> X rows y < ny
 //   YL_CONV2D: X rows y < ny, forward y, tensor product (kz = 0), inverse y -> X
 template <typename R, int MODE, int NT, bool I32>
-__global__ void __launch_bounds__(NT, 2) k_ylines(const cplx_t<R>* in, cplx_t<R>* out, const R* __restrict__ Nhat,
+__global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_ylines(const cplx_t<R>* in, cplx_t<R>* out, const R* __restrict__ Nhat,
                                                   DemagGeom g, int lgW, int ncompc, FastDiv fnl,
                                                   const cplx_t<R>* __restrict__ twy, int half) {
   using C = cplx_t<R>;

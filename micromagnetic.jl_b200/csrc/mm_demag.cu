@@ -27,9 +27,15 @@ template <typename R, int NT> struct PassCfg {
   static constexpr int minb = NT == 256 ? 3 : 1;
 };
 constexpr int kHotNT = 256;
-// threads of the fused-middle z kernel (384 in FP32, so that the first stage
-// of a 16-column tile takes one round, measured 17 % slower: register cap)
-template <typename R> constexpr int zconv2_nt() { return 256; }
+// threads of the fused-middle z kernel: one per middle task of the widest
+// tile (W * RA: FP32 16 x 16, FP64 8 x 16 for Pz = 128).  384 in FP32, so
+// that the first stage of a 16-column tile takes one round, measured 17 %
+// slower (register cap); FP64 at 128 threads is 5 % faster than at 256, whose
+// middle left half the threads idle.
+template <typename R> constexpr int zconv2_nt() { return sizeof(R) == 4 ? 256 : 128; }
+// blocks per SM the fused z kernels are compiled for: 80 (FP32) and 128
+// (FP64) registers a thread
+template <typename R, int NT> constexpr int zconv2_minb() { return (sizeof(R) == 4 ? 3 : 2) * 256 / NT; }
 constexpr size_t kMaxSmem = 227 * 1024;  // dynamic shared memory per block (opt-in maximum)
 constexpr int kTensorNT = 512;
 template <typename R> constexpr int hot_cap() { return PassCfg<R, kHotNT>::cap; }
@@ -478,7 +484,7 @@ __global__ void __launch_bounds__(NT, 2) k_zconv(cplx_t<R>* Y, const R* __restri
 // finally the inverse radix-RA stage straight to the Y rows kz < nz.
 // One shared buffer; requires W * RA <= NT (one middle task per thread).
 template <typename R, int RA, int RB, int NT, bool I32>
-__global__ void __launch_bounds__(NT, NT > 256 ? 2 : (sizeof(R) == 4 ? 3 : 2)) k_zconv2(cplx_t<R>* Y, const R* __restrict__ Nhat, DemagGeom g, int lgW,
+__global__ void __launch_bounds__(NT, (zconv2_minb<R, NT>())) k_zconv2(cplx_t<R>* Y, const R* __restrict__ Nhat, DemagGeom g, int lgW,
                                                   FastDiv fnl, const cplx_t<R>* __restrict__ twz) {
   using C = cplx_t<R>;
   using IX = std::conditional_t<I32, int, int64_t>;

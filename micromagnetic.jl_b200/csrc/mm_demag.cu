@@ -123,14 +123,28 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_fwd_x(
   buf = line_fft_to_smem<false, NT>(SmemLines<C>{buf, LS}, buf2, buf, LS, nl, fnl, g.plx, twx, 2);
   const int Hx = g.Hx;
   const R one_half = R(0.5);
-  for (int e = threadIdx.x; e < nlh * Hx; e += NT) {
-    const int l = fdiv(e, g.fHx), k = e - l * Hx;
+  auto spectrum = [&](int l, int k) {
     const C zk = buf[l * LS + (k == Lc ? 0 : k)];
     const C zc = cconj(buf[l * LS + (k == 0 ? 0 : Lc - k)]);
     const C ev = cscale(cadd(zk, zc), one_half);
     const C od = crot<false>(cscale(csub(zk, zc), one_half));  // (zk - zc)/(2i)
     const C w = __ldg(twx + k);
-    X[static_cast<int64_t>(line0 + l) * Hx + k] = cadd(ev, cmul(w, od));
+    return cadd(ev, cmul(w, od));
+  };
+  if (MODE == XM_MAGN && g.xT) {
+    // column-major X: consecutive threads write consecutive rows of one kx
+    for (int e = threadIdx.x; e < nl * Hx; e += NT) {
+      const int k = fdiv(e, fnl), l = e - k * nl;
+      if (l >= nlh) continue;
+      const int line = line0 + l;
+      const int c = fdiv(line, g.frows), row = line - c * rows;
+      X[(static_cast<int64_t>(c) * Hx + k) * rows + row] = spectrum(l, k);
+    }
+  } else {
+    for (int e = threadIdx.x; e < nlh * Hx; e += NT) {
+      const int l = fdiv(e, g.fHx), k = e - l * Hx;
+      X[static_cast<int64_t>(line0 + l) * Hx + k] = spectrum(l, k);
+    }
   }
 }
 
@@ -164,14 +178,27 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_inv_x(
   const int64_t N = static_cast<int64_t>(rows) * nx;
   const int line0 = blockIdx.x * nl;
   const int nlh = min(nl, lines_total - line0);
-  for (int e = threadIdx.x; e < nlh * Lc; e += NT) {
-    const int l = fdiv(e, g.fLc), k = e - l * Lc;
-    const C* xr = X + static_cast<int64_t>(line0 + l) * Hx;
-    const C a = xr[k];
-    const C b = cconj(xr[Lc - k]);
+  // Z'[k] = (A + B) + i (A - B) conj(W^k), A = X[k], B = conj(X[Lc - k])
+  auto pre = [&](int l, int k, C a, C b) {
     const C w = cconj(__ldg(twx + k));
-    // Z'[k] = (A + B) + i (A - B) conj(W^k)
     buf[l * LS + k] = cadd(cadd(a, b), crot<true>(cmul(csub(a, b), w)));
+  };
+  if (g.xT) {
+    // column-major X: consecutive threads read consecutive rows of one kx
+    for (int e = threadIdx.x; e < nl * Lc; e += NT) {
+      const int k = fdiv(e, fnl), l = e - k * nl;
+      if (l >= nlh) continue;
+      const int line = line0 + l;
+      const int c = fdiv(line, g.frows), row = line - c * rows;
+      const C* xc = X + static_cast<int64_t>(c) * Hx * rows + row;
+      pre(l, k, xc[static_cast<int64_t>(k) * rows], cconj(xc[static_cast<int64_t>(Lc - k) * rows]));
+    }
+  } else {
+    for (int e = threadIdx.x; e < nlh * Lc; e += NT) {
+      const int l = fdiv(e, g.fLc), k = e - l * Lc;
+      const C* xr = X + static_cast<int64_t>(line0 + l) * Hx;
+      pre(l, k, xr[k], cconj(xr[Lc - k]));
+    }
   }
   __syncthreads();
   buf = line_fft_to_smem<true, NT>(SmemLines<C>{buf, LS}, buf2, buf, LS, nl, fnl, g.plx, twx, 2);
@@ -216,7 +243,7 @@ __global__ void k_inv_x1(const cplx_t<R>* __restrict__ X, R* __restrict__ H, int
 // length L hold the 3 components at (kx0 + w, ky, kz); along y (kz = 0) or
 // along z (ky fixed).  The stored quadrant is unfolded with the component
 // parities (odd in y: xy, yz; odd in z: xz, yz).
-template <typename R, bool ALONG_Y, int NT>
+template <typename R, bool ALONG_Y, int NT, bool COLS = false>
 __device__ __forceinline__ void tensor_product(cplx_t<R>* buf, int LS, int lgW, int L, const FastDiv fL,
                                                int kx0, int ky_fixed, const R* __restrict__ Nhat, int Hx, int Py,
                                                int Pz) {
@@ -225,7 +252,16 @@ __device__ __forceinline__ void tensor_product(cplx_t<R>* buf, int LS, int lgW, 
   const int Tyq = Py / 2 + 1, Tzq = Pz / 2 + 1;
   const int64_t Ts = static_cast<int64_t>(Tzq) * Tyq * Hx;
   for (int e = threadIdx.x; e < W * L; e += NT) {
-    const int w = e & (W - 1), t = e >> lgW;  // w fastest: coalesced tensor reads
+    // coalesced tensor reads: w fastest (row-major tensor), t fastest (COLS,
+    // the column-major film tensor Nhat[(c*Hx + kx)*Tyq + ky])
+    int w, t;
+    if (COLS) {
+      w = fdiv(e, fL);
+      t = e - w * L;
+    } else {
+      w = e & (W - 1);
+      t = e >> lgW;
+    }
     const int kx = kx0 + w;
     if (kx >= Hx) continue;
     const int ky = ALONG_Y ? t : ky_fixed;
@@ -233,7 +269,7 @@ __device__ __forceinline__ void tensor_product(cplx_t<R>* buf, int LS, int lgW, 
     const bool fy = ky > Py / 2, fz = kz > Pz / 2;
     const int kyq = fy ? Py - ky : ky, kzq = fz ? Pz - kz : kz;
     const R sy = fy ? R(-1) : R(1), sz = fz ? R(-1) : R(1);
-    const int64_t b = (static_cast<int64_t>(kzq) * Tyq + kyq) * Hx + kx;
+    const int64_t b = COLS ? static_cast<int64_t>(kx) * Tyq + kyq : (static_cast<int64_t>(kzq) * Tyq + kyq) * Hx + kx;
     const R xx = __ldg(Nhat + b), yy = __ldg(Nhat + Ts + b), zz = __ldg(Nhat + 2 * Ts + b);
     const R xy = sy * __ldg(Nhat + 3 * Ts + b), xz = sz * __ldg(Nhat + 4 * Ts + b),
             yz = sy * sz * __ldg(Nhat + 5 * Ts + b);
@@ -245,7 +281,6 @@ __device__ __forceinline__ void tensor_product(cplx_t<R>* buf, int LS, int lgW, 
     *p1 = cmk<C>(xy * a.x + yy * bb.x + yz * c.x, xy * a.y + yy * bb.y + yz * c.y);
     *p2 = cmk<C>(xz * a.x + yz * bb.x + zz * c.x, xz * a.y + yz * bb.y + zz * c.y);
   }
-  (void)fL;
   __syncthreads();
 }
 
@@ -421,7 +456,8 @@ enum YLMode { YL_FWD = 0, YL_INV = 1, YL_CONV2D = 2 };
 //   YL_FWD:    X rows y < ny            -> Y rows 0..Py-1
 //   YL_INV:    Y rows 0..Py-1           -> X rows y < ny
 //   YL_CONV2D: X rows y < ny, forward y, tensor product (kz = 0), inverse y -> X
-template <typename R, int MODE, int NT, bool I32>
+// XT (YL_CONV2D of films): X column-major, see DemagGeom::xT.
+template <typename R, int MODE, int NT, bool I32, bool XT = false>
 __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_ylines(const cplx_t<R>* in, cplx_t<R>* out, const R* __restrict__ Nhat,
                                                   DemagGeom g, int lgW, int ncompc, FastDiv fnl,
                                                   const cplx_t<R>* __restrict__ twy, int half) {
@@ -440,7 +476,14 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_ylines(const cpl
                     static_cast<IX>(Hx), lgW, kx0, Hx, rin};
   RowsOut<C, IX> dst{out + static_cast<int64_t>(c0 * nz + z) * rout * Hx,
                      static_cast<IX>(static_cast<int64_t>(nz) * rout * Hx), static_cast<IX>(Hx), lgW, kx0, Hx, rout};
-  if (MODE == YL_CONV2D) {
+  if (MODE == YL_CONV2D && XT) {
+    // films (nz = 1): the three components of W columns, each contiguous
+    const ColsIn<C, IX> cin{in, ny, lgW, kx0, Hx, ny};
+    const ColsOut<C, IX> cout{out, ny, lgW, kx0, Hx, ny};
+    C* res = line_fft_to_smem<false, NT>(cin, a, b, LS, nlines, fnl, g.ply, twy, 1);
+    tensor_product<R, true, NT, true>(res, LS, lgW, Py, g.fPy, kx0, 0, Nhat, Hx, Py, g.Pz);
+    line_fft_from_smem<true, NT>(res, res == a ? b : a, cout, LS, nlines, fnl, g.ply, twy, 1);
+  } else if (MODE == YL_CONV2D) {
     C* res = line_fft_to_smem<false, NT>(src, a, b, LS, nlines, fnl, g.ply, twy, 1);
     tensor_product<R, true, NT>(res, LS, lgW, Py, g.fPy, kx0, 0, Nhat, Hx, Py, g.Pz);
     line_fft_from_smem<true, NT>(res, res == a ? b : a, dst, LS, nlines, fnl, g.ply, twy, 1);
@@ -555,6 +598,18 @@ __global__ void __launch_bounds__(NT, (zconv2_minb<R, NT>())) k_zconv2(cplx_t<R>
   }
   __syncthreads();
   lstage<RA, true, true, NT>(A, dst, L, nlines, fnl, RB, twz, 1);
+}
+
+// FP64 film tensor quadrant [6][Tyq][Hx] (Tzq = 1) to RO, column-major [6][Hx][Tyq]
+template <typename RO>
+__global__ void k_cast_cols(const double* __restrict__ a, RO* __restrict__ b, int Tyq, int Hx) {
+  const int64_t plane = static_cast<int64_t>(Tyq) * Hx, n = 6 * plane;
+  for (int64_t o = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; o < n;
+       o += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t c = o / plane, r = o - c * plane;
+    const int64_t kx = r / Tyq, ky = r - kx * Tyq;
+    b[o] = static_cast<RO>(a[c * plane + ky * Hx + kx]);
+  }
 }
 
 template <typename RO>
@@ -695,6 +750,8 @@ static void set_smem_attrs_nt() {
   cudaFuncSetAttribute(k_ylines<R, YL_FWD, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_ylines<R, YL_INV, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_zconv<R, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
 
@@ -767,6 +824,7 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
   g.fpady = make_fastdiv(std::max(1, g.Py - ny));
   g.fpadz = make_fastdiv(std::max(1, g.Pz - nz));
   fused2d = !long_y && (g.Pz == 1) && (2 * 3 * (g.Py | 1) * sizeof(C) <= static_cast<size_t>(smem_budget_bytes()));
+  g.xT = fused2d && g.Px > 1 && !long_x ? 1 : 0;  // the global-memory x stages keep rows
   set_smem_attrs<R>();
   set_smem_attrs<double>();
   const int64_t nX = 3LL * nz * ny * g.Hx;
@@ -1136,12 +1194,20 @@ static void launch_ylines(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* ou
   const int half = ncompc * W * (g.Py | 1);
   dim3 grid((g.Hx + W - 1) / W, g.nz, 3 / ncompc);
   const size_t sm = static_cast<size_t>(std::max(1, nbuf)) * sizeof(C) * half;
+  const FastDiv fnl = make_fastdiv(ncompc * W);
+  if constexpr (MODE == YL_CONV2D) {
+    if (g.xT) {
+      if (offsets_fit_int(g))
+        k_ylines<R, MODE, kHotNT, true, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
+      else
+        k_ylines<R, MODE, kHotNT, false, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
+      return;
+    }
+  }
   if (offsets_fit_int(g))
-    k_ylines<R, MODE, kHotNT, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc,
-                                                              make_fastdiv(ncompc * W), twy, half);
+    k_ylines<R, MODE, kHotNT, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
   else
-    k_ylines<R, MODE, kHotNT, false><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc,
-                                                               make_fastdiv(ncompc * W), twy, half);
+    k_ylines<R, MODE, kHotNT, false><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
 }
 
 template <typename R, int RA, int RB>
@@ -1458,7 +1524,8 @@ int DemagPlan<R>::set_tensor(const double* T6N, cudaStream_t st) {
         launch_zpass<double, ZM_TENSOR_Q, NT>(g64, Y64, nullptr, Tq + c * Ts, 1, g.Tyq, tz, sz, scale, st);
       }
     }
-    k_cast<R><<<1024, 256, 0, st>>>(Tq, Nhat, 6 * Ts);
+    if (g.xT) k_cast_cols<R><<<1024, 256, 0, st>>>(Tq, Nhat, g.Tyq, g.Hx);
+    else k_cast<R><<<1024, 256, 0, st>>>(Tq, Nhat, 6 * Ts);
     rc = static_cast<int>(cudaGetLastError());
     cudaStreamSynchronize(st);
   }

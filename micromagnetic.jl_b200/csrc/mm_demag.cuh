@@ -25,6 +25,10 @@ struct DemagGeom {
   int Tyq, Tzq;    // Py/2 + 1, Pz/2 + 1
   FftPlan1 plx, ply, plz;
   FastDiv fLc, fHx, fPy, fPz, fny, fnz, frows, fpady, fpadz;
+  // films on the fused y-convolution path keep the x spectrum column-major,
+  // X[(c*Hx + kx)*ny + y], and the tensor quadrant as Nhat[(c*Hx + kx)*Tyq + ky],
+  // so that a y line is contiguous in HBM (row-major: X[(c*ny + y)*Hx + kx])
+  int xT;
   const int* gate;  // device flag: kernels return at once when *gate == 0 (null: always run)
 };
 

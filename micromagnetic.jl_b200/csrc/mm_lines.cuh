@@ -57,6 +57,32 @@ struct RowsOut {
   }
 };
 
+// columns of a column-major spectrum (films): element (line, pos) at
+// base[(comp * Hx + kx) * ld + pos], kx = kx0 + w, comp = line >> lgW.
+template <typename C, typename IX = int64_t>
+struct ColsIn {
+  const C* base;
+  int ld, lgW, kx0, Hx, nrows;  // pos >= nrows reads as zero
+  __device__ __forceinline__ C load(int line, int pos) const {
+    const int w = line & ((1 << lgW) - 1), comp = line >> lgW;
+    const int kx = kx0 + w;
+    if (pos >= nrows || kx >= Hx) return cmk<C>(0, 0);
+    return base[(static_cast<IX>(comp) * Hx + kx) * ld + pos];
+  }
+};
+
+template <typename C, typename IX = int64_t>
+struct ColsOut {
+  C* base;
+  int ld, lgW, kx0, Hx, nrows;  // pos >= nrows is not written
+  __device__ __forceinline__ void store(int line, int pos, C v) const {
+    const int w = line & ((1 << lgW) - 1), comp = line >> lgW;
+    const int kx = kx0 + w;
+    if (pos >= nrows || kx >= Hx) return;
+    base[(static_cast<IX>(comp) * Hx + kx) * ld + pos] = v;
+  }
+};
+
 template <int R, bool INV, bool POW2, int NT, class SRC, class DST, typename C>
 __device__ __forceinline__ void lstage(const SRC& src, const DST& dst, int L, int nlines, const FastDiv fnl, int p,
                                        const C* __restrict__ tw, int tw_mul) {

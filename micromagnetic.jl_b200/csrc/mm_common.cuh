@@ -59,9 +59,9 @@ inline int radix_code(int r) {
   }
 }
 
-// Stage radices for a 7-smooth length.  Powers of two are split into the
-// fewest stages of radix <= max_pow2_radix with balanced exponents (2^11 with
-// 16 -> 16,16,8); other lengths take 8, 7, 5, 4, 3, 2 greedily.
+// Stage radices for a 7-smooth length.  The power-of-two factor is split into
+// the fewest stages of radix <= max_pow2_radix with balanced exponents (2^11
+// with 16 -> 16,16,8); the odd factor takes 7, 5, 3 (2000 with 16 -> 16,5,5,5).
 inline bool make_fft_plan(int L, FftPlan1& p, int max_pow2_radix = 8) {
   p.L = L;
   p.nst = 0;
@@ -73,28 +73,26 @@ inline bool make_fft_plan(int L, FftPlan1& p, int max_pow2_radix = 8) {
     ++p.nst;
     return true;
   };
-  if (p.pow2) {
-    int lg = 0;
-    while ((1 << lg) < L) ++lg;
+  if (L < 1) return false;
+  int m = L, lg = 0;
+  while (m % 2 == 0) {
+    m /= 2;
+    ++lg;
+  }
+  if (lg > 0) {
     int lmax = 0;
     while ((1 << lmax) < max_pow2_radix) ++lmax;
-    if (lg == 0) return true;
     const int ns = (lg + lmax - 1) / lmax;
     for (int s = 0; s < ns; ++s) {
       const int e = lg / ns + (s < lg % ns ? 1 : 0);
       if (!push(1 << e)) return false;
     }
-    return true;
   }
-  int m = L;
   while (m > 1) {
     int r = 0;
-    if (m % 8 == 0) r = 8;
-    else if (m % 7 == 0) r = 7;
+    if (m % 7 == 0) r = 7;
     else if (m % 5 == 0) r = 5;
-    else if (m % 4 == 0) r = 4;
     else if (m % 3 == 0) r = 3;
-    else if (m % 2 == 0) r = 2;
     else return false;
     if (!push(r)) return false;
     m /= r;

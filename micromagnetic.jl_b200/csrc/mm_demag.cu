@@ -273,9 +273,10 @@ __device__ __forceinline__ void tensor_product(cplx_t<R>* buf, int LS, int lgW, 
     const R xx = __ldg(Nhat + b), yy = __ldg(Nhat + Ts + b), zz = __ldg(Nhat + 2 * Ts + b);
     const R xy = sy * __ldg(Nhat + 3 * Ts + b), xz = sz * __ldg(Nhat + 4 * Ts + b),
             yz = sy * sz * __ldg(Nhat + 5 * Ts + b);
-    C* p0 = buf + (0 * W + w) * LS + t;
-    C* p1 = buf + (1 * W + w) * LS + t;
-    C* p2 = buf + (2 * W + w) * LS + t;
+    const int tp = COLS ? t + (t >> 4) : t;  // COLS blocks use padded lines (SmemLines PAD)
+    C* p0 = buf + (0 * W + w) * LS + tp;
+    C* p1 = buf + (1 * W + w) * LS + tp;
+    C* p2 = buf + (2 * W + w) * LS + tp;
     const C a = *p0, bb = *p1, c = *p2;
     *p0 = cmk<C>(xx * a.x + xy * bb.x + xz * c.x, xx * a.y + xy * bb.y + xz * c.y);
     *p1 = cmk<C>(xy * a.x + yy * bb.x + yz * c.x, xy * a.y + yy * bb.y + yz * c.y);
@@ -467,7 +468,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_ylines(const cpl
   C* a = reinterpret_cast<C*>(smem_raw);
   C* b = a + half;
   if (g.gate && !*g.gate) return;
-  const int Py = g.Py, LS = Py | 1, Hx = g.Hx, ny = g.ny, nz = g.nz;
+  const int Py = g.Py, LS = XT ? padded_line_stride(Py) : Py | 1, Hx = g.Hx, ny = g.ny, nz = g.nz;
   const int W = 1 << lgW;
   const int kx0 = blockIdx.x * W, z = blockIdx.y, c0 = blockIdx.z * ncompc;
   const int nlines = ncompc * W;
@@ -480,9 +481,9 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_ylines(const cpl
     // films (nz = 1): the three components of W columns, each contiguous
     const ColsIn<C, IX> cin{in, ny, lgW, kx0, Hx, ny};
     const ColsOut<C, IX> cout{out, ny, lgW, kx0, Hx, ny};
-    C* res = line_fft_to_smem<false, NT>(cin, a, b, LS, nlines, fnl, g.ply, twy, 1);
+    C* res = line_fft_to_smem<false, NT, true>(cin, a, b, LS, nlines, fnl, g.ply, twy, 1);
     tensor_product<R, true, NT, true>(res, LS, lgW, Py, g.fPy, kx0, 0, Nhat, Hx, Py, g.Pz);
-    line_fft_from_smem<true, NT>(res, res == a ? b : a, cout, LS, nlines, fnl, g.ply, twy, 1);
+    line_fft_from_smem<true, NT, true>(res, res == a ? b : a, cout, LS, nlines, fnl, g.ply, twy, 1);
   } else if (MODE == YL_CONV2D) {
     C* res = line_fft_to_smem<false, NT>(src, a, b, LS, nlines, fnl, g.ply, twy, 1);
     tensor_product<R, true, NT>(res, LS, lgW, Py, g.fPy, kx0, 0, Nhat, Hx, Py, g.Pz);
@@ -1165,7 +1166,7 @@ template <typename R>
 static size_t pass_smem(const DemagGeom& g, int which, bool fused2d, int W) {
   using C = cplx_t<R>;
   if (which == 1 || which == 3) return static_cast<size_t>(std::max(1, line_fft_buffers(g.ply))) * sizeof(C) * W * (g.Py | 1);
-  if (fused2d) return 2 * sizeof(C) * 3 * W * (g.Py | 1);
+  if (fused2d) return 2 * sizeof(C) * 3 * W * (g.xT ? padded_line_stride(g.Py) : g.Py | 1);
   const bool zc2 = (g.Pz & (g.Pz - 1)) == 0 && g.Pz >= 4 && (g.Pz <= 128 || (sizeof(R) == 4 && g.Pz == 256));
   return (zc2 ? 1 : 2) * sizeof(C) * 3 * W * (g.Pz | 1);
 }
@@ -1190,8 +1191,9 @@ static void launch_ylines(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* ou
   using C = cplx_t<R>;
   const int ncompc = MODE == YL_CONV2D ? 3 : 1;
   const int nbuf = MODE == YL_CONV2D ? 2 : line_fft_buffers(g.ply);
+  const bool xt = MODE == YL_CONV2D && g.xT;
   const int W = Wforce > 0 ? Wforce : lines_tile<R>(g.Hx, g.Py, ncompc, nbuf);
-  const int half = ncompc * W * (g.Py | 1);
+  const int half = ncompc * W * (xt ? padded_line_stride(g.Py) : g.Py | 1);
   dim3 grid((g.Hx + W - 1) / W, g.nz, 3 / ncompc);
   const size_t sm = static_cast<size_t>(std::max(1, nbuf)) * sizeof(C) * half;
   const FastDiv fnl = make_fastdiv(ncompc * W);

@@ -18,13 +18,21 @@
 
 namespace mm {
 
-template <typename C>
+// Lines in shared memory, element (line, pos) at line * LS + pos.  PAD
+// inserts one slot after every 16 elements (pos + pos / 16; LS >= padded
+// length): with few lines per block (the three components of one film
+// column), a warp spans consecutive butterflies of one line, whose Stockham
+// stores at stride R would otherwise fall into the same banks.
+template <typename C, bool PAD = false>
 struct SmemLines {
   C* b;
   int LS;
-  __device__ __forceinline__ C load(int line, int pos) const { return b[line * LS + pos]; }
-  __device__ __forceinline__ void store(int line, int pos, C v) const { b[line * LS + pos] = v; }
+  __device__ __forceinline__ int at(int line, int pos) const { return line * LS + (PAD ? pos + (pos >> 4) : pos); }
+  __device__ __forceinline__ C load(int line, int pos) const { return b[at(line, pos)]; }
+  __device__ __forceinline__ void store(int line, int pos, C v) const { b[at(line, pos)] = v; }
 };
+// line stride of PAD lines of length L
+__host__ __device__ __forceinline__ int padded_line_stride(int L) { return (L + (L >> 4)) | 1; }
 
 // rows of a spectrum array: element (line, pos) at
 // base[comp * comp_stride + pos * row_stride + kx0 + w], comp = line >> lgW.
@@ -172,12 +180,12 @@ __device__ void line_fft(const SRC& src, const DST& dst, C* a, C* b, int LS, int
 
 // All stages of pl from src into shared memory (a and b ping-pong); returns
 // the buffer that holds the result.
-template <bool INV, bool POW2, int NT, class SRC, typename C>
+template <bool INV, bool POW2, int NT, bool PAD, class SRC, typename C>
 __device__ __forceinline__ C* line_fft_to_smem_impl(const SRC& src, C* a, C* b, int LS, int nlines,
                                                     const FastDiv fnl, const FftPlan1 pl, const C* __restrict__ tw,
                                                     int tw_mul) {
   const int L = pl.L;
-  SmemLines<C> A{a, LS}, B{b, LS};
+  SmemLines<C, PAD> A{a, LS}, B{b, LS};
   if (pl.nst == 0) {
     for (int line = threadIdx.x; line < nlines; line += NT) A.store(line, 0, src.load(line, 0));
     __syncthreads();
@@ -191,7 +199,7 @@ __device__ __forceinline__ C* line_fft_to_smem_impl(const SRC& src, C* a, C* b, 
     R = plan_radix(pl, s);
     lstage_any<INV, POW2, NT>(R, A, B, L, nlines, fnl, p, tw, tw_mul);
     p *= R;
-    const SmemLines<C> t = A;
+    const SmemLines<C, PAD> t = A;
     A = B;
     B = t;
   }
@@ -199,12 +207,12 @@ __device__ __forceinline__ C* line_fft_to_smem_impl(const SRC& src, C* a, C* b, 
 }
 
 // All stages of pl from shared buffer x (y is free) into dst.
-template <bool INV, bool POW2, int NT, class DST, typename C>
+template <bool INV, bool POW2, int NT, bool PAD, class DST, typename C>
 __device__ __forceinline__ void line_fft_from_smem_impl(C* x, C* y, const DST& dst, int LS, int nlines,
                                                         const FastDiv fnl, const FftPlan1 pl,
                                                         const C* __restrict__ tw, int tw_mul) {
   const int L = pl.L;
-  SmemLines<C> A{x, LS}, B{y, LS};
+  SmemLines<C, PAD> A{x, LS}, B{y, LS};
   if (pl.nst == 0) {
     for (int line = threadIdx.x; line < nlines; line += NT) dst.store(line, 0, A.load(line, 0));
     __syncthreads();
@@ -215,25 +223,25 @@ __device__ __forceinline__ void line_fft_from_smem_impl(C* x, C* y, const DST& d
     const int R = plan_radix(pl, s);
     lstage_any<INV, POW2, NT>(R, A, B, L, nlines, fnl, p, tw, tw_mul);
     p *= R;
-    const SmemLines<C> t = A;
+    const SmemLines<C, PAD> t = A;
     A = B;
     B = t;
   }
   lstage_any<INV, POW2, NT>(plan_radix(pl, pl.nst - 1), A, dst, L, nlines, fnl, p, tw, tw_mul);
 }
 
-template <bool INV, int NT, class SRC, typename C>
+template <bool INV, int NT, bool PAD = false, class SRC, typename C>
 __device__ C* line_fft_to_smem(const SRC& src, C* a, C* b, int LS, int nlines, const FastDiv fnl, const FftPlan1 pl,
                                const C* __restrict__ tw, int tw_mul) {
-  if (pl.pow2) return line_fft_to_smem_impl<INV, true, NT>(src, a, b, LS, nlines, fnl, pl, tw, tw_mul);
-  return line_fft_to_smem_impl<INV, false, NT>(src, a, b, LS, nlines, fnl, pl, tw, tw_mul);
+  if (pl.pow2) return line_fft_to_smem_impl<INV, true, NT, PAD>(src, a, b, LS, nlines, fnl, pl, tw, tw_mul);
+  return line_fft_to_smem_impl<INV, false, NT, PAD>(src, a, b, LS, nlines, fnl, pl, tw, tw_mul);
 }
 
-template <bool INV, int NT, class DST, typename C>
+template <bool INV, int NT, bool PAD = false, class DST, typename C>
 __device__ void line_fft_from_smem(C* x, C* y, const DST& dst, int LS, int nlines, const FastDiv fnl,
                                    const FftPlan1 pl, const C* __restrict__ tw, int tw_mul) {
-  if (pl.pow2) line_fft_from_smem_impl<INV, true, NT>(x, y, dst, LS, nlines, fnl, pl, tw, tw_mul);
-  else line_fft_from_smem_impl<INV, false, NT>(x, y, dst, LS, nlines, fnl, pl, tw, tw_mul);
+  if (pl.pow2) line_fft_from_smem_impl<INV, true, NT, PAD>(x, y, dst, LS, nlines, fnl, pl, tw, tw_mul);
+  else line_fft_from_smem_impl<INV, false, NT, PAD>(x, y, dst, LS, nlines, fnl, pl, tw, tw_mul);
 }
 
 // Number of shared buffers line_fft needs for a plan (0 for one stage).

@@ -96,6 +96,7 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_fwd_x(
   const int64_t N = static_cast<int64_t>(rows) * nx;
   const int line0 = blockIdx.x * nl;
   const int nlh = min(nl, lines_total - line0);
+#pragma unroll 4  // several iterations' global loads in flight
   for (int e = threadIdx.x; e < nlh * Lc; e += NT) {
     const int l = fdiv(e, g.fLc), t = e - l * Lc;
     const int line = line0 + l;
@@ -185,6 +186,7 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_inv_x(
   };
   if (g.xT) {
     // column-major X: consecutive threads read consecutive rows of one kx
+#pragma unroll 4  // several iterations' global loads in flight
     for (int e = threadIdx.x; e < nl * Lc; e += NT) {
       const int k = fdiv(e, fnl), l = e - k * nl;
       if (l >= nlh) continue;
@@ -194,6 +196,7 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_inv_x(
       pre(l, k, xc[static_cast<int64_t>(k) * rows], cconj(xc[static_cast<int64_t>(Lc - k) * rows]));
     }
   } else {
+#pragma unroll 4  // several iterations' global loads in flight
     for (int e = threadIdx.x; e < nlh * Lc; e += NT) {
       const int l = fdiv(e, g.fLc), k = e - l * Lc;
       const C* xr = X + static_cast<int64_t>(line0 + l) * Hx;

@@ -827,8 +827,14 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
   g.frows = make_fastdiv(ny * nz);
   g.fpady = make_fastdiv(std::max(1, g.Py - ny));
   g.fpadz = make_fastdiv(std::max(1, g.Pz - nz));
-  fused2d = !long_y && (g.Pz == 1) && (2 * 3 * (g.Py | 1) * sizeof(C) <= static_cast<size_t>(smem_budget_bytes()));
-  g.xT = fused2d && g.Px > 1 && !long_x ? 1 : 0;  // the global-memory x stages keep rows
+  // films: the y transform, tensor product and inverse of a column run in one
+  // block when its three lines (two buffers) fit the tile budget, or, in the
+  // column-major layout, one block's shared memory (one column per block)
+  const bool cols_ok = g.Px > 1 && !long_x;  // the global-memory x stages keep rows
+  fused2d = !long_y && (g.Pz == 1) &&
+            (2 * 3 * (g.Py | 1) * sizeof(C) <= static_cast<size_t>(smem_budget_bytes()) ||
+             (cols_ok && 2 * 3 * static_cast<size_t>(padded_line_stride(g.Py)) * sizeof(C) <= kMaxSmem));
+  g.xT = fused2d && cols_ok ? 1 : 0;
   set_smem_attrs<R>();
   set_smem_attrs<double>();
   const int64_t nX = 3LL * nz * ny * g.Hx;

@@ -808,6 +808,17 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
              static_cast<int>(kMaxSmem / (6 * cR)) - 1);
     return -1;
   }
+  // films: the y transform, tensor product and inverse of a column run in one
+  // block when its three lines (two buffers) fit the tile budget, or, in the
+  // column-major layout, one block's shared memory (one column per block);
+  // longer film columns run the y transforms as global-memory stages
+  // (coalesced across kx) instead of one-column shared-memory tiles
+  const bool cols_ok = g.Px > 1 && !long_x;  // the global-memory x stages keep rows
+  fused2d = !long_y && (g.Pz == 1) &&
+            (2 * 3 * (g.Py | 1) * sizeof(C) <= static_cast<size_t>(smem_budget_bytes()) ||
+             (cols_ok && 2 * 3 * static_cast<size_t>(padded_line_stride(g.Py)) * sizeof(C) <= kMaxSmem));
+  if (g.Pz == 1 && !fused2d && cols_ok) long_y = true;
+  g.xT = fused2d && cols_ok ? 1 : 0;
   if ((long_x && !make_fft_plan(g.Lc, gplx, 8)) || (long_y && !make_fft_plan(g.Py, gply, 8))) {
     snprintf(err, nerr, "demag: no radix plan");
     return -1;
@@ -827,14 +838,6 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
   g.frows = make_fastdiv(ny * nz);
   g.fpady = make_fastdiv(std::max(1, g.Py - ny));
   g.fpadz = make_fastdiv(std::max(1, g.Pz - nz));
-  // films: the y transform, tensor product and inverse of a column run in one
-  // block when its three lines (two buffers) fit the tile budget, or, in the
-  // column-major layout, one block's shared memory (one column per block)
-  const bool cols_ok = g.Px > 1 && !long_x;  // the global-memory x stages keep rows
-  fused2d = !long_y && (g.Pz == 1) &&
-            (2 * 3 * (g.Py | 1) * sizeof(C) <= static_cast<size_t>(smem_budget_bytes()) ||
-             (cols_ok && 2 * 3 * static_cast<size_t>(padded_line_stride(g.Py)) * sizeof(C) <= kMaxSmem));
-  g.xT = fused2d && cols_ok ? 1 : 0;
   set_smem_attrs<R>();
   set_smem_attrs<double>();
   const int64_t nX = 3LL * nz * ny * g.Hx;

@@ -108,6 +108,28 @@ def test_demag_long_lines(mesh, form):
         assert rel_maxnorm(fn, fo) <= TENSOR_TOL
 
 
+@pytest.mark.parametrize("form", [0, 1])
+@pytest.mark.parametrize("mesh", [(100, 80, 1), (40, 600, 1), (24, 1300, 1), (6, 2400, 1)])
+def test_film_paths(mesh, form):
+    """The film paths by column length (padded y = 160, 1200, 2600, 4800):
+    the fused column-major y convolution within the tile budget or filling one
+    block (FP64 y = 1200, FP32 y = 2600), and the global-memory y stages for
+    columns that fit no block (FP64 y = 2600, both forms at y = 4800); field
+    and two RK4 steps against the oracle."""
+    from oracle.oracle import demag_tensor
+
+    nx, ny, nz = mesh
+    cfg = random_config(29 + nx + ny, nx, ny, nz, "", terms=("exch", "demag"), spatial=False)
+    T = demag_tensor(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, _ = build_oracle(cfg, tensor=T)
+    g = GpuSim(cfg, form=form, tensor=T)
+    tol = TOL64 if form == 0 else TOL32
+    assert rel_maxnorm(g.field(), o.effective_field()) <= tol
+    o.rk4(2e-14, 2)
+    g.rk4(2e-14, 2)
+    assert rel_maxnorm(g.m(), o.get_m()) <= (1e-11 if form == 0 else TOL32)
+
+
 def test_long_lines_rk4_and_dopri_fp64():
     """Stepping through the global-memory line stages, gated in the adaptive
     stepper's graph (y = 7500 film with exchange, anisotropy and Zeeman)."""

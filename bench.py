@@ -8,6 +8,9 @@ RK4) on B200 through libmmcuda's C ABI.
 One JSON line on rank 0.  Metric: LLG cell-steps/s = cells x RK4 steps / s,
 whole job (N replicas of the mesh under torchrun: the path has no exchange
 step between meshes, so ranks run independent replicas, scaling "weak").
+`e2e`: the same metric through the C ABI with pinned host arrays, copying m
+in and out every step; the FP32 form's host arrays are Float32 (sim.spin in
+the reference's Float32 mode), `e2e_f64_host` repeats it with Float64 arrays.
 
 Workloads (seeded synthetic inputs, numpy PCG64):
   c2  256x256x64 cells, 2 nm: exchange A=1e-11, bulk DMI 3e-3, Ku=5e5 along z,
@@ -503,31 +506,43 @@ def run_native(args):
         res["kernels"] = kern
         if fname == "fp32":
             # end to end through the public API with host buffers: per step,
-            # H2D of m from pinned memory, one RK4 step, D2H of m
-            pin_in = torch.from_numpy(m0.copy()).pin_memory()
-            pin_out = torch.empty(3 * n, dtype=torch.float64).pin_memory()
-            pin_in_p = ctypes.cast(pin_in.data_ptr(), ctypes.POINTER(ctypes.c_double))
-            pin_out_p = ctypes.cast(pin_out.data_ptr(), ctypes.POINTER(ctypes.c_double))
+            # H2D of m from pinned memory, one RK4 step, D2H of m.  The FP32
+            # form's host arrays are Float32 (sim.spin in the reference's
+            # Float32 mode: mm_set_m_f32 / mm_get_m_f32); the Float64-array
+            # boundary is reported beside it
             k2 = max(3, args.steps // 10)
-            for _ in range(2):
-                h.call("mm_set_m", pin_in_p)
-                h.call(step_fn, dt, 1)
-                h.call("mm_get_m", pin_out_p)
-            if dist is not None:
-                dist.barrier()
-            torch.cuda.synchronize()
-            e0.record(stream)
-            for _ in range(k2):
-                h.call("mm_set_m", pin_in_p)
-                h.call(step_fn, dt, 1)
-                h.call("mm_get_m", pin_out_p)
-            e1.record(stream)
-            e1.synchronize()
-            t = torch.tensor([e0.elapsed_time(e1)], device=f"cuda:{device}")
-            if dist is not None:
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            res["e2e"] = {"value": ws * n * k2 / (float(t.item()) / 1e3), "unit": "cell-steps/s",
-                          "h2d_bytes_per_step": 8 * 3 * n, "d2h_bytes_per_step": 8 * 3 * n, "steps": k2}
+
+            def e2e(f32):
+                dt_np, ct = (np.float32, ctypes.c_float) if f32 else (np.float64, ctypes.c_double)
+                pin_in = torch.from_numpy(m0.astype(dt_np)).pin_memory()
+                pin_out = torch.empty(3 * n, dtype=torch.float32 if f32 else torch.float64).pin_memory()
+                p_in = ctypes.cast(pin_in.data_ptr(), ctypes.POINTER(ct))
+                p_out = ctypes.cast(pin_out.data_ptr(), ctypes.POINTER(ct))
+                set_fn, get_fn = ("mm_set_m_f32", "mm_get_m_f32") if f32 else ("mm_set_m", "mm_get_m")
+                for _ in range(2):
+                    h.call(set_fn, p_in)
+                    h.call(step_fn, dt, 1)
+                    h.call(get_fn, p_out)
+                if dist is not None:
+                    dist.barrier()
+                torch.cuda.synchronize()
+                e0.record(stream)
+                for _ in range(k2):
+                    h.call(set_fn, p_in)
+                    h.call(step_fn, dt, 1)
+                    h.call(get_fn, p_out)
+                e1.record(stream)
+                e1.synchronize()
+                t = torch.tensor([e0.elapsed_time(e1)], device=f"cuda:{device}")
+                if dist is not None:
+                    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                nb = (4 if f32 else 8) * 3 * n
+                return {"value": ws * n * k2 / (float(t.item()) / 1e3), "unit": "cell-steps/s",
+                        "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb, "steps": k2,
+                        "host_dtype": "f32" if f32 else "f64"}
+
+            res["e2e"] = e2e(True)
+            res["e2e_f64_host"] = e2e(False)
         results[fname] = res
         h.close()
         del stream
@@ -551,8 +566,9 @@ def run_native(args):
         evals = 2 if heun else 1
         unit = "cell-evals/s" if heun else "cell-steps/s"
         if heun:
-            r["e2e"]["value"] *= evals
-            r["e2e"]["unit"] = unit
+            for k in ("e2e", "e2e_f64_host"):
+                r[k]["value"] *= evals
+                r[k]["unit"] = unit
         line = {
             "metric": ("LLG cell-evals/s (H_eff+demag+Heun, 2 evals per step)" if heun
                        else "LLG cell-steps/s (H_eff+demag+RK4)"),
@@ -568,6 +584,7 @@ def run_native(args):
                        "demag_tiles_autotuned": r.get("tiles"),
                        "parallelism": f"replicas x{ws}", "l2": "working set > 126 MB L2 (inputs larger than L2)"},
             "e2e": r["e2e"],
+            "e2e_f64_host": r["e2e_f64_host"],
             "gpu_launches": r["launches_per_step"] * args.steps,
             "fp64": ({"value": evals * results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
                       "fp32_over_fp64": r["value"] / results["fp64"]["value"]} if "fp64" in results else None),

@@ -100,6 +100,12 @@ int mm_set_Ms(mm_handle* h, const double* Ms, double Ms_uniform);
 int mm_set_m(mm_handle* h, const double* m_aos);
 /* sim.spin copy-out */
 int mm_get_m(mm_handle* h, double* m_aos);
+/* The same with a Float32 host array: sim.spin in the reference's Float32
+   mode (set_precision(Float32), src/MicroMagnetic.jl:22-38; sim.spin =
+   create_zeros(3n) of Float[], src/sim.jl:70).  Half the host<->device bytes
+   of the double calls; the state keeps its form's precision. */
+int mm_set_m_f32(mm_handle* h, const float* m_aos);
+int mm_get_m_f32(mm_handle* h, float* m_aos);
 /* set_pinning  src/sim.jl (sim.pins): NULL clears */
 int mm_set_pins(mm_handle* h, const uint8_t* pins);
 /* LLG driver parameters  src/driver.jl:15-21 (alpha, gamma, precession) */

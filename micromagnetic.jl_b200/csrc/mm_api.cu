@@ -69,6 +69,8 @@ class EngineBase {
   virtual int set_Ms(const double* Ms, double uni) = 0;
   virtual int set_m(const double* m) = 0;
   virtual int get_m(double* m) = 0;
+  virtual int set_m_f32(const float* m) = 0;
+  virtual int get_m_f32(float* m) = 0;
   virtual int set_pins(const uint8_t* p) = 0;
   virtual int set_llg(double alpha, double gamma, int prec) = 0;
   virtual int zeeman(const double* H, double hx, double hy, double hz, bool replace) = 0;
@@ -169,12 +171,21 @@ class Engine : public EngineBase {
     return MM_OK;
   }
 
-  int set_m(const double* mh) override {
+  int set_m(const double* mh) override { return set_m_t(mh); }
+  int set_m_f32(const float* mh) override { return set_m_t(mh); }
+  int get_m(double* mh) override { return get_m_t(mh); }
+  int get_m_f32(float* mh) override { return get_m_t(mh); }
+
+  // host AoS of T (double, or float in the reference's Float32 mode) through
+  // the FP64 staging buffer (3N doubles hold 3N floats)
+  template <typename T>
+  int set_m_t(const T* mh) {
     // NaN check of init_m0 (src/sim.jl:295-297), done by the conversion kernel
     int* flag = reinterpret_cast<int*>(scal + 63);
+    T* stage = reinterpret_cast<T*>(stage64);
     MM_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st_));
-    MM_CUDA(cudaMemcpyAsync(stage64, mh, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st_));
-    launch_aos_to_soa<R>(stage64, m, m_lo, N, flag, st_);
+    MM_CUDA(cudaMemcpyAsync(stage, mh, sizeof(T) * 3 * N, cudaMemcpyHostToDevice, st_));
+    launch_aos_to_soa<R, T>(stage, m, m_lo, N, flag, st_);
     int hflag = 0;
     MM_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, st_));
     MM_CUDA(cudaStreamSynchronize(st_));
@@ -189,9 +200,11 @@ class Engine : public EngineBase {
     return MM_OK;
   }
 
-  int get_m(double* mh) override {
-    launch_soa_to_aos<R>(m, m_lo, stage64, N, st_);
-    MM_CUDA(cudaMemcpyAsync(mh, stage64, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st_));
+  template <typename T>
+  int get_m_t(T* mh) {
+    T* stage = reinterpret_cast<T*>(stage64);
+    launch_soa_to_aos<R, T>(m, m_lo, stage, N, st_);
+    MM_CUDA(cudaMemcpyAsync(mh, stage, sizeof(T) * 3 * N, cudaMemcpyDeviceToHost, st_));
     MM_CUDA(cudaStreamSynchronize(st_));
     return MM_OK;
   }
@@ -1453,6 +1466,16 @@ int mm_get_m(mm_handle* h, double* m) {
   MM_HANDLE(h);
   if (!m) return fail(MM_ERR_ARG, "null m");
   MM_GUARD(h->eng->get_m(m));
+}
+int mm_set_m_f32(mm_handle* h, const float* m) {
+  MM_HANDLE(h);
+  if (!m) return fail(MM_ERR_ARG, "null m");
+  MM_GUARD(h->eng->set_m_f32(m));
+}
+int mm_get_m_f32(mm_handle* h, float* m) {
+  MM_HANDLE(h);
+  if (!m) return fail(MM_ERR_ARG, "null m");
+  MM_GUARD(h->eng->get_m_f32(m));
 }
 int mm_set_pins(mm_handle* h, const uint8_t* p) { MM_HANDLE(h); MM_GUARD(h->eng->set_pins(p)); }
 int mm_set_llg(mm_handle* h, double a, double g, int p) { MM_HANDLE(h); MM_GUARD(h->eng->set_llg(a, g, p)); }

@@ -686,14 +686,15 @@ void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<
 }
 
 // --------------------------------------------------------- conversions ---
-template <typename R>
-__global__ void k_aos_to_soa(const double* __restrict__ aos, R* __restrict__ hi, R* __restrict__ lo, int64_t N,
+// host element type T: double, or float (the reference's Float32 mode)
+template <typename R, typename T>
+__global__ void k_aos_to_soa(const T* __restrict__ aos, R* __restrict__ hi, R* __restrict__ lo, int64_t N,
                              int* __restrict__ nanflag) {
   const int64_t I = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   if (I >= N) return;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const double v = aos[3 * I + c];
+    const double v = static_cast<double>(aos[3 * I + c]);
     if (nanflag && isnan(v)) *nanflag = 1;
     const R h = static_cast<R>(v);
     hi[c * N + I] = h;
@@ -701,15 +702,15 @@ __global__ void k_aos_to_soa(const double* __restrict__ aos, R* __restrict__ hi,
   }
 }
 
-template <typename R>
-__global__ void k_soa_to_aos(const R* __restrict__ hi, const R* __restrict__ lo, double* __restrict__ aos, int64_t N) {
+template <typename R, typename T>
+__global__ void k_soa_to_aos(const R* __restrict__ hi, const R* __restrict__ lo, T* __restrict__ aos, int64_t N) {
   const int64_t I = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   if (I >= N) return;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     double v = static_cast<double>(hi[c * N + I]);
     if (lo) v += static_cast<double>(lo[c * N + I]);
-    aos[3 * I + c] = v;
+    aos[3 * I + c] = static_cast<T>(v);
   }
 }
 
@@ -719,13 +720,13 @@ __global__ void k_scalar_to_R(const double* __restrict__ a, R* __restrict__ b, i
   if (i < n) b[i] = static_cast<R>(a[i] * scale);
 }
 
-template <typename R>
-void launch_aos_to_soa(const double* aos, R* hi, R* lo, int64_t N, int* nanflag, cudaStream_t st) {
-  k_aos_to_soa<R><<<stage_blocks(N), kStageThreads, 0, st>>>(aos, hi, lo, N, nanflag);
+template <typename R, typename T>
+void launch_aos_to_soa(const T* aos, R* hi, R* lo, int64_t N, int* nanflag, cudaStream_t st) {
+  k_aos_to_soa<R, T><<<stage_blocks(N), kStageThreads, 0, st>>>(aos, hi, lo, N, nanflag);
 }
-template <typename R>
-void launch_soa_to_aos(const R* hi, const R* lo, double* aos, int64_t N, cudaStream_t st) {
-  k_soa_to_aos<R><<<stage_blocks(N), kStageThreads, 0, st>>>(hi, lo, aos, N);
+template <typename R, typename T>
+void launch_soa_to_aos(const R* hi, const R* lo, T* aos, int64_t N, cudaStream_t st) {
+  k_soa_to_aos<R, T><<<stage_blocks(N), kStageThreads, 0, st>>>(hi, lo, aos, N);
 }
 template <typename R>
 void launch_scalar_to_R(const double* a, R* b, int64_t n, double scale, cudaStream_t st) {
@@ -1065,8 +1066,10 @@ void launch_adj_field(const FieldArgs<R>& fa_lin, const R* w, const R* q, const 
 #define MM_INST(R)                                                                                       \
   template void launch_stage<R>(int, const FieldArgs<R>&, const R*, const StageArgs<R>&, cudaStream_t); \
   template void launch_nbmask<R>(int, int, int, int, const R*, uint8_t*, cudaStream_t);                 \
-  template void launch_aos_to_soa<R>(const double*, R*, R*, int64_t, int*, cudaStream_t);                     \
-  template void launch_soa_to_aos<R>(const R*, const R*, double*, int64_t, cudaStream_t);               \
+  template void launch_aos_to_soa<R, double>(const double*, R*, R*, int64_t, int*, cudaStream_t);           \
+  template void launch_aos_to_soa<R, float>(const float*, R*, R*, int64_t, int*, cudaStream_t);             \
+  template void launch_soa_to_aos<R, double>(const R*, const R*, double*, int64_t, cudaStream_t);           \
+  template void launch_soa_to_aos<R, float>(const R*, const R*, float*, int64_t, cudaStream_t);             \
   template void launch_scalar_to_R<R>(const double*, R*, int64_t, double, cudaStream_t);                \
   template void launch_average_m<R>(const R*, const R*, int64_t, double*, double*, cudaStream_t);      \
   template void launch_thermal<R>(uint64_t, const long long*, const double*, double, double, const R*, double,   \

@@ -148,11 +148,11 @@ StageGrid stage_grid(int nx, int ny, int nz);
 template <typename R>
 void launch_nbmask(int nx, int ny, int nz, int pbc, const R* Ms, uint8_t* nbm, cudaStream_t st);
 
-// AoS double <-> SoA R (+ compensated low part)
-template <typename R>
-void launch_aos_to_soa(const double* aos, R* hi, R* lo, int64_t N, int* nanflag, cudaStream_t st);
-template <typename R>
-void launch_soa_to_aos(const R* hi, const R* lo, double* aos, int64_t N, cudaStream_t st);
+// AoS T (double or float) <-> SoA R (+ compensated low part)
+template <typename R, typename T = double>
+void launch_aos_to_soa(const T* aos, R* hi, R* lo, int64_t N, int* nanflag, cudaStream_t st);
+template <typename R, typename T = double>
+void launch_soa_to_aos(const R* hi, const R* lo, T* aos, int64_t N, cudaStream_t st);
 template <typename R>
 void launch_scalar_to_R(const double* a, R* b, int64_t n, double scale, cudaStream_t st);
 

@@ -74,7 +74,7 @@ function attach!(sim::MicroMagnetic.MicroSim; form::Symbol=:fp64, device::Intege
     finalizer(x -> ccall((:mm_destroy, libmmcuda), Cint, (Ptr{Cvoid},), x.ptr), h)
     Ms = f64(sim.mu0_Ms) ./ MicroMagnetic.mu_0
     check(ccall((:mm_set_Ms, libmmcuda), Cint, (Ptr{Cvoid}, Ptr{Float64}, Float64), h.ptr, Ms, 0.0))
-    check(ccall((:mm_set_m, libmmcuda), Cint, (Ptr{Cvoid}, Ptr{Float64}), h.ptr, f64(sim.spin)))
+    push_spin!(h, sim.spin)
     pins = UInt8.(Array(sim.pins))
     check(ccall((:mm_set_pins, libmmcuda), Cint, (Ptr{Cvoid}, Ptr{UInt8}), h.ptr, pins))
     drv = sim.driver
@@ -120,9 +120,26 @@ add_term!(h, t) = error("term $(typeof(t)) is not on the accelerated path")
 
 handle(sim) = get(HANDLES, sim, nothing)
 
+# sim.spin crosses the boundary in its own element type: Float32 in the
+# reference's Float32 mode (set_precision(Float32), src/MicroMagnetic.jl:22-38)
+function push_spin!(h, spin)
+    a = Array(spin)
+    if eltype(a) == Float32
+        check(ccall((:mm_set_m_f32, libmmcuda), Cint, (Ptr{Cvoid}, Ptr{Float32}), h.ptr, Vector{Float32}(a)))
+    else
+        check(ccall((:mm_set_m, libmmcuda), Cint, (Ptr{Cvoid}, Ptr{Float64}), h.ptr, f64(a)))
+    end
+    return nothing
+end
+
 function pull_spin!(sim, h)
-    m = Vector{Float64}(undef, 3 * h.n)
-    check(ccall((:mm_get_m, libmmcuda), Cint, (Ptr{Cvoid}, Ptr{Float64}), h.ptr, m))
+    if eltype(sim.spin) == Float32
+        m = Vector{Float32}(undef, 3 * h.n)
+        check(ccall((:mm_get_m_f32, libmmcuda), Cint, (Ptr{Cvoid}, Ptr{Float32}), h.ptr, m))
+    else
+        m = Vector{Float64}(undef, 3 * h.n)
+        check(ccall((:mm_get_m, libmmcuda), Cint, (Ptr{Cvoid}, Ptr{Float64}), h.ptr, m))
+    end
     copyto!(sim.spin, m)
     return sim.spin
 end
@@ -131,7 +148,7 @@ end
 function effective_field(sim::MicroMagnetic.MicroSim, spin, t::Float64=0.0)
     h = handle(sim)
     h === nothing && return invoke(effective_field, Tuple{MicroMagnetic.AbstractSim,Any,Float64}, sim, spin, t)
-    check(ccall((:mm_set_m, libmmcuda), Cint, (Ptr{Cvoid}, Ptr{Float64}), h.ptr, f64(spin)))
+    push_spin!(h, spin)
     H = Vector{Float64}(undef, 3 * h.n)
     check(ccall((:mm_effective_field, libmmcuda), Cint, (Ptr{Cvoid}, Ptr{Float64}), h.ptr, H))
     copyto!(sim.field, H)

@@ -37,7 +37,7 @@ DRIVER_SD, DRIVER_LLG = 0, 1
 # every exported symbol of include/mmcuda.h
 EXPORTS = (
     "mm_abi_version", "mm_last_error", "mm_create", "mm_destroy", "mm_get_stream", "mm_synchronize",
-    "mm_device_bytes", "mm_set_Ms", "mm_set_m", "mm_get_m", "mm_set_pins", "mm_set_llg", "mm_add_zeeman",
+    "mm_device_bytes", "mm_set_Ms", "mm_set_m", "mm_get_m", "mm_set_m_f32", "mm_get_m_f32", "mm_set_pins", "mm_set_llg", "mm_add_zeeman",
     "mm_update_zeeman", "mm_add_exch", "mm_add_dmi_bulk", "mm_add_dmi_interfacial", "mm_add_anis",
     "mm_add_demag", "mm_add_demag_tensor", "mm_effective_field", "mm_term_field", "mm_energy",
     "mm_llg_rhs", "mm_average_m", "mm_rk4_run", "mm_rk4_state", "mm_dopri_set_tol", "mm_run_until",
@@ -73,6 +73,7 @@ class Stats(ctypes.Structure):
 
 _lib = None
 _dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
 _vp = ctypes.c_void_p
 
 
@@ -96,6 +97,8 @@ def load():
         "mm_set_Ms": ([_vp, _dp, d], i),
         "mm_set_m": ([_vp, _dp], i),
         "mm_get_m": ([_vp, _dp], i),
+        "mm_set_m_f32": ([_vp, _fp], i),
+        "mm_get_m_f32": ([_vp, _fp], i),
         "mm_set_pins": ([_vp, ctypes.POINTER(ctypes.c_uint8)], i),
         "mm_set_llg": ([_vp, d, d, i], i),
         "mm_add_zeeman": ([_vp, _dp, d, d, d], i),
@@ -168,6 +171,13 @@ def dptr(a: np.ndarray | None):
     return a.ctypes.data_as(_dp)
 
 
+def fptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_fp)
+
+
 class Batch:
     """Owns one mm_batch over a list of Handles (kept alive by the batch)."""
 
@@ -237,13 +247,23 @@ class Handle:
         self.call("mm_rk4_launches_per_step", ctypes.byref(n))
         return n.value
 
-    def get_m(self, out=None):
-        out = np.empty(3 * self.n) if out is None else out
-        self.call("mm_get_m", dptr(out))
+    def get_m(self, out=None, dtype=np.float64):
+        """m (AoS); dtype float32 copies out through mm_get_m_f32."""
+        f32 = (out.dtype if out is not None else np.dtype(dtype)) == np.float32
+        out = np.empty(3 * self.n, dtype=np.float32 if f32 else np.float64) if out is None else out
+        if f32:
+            self.call("mm_get_m_f32", fptr(out))
+        else:
+            self.call("mm_get_m", dptr(out))
         return out
 
     def set_m(self, m):
-        a = np.ascontiguousarray(m, dtype=np.float64).reshape(-1)
+        """m (AoS); a float32 array is copied in through mm_set_m_f32."""
+        f32 = isinstance(m, np.ndarray) and m.dtype == np.float32
+        a = np.ascontiguousarray(m, dtype=np.float32 if f32 else np.float64).reshape(-1)
         if a.size != 3 * self.n:
             raise ValueError("m must have 3N entries")
-        self.call("mm_set_m", dptr(a))
+        if f32:
+            self.call("mm_set_m_f32", fptr(a))
+        else:
+            self.call("mm_set_m", dptr(a))

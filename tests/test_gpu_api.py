@@ -91,3 +91,46 @@ def test_ovf_sim(api, tmp_path, ovf_type):
     assert ovf.name == "saving" and len(ovf.data) == 6 and np.max(np.abs(ovf.data - m)) < 1e-6
     sim.close()
     sim2.close()
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_float32_host_boundary(form):
+    """mm_set_m_f32 / mm_get_m_f32: sim.spin as a Float32 array (the
+    reference's set_precision(Float32)) crosses the ABI unchanged, gives the
+    same field as the Float64 copy of the same values, and is NaN-checked."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from mmcuda import _lib
+
+    nx, ny, nz = 24, 20, 3
+    n = nx * ny * nz
+    rng = np.random.default_rng(41)
+    m = rng.normal(size=(n, 3))
+    m /= np.linalg.norm(m, axis=1, keepdims=True)
+    m32 = m.astype(np.float32).reshape(-1)
+    hs = []
+    for f32_in in (True, False):
+        h = _lib.Handle(nx, ny, nz, 2e-9, 2e-9, 2e-9, 0, form, 0)
+        h.call("mm_set_Ms", None, 6e5)
+        h.call("mm_add_exch", None, 1.3e-11, 1.3e-11, 1.3e-11)
+        h.call("mm_add_demag", 0, 0, 0)
+        h.set_m(m32 if f32_in else m32.astype(np.float64))
+        hs.append(h)
+    assert np.array_equal(hs[0].get_m(), m32.astype(np.float64))
+    assert np.array_equal(hs[0].get_m(dtype=np.float32), m32)
+    f = []
+    for h in hs:
+        out = np.empty(3 * n)
+        h.call("mm_effective_field", _lib.dptr(out))
+        f.append(out)
+    assert np.array_equal(f[0], f[1])
+    hs[1].set_m(m.reshape(-1))
+    got = hs[1].get_m(dtype=np.float32)
+    assert np.allclose(got, m.reshape(-1).astype(np.float32), rtol=2 ** -23, atol=0)
+    bad = m32.copy()
+    bad[7] = np.nan
+    with pytest.raises(_lib.MMError):
+        hs[0].set_m(bad)
+    for h in hs:
+        h.close()

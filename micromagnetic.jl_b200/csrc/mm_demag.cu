@@ -72,6 +72,16 @@ static int smem_budget_bytes() {
 }
 
 
+// 3-D column-major spectra (DemagGeom::yT) unless MMCUDA_COLS3D=0 keeps the
+// row-major layout; both run the same arithmetic on every line
+static bool cols3d_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MMCUDA_COLS3D");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 // ============================================================== kernels ====
 template <typename R> struct Vec2;
 template <> struct Vec2<float> { using T = float2; };
@@ -491,6 +501,13 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_ylines(const cpl
     C* res = line_fft_to_smem<false, NT>(src, a, b, LS, nlines, fnl, g.ply, twy, 1);
     tensor_product<R, true, NT>(res, LS, lgW, Py, g.fPy, kx0, 0, Nhat, Hx, Py, g.Pz);
     line_fft_from_smem<true, NT>(res, res == a ? b : a, dst, LS, nlines, fnl, g.ply, twy, 1);
+  } else if (XT) {
+    // 3-D column-major spectra (DemagGeom::yT): W contiguous columns of plane z
+    // of one component, X[((c*Hx + kx)*nz + z)*ny + y] <-> Y[((c*Hx + kx)*nz + z)*Py + ky]
+    const int lin = MODE == YL_INV ? Py : ny, lout = MODE == YL_FWD ? Py : ny;
+    const ColsIn<C, IX> cin{in + (static_cast<int64_t>(c0) * Hx * nz + z) * lin, nz * lin, lgW, kx0, Hx, lin};
+    const ColsOut<C, IX> cout{out + (static_cast<int64_t>(c0) * Hx * nz + z) * lout, nz * lout, lgW, kx0, Hx, lout};
+    line_fft<MODE == YL_INV, NT, true>(cin, cout, a, b, LS, nlines, fnl, g.ply, twy, 1);
   } else {
     line_fft<MODE == YL_INV, NT>(src, dst, a, b, LS, nlines, fnl, g.ply, twy, 1);
   }
@@ -530,7 +547,11 @@ __global__ void __launch_bounds__(NT, 2) k_zconv(cplx_t<R>* Y, const R* __restri
 // inputs are the same positions), written back in place after a barrier;
 // finally the inverse radix-RA stage straight to the Y rows kz < nz.
 // One shared buffer; requires W * RA <= NT (one middle task per thread).
-template <typename R, int RA, int RB, int NT, bool I32>
+// YT (column-major spectra, DemagGeom::yT): a block takes one kx and a tile of
+// W consecutive ky (grid: (Hx, ky tiles), tile q and its mirror Py/W-1-q
+// adjacent in launch order); the tile's rows are W contiguous entries of
+// Y[((c*Hx + kx)*nz + z)*Py + ky], the tensor Nhat[((c*Tzq + kz)*Hx + kx)*Tyq + ky].
+template <typename R, int RA, int RB, int NT, bool I32, bool YT = false>
 __global__ void __launch_bounds__(NT, (zconv2_minb<R, NT>())) k_zconv2(cplx_t<R>* Y, const R* __restrict__ Nhat, DemagGeom g, int lgW,
                                                   FastDiv fnl, const cplx_t<R>* __restrict__ twz) {
   using C = cplx_t<R>;
@@ -541,21 +562,32 @@ __global__ void __launch_bounds__(NT, (zconv2_minb<R, NT>())) k_zconv2(cplx_t<R>
   if (g.gate && !*g.gate) return;
   const int LS = L | 1, Hx = g.Hx, Py = g.Py, nz = g.nz;
   const int W = 1 << lgW;
-  const int kx0 = blockIdx.x * W;
   const int bq = blockIdx.y;
-  const int q = (bq + 1) >> 1;
-  const int ky = bq == 0 ? 0 : ((bq & 1) ? q : Py - q);
+  int kx0, ky0;  // first column of the tile: (kx0 + w, ky0) or, YT, (kx0, ky0 + w)
+  if (YT) {
+    const int nq = gridDim.y;
+    kx0 = blockIdx.x;
+    ky0 = ((bq & 1) ? nq - 1 - (bq >> 1) : (bq >> 1)) << lgW;
+  } else {
+    const int q = (bq + 1) >> 1;
+    kx0 = blockIdx.x * W;
+    ky0 = bq == 0 ? 0 : ((bq & 1) ? q : Py - q);
+  }
   const int nlines = 3 * W;
-  const IX cs = static_cast<IX>(static_cast<int64_t>(nz) * Py * Hx), rs = static_cast<IX>(static_cast<int64_t>(Py) * Hx);
-  RowsIn<C, IX> src{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
-  RowsOut<C, IX> dst{Y + static_cast<int64_t>(ky) * Hx, cs, rs, lgW, kx0, Hx, nz};
+  // rows of the tile: element (c, z, w) at base + c*cs + z*rs + (t0 + w), t0 + w < tn
+  const IX cs = static_cast<IX>(static_cast<int64_t>(nz) * Py * Hx), rs = static_cast<IX>(YT ? Py : static_cast<int64_t>(Py) * Hx);
+  C* base = YT ? Y + static_cast<int64_t>(kx0) * nz * Py : Y + static_cast<int64_t>(ky0) * Hx;
+  const int t0 = YT ? ky0 : kx0, tn = YT ? Py : Hx;
+  RowsIn<C, IX> src{base, cs, rs, lgW, t0, tn, nz};
+  RowsOut<C, IX> dst{base, cs, rs, lgW, t0, tn, nz};
   SmemLines<C> A{a, LS};
   lstage<RA, false, true, NT>(src, A, L, nlines, fnl, 1, twz, 1);
   // fused middle: thread -> (w, i), w fastest
   const int task = threadIdx.x;
   const bool act = task < W * RA;
   const int w = task & (W - 1), i = task >> lgW;
-  const int kx = kx0 + w;
+  const int kx = YT ? kx0 : kx0 + w;
+  const int ky = YT ? ky0 + w : ky0;
   C v[3][RB];
   if (act) {
 #pragma unroll
@@ -567,7 +599,7 @@ __global__ void __launch_bounds__(NT, (zconv2_minb<R, NT>())) k_zconv2(cplx_t<R>
       for (int r = 1; r < RB; ++r) v[c][r] = cmul(v[c][r], __ldg(twz + r * i));
       dftR<RB, false>(v[c]);
     }
-    if (kx < Hx) {
+    if (kx < Hx && ky < Py) {
       const int Tyq = Py / 2 + 1, Tzq = L / 2 + 1;
       const int64_t Ts = static_cast<int64_t>(Tzq) * Tyq * Hx;
       const bool fy = ky > Py / 2;
@@ -579,7 +611,8 @@ __global__ void __launch_bounds__(NT, (zconv2_minb<R, NT>())) k_zconv2(cplx_t<R>
         const bool fz = kz > L / 2;
         const int kzq = fz ? L - kz : kz;
         const R sz = fz ? R(-1) : R(1);
-        const int64_t b = (static_cast<int64_t>(kzq) * Tyq + kyq) * Hx + kx;
+        const int64_t b = YT ? (static_cast<int64_t>(kzq) * Hx + kx) * Tyq + kyq
+                             : (static_cast<int64_t>(kzq) * Tyq + kyq) * Hx + kx;
         const R xx = __ldg(Nhat + b), yy = __ldg(Nhat + Ts + b), zz = __ldg(Nhat + 2 * Ts + b);
         const R xy = sy * __ldg(Nhat + 3 * Ts + b), xz = sz * __ldg(Nhat + 4 * Ts + b),
                 yz = sy * sz * __ldg(Nhat + 5 * Ts + b);
@@ -604,10 +637,11 @@ __global__ void __launch_bounds__(NT, (zconv2_minb<R, NT>())) k_zconv2(cplx_t<R>
   lstage<RA, true, true, NT>(A, dst, L, nlines, fnl, RB, twz, 1);
 }
 
-// FP64 film tensor quadrant [6][Tyq][Hx] (Tzq = 1) to RO, column-major [6][Hx][Tyq]
+// FP64 tensor quadrant [6][Tzq][Tyq][Hx] to RO, column-major [6][Tzq][Hx][Tyq]
+// (films: Tzq = 1)
 template <typename RO>
-__global__ void k_cast_cols(const double* __restrict__ a, RO* __restrict__ b, int Tyq, int Hx) {
-  const int64_t plane = static_cast<int64_t>(Tyq) * Hx, n = 6 * plane;
+__global__ void k_cast_cols(const double* __restrict__ a, RO* __restrict__ b, int Tyq, int Hx, int Tzq) {
+  const int64_t plane = static_cast<int64_t>(Tyq) * Hx, n = 6LL * Tzq * plane;
   for (int64_t o = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; o < n;
        o += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t c = o / plane, r = o - c * plane;
@@ -756,6 +790,10 @@ static void set_smem_attrs_nt() {
   cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_FWD, NT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_FWD, NT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_INV, NT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_ylines<R, YL_INV, NT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_zconv<R, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
 
@@ -782,6 +820,9 @@ DemagPlan<R>::~DemagPlan() {
   cudaFree(twy);
   cudaFree(twz);
 }
+
+template <typename R>
+static int lines_tile(int Hx, int L, int lines_per_col, int nbuf);
 
 template <typename R>
 int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_t nerr) {
@@ -819,6 +860,16 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
              (cols_ok && 2 * 3 * static_cast<size_t>(padded_line_stride(g.Py)) * sizeof(C) <= kMaxSmem));
   if (g.Pz == 1 && !fused2d && cols_ok) long_y = true;
   g.xT = fused2d && cols_ok ? 1 : 0;
+  // 3-D meshes whose shared-memory y lines leave row tiles narrower than 8
+  // columns (16- to 64-byte row segments) keep the spectra column-major
+  // (DemagGeom::yT) when the z convolution is the fused power-of-two kernel
+  g.yT = 0;
+  const bool zc2 = (g.Pz & (g.Pz - 1)) == 0 && g.Pz >= 4 && (g.Pz <= 128 || (sizeof(R) == 4 && g.Pz == 256));
+  if (g.Pz > 1 && !long_y && cols_ok && zc2 && cols3d_enabled()) {
+    FftPlan1 py;
+    make_fft_plan(g.Py, py, sizeof(R) == 4 ? 32 : 8);
+    if (lines_tile<R>(g.Hx, g.Py, 1, std::max(1, line_fft_buffers(py))) < 8) g.yT = g.xT = 1;
+  }
   if ((long_x && !make_fft_plan(g.Lc, gplx, 8)) || (long_y && !make_fft_plan(g.Py, gply, 8))) {
     snprintf(err, nerr, "demag: no radix plan");
     return -1;
@@ -1177,7 +1228,9 @@ static int lines_tile(int Hx, int L, int lines_per_col, int nbuf) {
 template <typename R>
 static size_t pass_smem(const DemagGeom& g, int which, bool fused2d, int W) {
   using C = cplx_t<R>;
-  if (which == 1 || which == 3) return static_cast<size_t>(std::max(1, line_fft_buffers(g.ply))) * sizeof(C) * W * (g.Py | 1);
+  if (which == 1 || which == 3)
+    return static_cast<size_t>(std::max(1, line_fft_buffers(g.ply))) * sizeof(C) * W *
+           (g.yT ? padded_line_stride(g.Py) : g.Py | 1);
   if (fused2d) return 2 * sizeof(C) * 3 * W * (g.xT ? padded_line_stride(g.Py) : g.Py | 1);
   const bool zc2 = (g.Pz & (g.Pz - 1)) == 0 && g.Pz >= 4 && (g.Pz <= 128 || (sizeof(R) == 4 && g.Pz == 256));
   return (zc2 ? 1 : 2) * sizeof(C) * 3 * W * (g.Pz | 1);
@@ -1203,20 +1256,18 @@ static void launch_ylines(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* ou
   using C = cplx_t<R>;
   const int ncompc = MODE == YL_CONV2D ? 3 : 1;
   const int nbuf = MODE == YL_CONV2D ? 2 : line_fft_buffers(g.ply);
-  const bool xt = MODE == YL_CONV2D && g.xT;
+  const bool xt = MODE == YL_CONV2D ? g.xT != 0 : g.yT != 0;
   const int W = Wforce > 0 ? Wforce : lines_tile<R>(g.Hx, g.Py, ncompc, nbuf);
   const int half = ncompc * W * (xt ? padded_line_stride(g.Py) : g.Py | 1);
   dim3 grid((g.Hx + W - 1) / W, g.nz, 3 / ncompc);
   const size_t sm = static_cast<size_t>(std::max(1, nbuf)) * sizeof(C) * half;
   const FastDiv fnl = make_fastdiv(ncompc * W);
-  if constexpr (MODE == YL_CONV2D) {
-    if (g.xT) {
-      if (offsets_fit_int(g))
-        k_ylines<R, MODE, kHotNT, true, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
-      else
-        k_ylines<R, MODE, kHotNT, false, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
-      return;
-    }
+  if (xt) {
+    if (offsets_fit_int(g))
+      k_ylines<R, MODE, kHotNT, true, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
+    else
+      k_ylines<R, MODE, kHotNT, false, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
+    return;
   }
   if (offsets_fit_int(g))
     k_ylines<R, MODE, kHotNT, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
@@ -1230,22 +1281,35 @@ static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const
   using C = cplx_t<R>;
   constexpr int L = RA * RB;
   constexpr int NTZ = zconv2_nt<R>();
-  int W = Wforce > 0 ? Wforce : lines_tile<R>(g.Hx, L, 3, 1);
+  // tiles of W columns along kx, or along ky for column-major spectra (yT)
+  int W = Wforce > 0 ? Wforce : lines_tile<R>(g.yT ? g.Py : g.Hx, L, 3, 1);
   while (W * RA > NTZ) W /= 2;
   const size_t sm = sizeof(C) * 3 * W * (L | 1);
   static uint64_t done = 0;
   int dev = 0;
   cudaGetDevice(&dev);
   if (!((done >> dev) & 1ull)) {
-    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
-    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
+    const int mx = static_cast<int>(kMaxSmem);
+    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
     done |= 1ull << dev;
+  }
+  const FastDiv fnl = make_fastdiv(3 * W);
+  if (g.yT) {
+    dim3 grid(g.Hx, (g.Py + W - 1) / W, 1);
+    if (offsets_fit_int(g))
+      k_zconv2<R, RA, RB, NTZ, true, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz);
+    else
+      k_zconv2<R, RA, RB, NTZ, false, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz);
+    return;
   }
   dim3 grid((g.Hx + W - 1) / W, g.Py, 1);
   if (offsets_fit_int(g))
-    k_zconv2<R, RA, RB, NTZ, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz);
+    k_zconv2<R, RA, RB, NTZ, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz);
   else
-    k_zconv2<R, RA, RB, NTZ, false><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz);
+    k_zconv2<R, RA, RB, NTZ, false><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz);
 }
 
 // Power-of-two z lengths with a fused-middle kernel: L = RA * RB
@@ -1409,14 +1473,15 @@ int DemagPlan<R>::autotune(const R* m, const R* mu0Ms, R* Hd, cudaStream_t st) {
     int W0 = 1;
     {
       const int nb = which == 2 ? (fused2d ? 2 : (zc2 ? 1 : 2)) : std::max(1, line_fft_buffers(g.ply));
-      W0 = which == 2 && !fused2d ? lines_tile<R>(g.Hx, g.Pz, 3, nb) : lines_tile<R>(g.Hx, g.Py, which == 2 ? 3 : 1, nb);
+      W0 = which == 2 && !fused2d ? lines_tile<R>(g.yT ? g.Py : g.Hx, g.Pz, 3, nb)
+                                  : lines_tile<R>(g.Hx, g.Py, which == 2 ? 3 : 1, nb);
       if (which == 2 && zc2)
         while (W0 * ra > zconv2_nt<R>()) W0 /= 2;
     }
     float ms0 = 0.f, best = 1e30f;
     int bestW = W0;
     for (int W = 1; W <= wmax; W *= 2) {
-      if (W / 2 >= g.Hx) break;
+      if (W / 2 >= (which == 2 && g.yT ? g.Py : g.Hx)) break;
       if (pass_smem<R>(g, which, fused2d, W) > kMaxSmem) break;
       if (which == 2 && zc2 && W * ra > zconv2_nt<R>()) break;
       tile[which] = W;
@@ -1538,7 +1603,7 @@ int DemagPlan<R>::set_tensor(const double* T6N, cudaStream_t st) {
         launch_zpass<double, ZM_TENSOR_Q, NT>(g64, Y64, nullptr, Tq + c * Ts, 1, g.Tyq, tz, sz, scale, st);
       }
     }
-    if (g.xT) k_cast_cols<R><<<1024, 256, 0, st>>>(Tq, Nhat, g.Tyq, g.Hx);
+    if (g.xT) k_cast_cols<R><<<1024, 256, 0, st>>>(Tq, Nhat, g.Tyq, g.Hx, g.Tzq);
     else k_cast<R><<<1024, 256, 0, st>>>(Tq, Nhat, 6 * Ts);
     rc = static_cast<int>(cudaGetLastError());
     cudaStreamSynchronize(st);

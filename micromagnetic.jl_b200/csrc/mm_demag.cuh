@@ -29,6 +29,11 @@ struct DemagGeom {
   // X[(c*Hx + kx)*ny + y], and the tensor quadrant as Nhat[(c*Hx + kx)*Tyq + ky],
   // so that a y line is contiguous in HBM (row-major: X[(c*ny + y)*Hx + kx])
   int xT;
+  // 3-D meshes whose y lines are too long for wide row tiles keep the spectra
+  // column-major too: X[((c*Hx + kx)*nz + z)*ny + y] (xT is set),
+  // Y[((c*Hx + kx)*nz + z)*Py + ky], Nhat[((c*Tzq + kz)*Hx + kx)*Tyq + ky];
+  // the z convolution then tiles along ky
+  int yT;
   const int* gate;  // device flag: kernels return at once when *gate == 0 (null: always run)
 };
 

@@ -140,7 +140,7 @@ __device__ __forceinline__ void lstage_any(int R, const SRC& src, const DST& dst
 }
 
 // All stages of pl: src -> (shared ping-pong a, b) -> dst.  Identity copy for L == 1.
-template <bool INV, bool POW2, int NT, class SRC, class DST, typename C>
+template <bool INV, bool POW2, int NT, bool PAD, class SRC, class DST, typename C>
 __device__ __forceinline__ void line_fft_impl(const SRC& src, const DST& dst, C* a, C* b, int LS, int nlines,
                                               const FastDiv fnl, const FftPlan1 pl, const C* __restrict__ tw,
                                               int tw_mul) {
@@ -154,7 +154,7 @@ __device__ __forceinline__ void line_fft_impl(const SRC& src, const DST& dst, C*
     lstage_any<INV, POW2, NT>(plan_radix(pl, 0), src, dst, L, nlines, fnl, 1, tw, tw_mul);
     return;
   }
-  SmemLines<C> A{a, LS}, B{b, LS};
+  SmemLines<C, PAD> A{a, LS}, B{b, LS};
   int p = 1;
   int R = plan_radix(pl, 0);
   lstage_any<INV, POW2, NT>(R, src, A, L, nlines, fnl, p, tw, tw_mul);
@@ -163,7 +163,7 @@ __device__ __forceinline__ void line_fft_impl(const SRC& src, const DST& dst, C*
     R = plan_radix(pl, s);
     lstage_any<INV, POW2, NT>(R, A, B, L, nlines, fnl, p, tw, tw_mul);
     p *= R;
-    const SmemLines<C> t = A;
+    const SmemLines<C, PAD> t = A;
     A = B;
     B = t;
   }
@@ -171,11 +171,11 @@ __device__ __forceinline__ void line_fft_impl(const SRC& src, const DST& dst, C*
   lstage_any<INV, POW2, NT>(R, A, dst, L, nlines, fnl, p, tw, tw_mul);
 }
 
-template <bool INV, int NT, class SRC, class DST, typename C>
+template <bool INV, int NT, bool PAD = false, class SRC, class DST, typename C>
 __device__ void line_fft(const SRC& src, const DST& dst, C* a, C* b, int LS, int nlines, const FastDiv fnl,
                          const FftPlan1 pl, const C* __restrict__ tw, int tw_mul) {
-  if (pl.pow2) line_fft_impl<INV, true, NT>(src, dst, a, b, LS, nlines, fnl, pl, tw, tw_mul);
-  else line_fft_impl<INV, false, NT>(src, dst, a, b, LS, nlines, fnl, pl, tw, tw_mul);
+  if (pl.pow2) line_fft_impl<INV, true, NT, PAD>(src, dst, a, b, LS, nlines, fnl, pl, tw, tw_mul);
+  else line_fft_impl<INV, false, NT, PAD>(src, dst, a, b, LS, nlines, fnl, pl, tw, tw_mul);
 }
 
 // All stages of pl from src into shared memory (a and b ping-pong); returns

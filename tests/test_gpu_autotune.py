@@ -38,7 +38,7 @@ def _field(cfg, form, tune):
 
 
 @pytest.mark.parametrize("form", [0, 1])
-@pytest.mark.parametrize("mesh", [(64, 48, 16, ""), (100, 80, 1, ""), (30, 20, 7, "xy")])
+@pytest.mark.parametrize("mesh", [(64, 48, 16, ""), (100, 80, 1, ""), (30, 20, 7, "xy"), (6, 210, 16, "")])
 def test_autotuned_tiles_give_identical_fields(mesh, form):
     cfg = random_config(31, *mesh, terms=("exch", "demag"))
     f_static, t_static = _field(cfg, form, False)

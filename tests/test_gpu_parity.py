@@ -130,6 +130,27 @@ def test_film_paths(mesh, form):
     assert rel_maxnorm(g.m(), o.get_m()) <= (1e-11 if form == 0 else TOL32)
 
 
+@pytest.mark.parametrize("form", [0, 1])
+@pytest.mark.parametrize("mesh", [(6, 210, 16), (6, 410, 16), (5, 130, 64)])
+def test_column_major_3d(mesh, form):
+    """3-D meshes whose y lines leave row tiles narrower than 8 columns keep
+    the spectra column-major and tile the z convolution along ky (FP64 from
+    padded y = 420, FP32 from y = 840; nz = 16 and 64 give power-of-two z):
+    field and two RK4 steps against the oracle."""
+    from oracle.oracle import demag_tensor
+
+    nx, ny, nz = mesh
+    cfg = random_config(31 + nx + ny + nz, nx, ny, nz, "", terms=("exch", "demag"), spatial=False)
+    T = demag_tensor(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, _ = build_oracle(cfg, tensor=T)
+    g = GpuSim(cfg, form=form, tensor=T)
+    tol = TOL64 if form == 0 else TOL32
+    assert rel_maxnorm(g.field(), o.effective_field()) <= tol
+    o.rk4(2e-14, 2)
+    g.rk4(2e-14, 2)
+    assert rel_maxnorm(g.m(), o.get_m()) <= (1e-11 if form == 0 else TOL32)
+
+
 def test_long_lines_rk4_and_dopri_fp64():
     """Stepping through the global-memory line stages, gated in the adaptive
     stepper's graph (y = 7500 film with exchange, anisotropy and Zeeman)."""

@@ -194,8 +194,8 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_inv_x(
     const C w = cconj(__ldg(twx + k));
     buf[l * LS + k] = cadd(cadd(a, b), crot<true>(cmul(csub(a, b), w)));
   };
-  if (g.xT) {
-    // column-major X: consecutive threads read consecutive rows of one kx
+  if (g.xT && !g.yT) {
+    // column-major X (films): consecutive threads read consecutive rows of one kx
 #pragma unroll 4  // several iterations' global loads in flight
     for (int e = threadIdx.x; e < nl * Lc; e += NT) {
       const int k = fdiv(e, fnl), l = e - k * nl;
@@ -502,12 +502,19 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_ylines(const cpl
     tensor_product<R, true, NT>(res, LS, lgW, Py, g.fPy, kx0, 0, Nhat, Hx, Py, g.Pz);
     line_fft_from_smem<true, NT>(res, res == a ? b : a, dst, LS, nlines, fnl, g.ply, twy, 1);
   } else if (XT) {
-    // 3-D column-major spectra (DemagGeom::yT): W contiguous columns of plane z
-    // of one component, X[((c*Hx + kx)*nz + z)*ny + y] <-> Y[((c*Hx + kx)*nz + z)*Py + ky]
-    const int lin = MODE == YL_INV ? Py : ny, lout = MODE == YL_FWD ? Py : ny;
-    const ColsIn<C, IX> cin{in + (static_cast<int64_t>(c0) * Hx * nz + z) * lin, nz * lin, lgW, kx0, Hx, lin};
-    const ColsOut<C, IX> cout{out + (static_cast<int64_t>(c0) * Hx * nz + z) * lout, nz * lout, lgW, kx0, Hx, lout};
-    line_fft<MODE == YL_INV, NT, true>(cin, cout, a, b, LS, nlines, fnl, g.ply, twy, 1);
+    // 3-D column-major spectra (DemagGeom::yT): the forward pass reads W
+    // contiguous columns of X[((c*Hx + kx)*nz + z)*ny + y] and writes Y
+    // columns Y[((c*Hx + kx)*nz + z)*Py + ky]; the inverse pass reads Y
+    // columns and writes X back row-major (the inverse x pass reads rows)
+    const int64_t yoff = (static_cast<int64_t>(c0) * Hx * nz + z) * Py;
+    if (MODE == YL_FWD) {
+      const ColsIn<C, IX> cin{in + (static_cast<int64_t>(c0) * Hx * nz + z) * ny, nz * ny, lgW, kx0, Hx, ny};
+      const ColsOut<C, IX> cout{out + yoff, nz * Py, lgW, kx0, Hx, Py};
+      line_fft<false, NT, true>(cin, cout, a, b, LS, nlines, fnl, g.ply, twy, 1);
+    } else {
+      const ColsIn<C, IX> cin{in + yoff, nz * Py, lgW, kx0, Hx, Py};
+      line_fft<true, NT, true>(cin, dst, a, b, LS, nlines, fnl, g.ply, twy, 1);
+    }
   } else {
     line_fft<MODE == YL_INV, NT>(src, dst, a, b, LS, nlines, fnl, g.ply, twy, 1);
   }
@@ -1603,7 +1610,7 @@ int DemagPlan<R>::set_tensor(const double* T6N, cudaStream_t st) {
         launch_zpass<double, ZM_TENSOR_Q, NT>(g64, Y64, nullptr, Tq + c * Ts, 1, g.Tyq, tz, sz, scale, st);
       }
     }
-    if (g.xT) k_cast_cols<R><<<1024, 256, 0, st>>>(Tq, Nhat, g.Tyq, g.Hx, g.Tzq);
+    if (g.xT || g.yT) k_cast_cols<R><<<1024, 256, 0, st>>>(Tq, Nhat, g.Tyq, g.Hx, g.Tzq);
     else k_cast<R><<<1024, 256, 0, st>>>(Tq, Nhat, 6 * Ts);
     rc = static_cast<int>(cudaGetLastError());
     cudaStreamSynchronize(st);

@@ -30,9 +30,11 @@ struct DemagGeom {
   // so that a y line is contiguous in HBM (row-major: X[(c*ny + y)*Hx + kx])
   int xT;
   // 3-D meshes whose y lines are too long for wide row tiles keep the spectra
-  // column-major too: X[((c*Hx + kx)*nz + z)*ny + y] (xT is set),
-  // Y[((c*Hx + kx)*nz + z)*Py + ky], Nhat[((c*Tzq + kz)*Hx + kx)*Tyq + ky];
-  // the z convolution then tiles along ky
+  // column-major too: Y[((c*Hx + kx)*nz + z)*Py + ky] and
+  // Nhat[((c*Tzq + kz)*Hx + kx)*Tyq + ky] (the z convolution then tiles along
+  // ky); X is column-major, X[((c*Hx + kx)*nz + z)*ny + y], from the forward
+  // x pass to the forward y pass (xT is set), and row-major again from the
+  // inverse y pass to the inverse x pass
   int yT;
   const int* gate;  // device flag: kernels return at once when *gate == 0 (null: always run)
 };

@@ -558,9 +558,14 @@ __global__ void __launch_bounds__(NT, 2) k_zconv(cplx_t<R>* Y, const R* __restri
 // W consecutive ky (grid: (Hx, ky tiles), tile q and its mirror Py/W-1-q
 // adjacent in launch order); the tile's rows are W contiguous entries of
 // Y[((c*Hx + kx)*nz + z)*Py + ky], the tensor Nhat[((c*Tzq + kz)*Hx + kx)*Tyq + ky].
+// Row-major: blocks blockIdx.x < nfull take W-wide kx tiles; the columns
+// kx >= nfull * W left over (Hx = 16 m + 1 for nx = 2^k) are tiled along ky
+// instead, block (nfull + r, q) taking column nfull * W + r and ky in
+// [q W, q W + W) (the blocks with q W >= Py return), so that no block
+// transforms a tile of mostly absent columns.
 template <typename R, int RA, int RB, int NT, bool I32, bool YT = false>
 __global__ void __launch_bounds__(NT, (zconv2_minb<R, NT>())) k_zconv2(cplx_t<R>* Y, const R* __restrict__ Nhat, DemagGeom g, int lgW,
-                                                  FastDiv fnl, const cplx_t<R>* __restrict__ twz) {
+                                                  FastDiv fnl, const cplx_t<R>* __restrict__ twz, int nfull) {
   using C = cplx_t<R>;
   using IX = std::conditional_t<I32, int, int64_t>;
   constexpr int L = RA * RB;
@@ -570,31 +575,38 @@ __global__ void __launch_bounds__(NT, (zconv2_minb<R, NT>())) k_zconv2(cplx_t<R>
   const int LS = L | 1, Hx = g.Hx, Py = g.Py, nz = g.nz;
   const int W = 1 << lgW;
   const int bq = blockIdx.y;
-  int kx0, ky0;  // first column of the tile: (kx0 + w, ky0) or, YT, (kx0, ky0 + w)
+  int kx0, ky0;  // first column of the tile: (kx0 + w, ky0) or, along ky, (kx0, ky0 + w)
+  bool along_ky = YT;
   if (YT) {
     const int nq = gridDim.y;
     kx0 = blockIdx.x;
     ky0 = ((bq & 1) ? nq - 1 - (bq >> 1) : (bq >> 1)) << lgW;
+  } else if (static_cast<int>(blockIdx.x) >= nfull) {
+    if ((bq << lgW) >= Py) return;
+    kx0 = nfull * W + (blockIdx.x - nfull);
+    ky0 = bq << lgW;
+    along_ky = true;
   } else {
     const int q = (bq + 1) >> 1;
     kx0 = blockIdx.x * W;
     ky0 = bq == 0 ? 0 : ((bq & 1) ? q : Py - q);
   }
   const int nlines = 3 * W;
-  // rows of the tile: element (c, z, w) at base + c*cs + z*rs + (t0 + w), t0 + w < tn
+  // rows of the tile: element (c, z, w) at base + c*cs + z*rs + (t0 + w)*ws, t0 + w < tn
   const IX cs = static_cast<IX>(static_cast<int64_t>(nz) * Py * Hx), rs = static_cast<IX>(YT ? Py : static_cast<int64_t>(Py) * Hx);
-  C* base = YT ? Y + static_cast<int64_t>(kx0) * nz * Py : Y + static_cast<int64_t>(ky0) * Hx;
-  const int t0 = YT ? ky0 : kx0, tn = YT ? Py : Hx;
-  RowsIn<C, IX> src{base, cs, rs, lgW, t0, tn, nz};
-  RowsOut<C, IX> dst{base, cs, rs, lgW, t0, tn, nz};
+  C* base = YT ? Y + static_cast<int64_t>(kx0) * nz * Py : (along_ky ? Y + kx0 : Y + static_cast<int64_t>(ky0) * Hx);
+  const int t0 = along_ky ? ky0 : kx0, tn = along_ky ? Py : Hx;
+  const IX ws = static_cast<IX>(along_ky && !YT ? Hx : 1);
+  RowsInW<C, IX> src{base, cs, rs, ws, lgW, t0, tn, nz};
+  RowsOutW<C, IX> dst{base, cs, rs, ws, lgW, t0, tn, nz};
   SmemLines<C> A{a, LS};
   lstage<RA, false, true, NT>(src, A, L, nlines, fnl, 1, twz, 1);
   // fused middle: thread -> (w, i), w fastest
   const int task = threadIdx.x;
   const bool act = task < W * RA;
   const int w = task & (W - 1), i = task >> lgW;
-  const int kx = YT ? kx0 : kx0 + w;
-  const int ky = YT ? ky0 + w : ky0;
+  const int kx = along_ky ? kx0 : kx0 + w;
+  const int ky = along_ky ? ky0 + w : ky0;
   C v[3][RB];
   if (act) {
 #pragma unroll
@@ -1307,16 +1319,20 @@ static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const
   if (g.yT) {
     dim3 grid(g.Hx, (g.Py + W - 1) / W, 1);
     if (offsets_fit_int(g))
-      k_zconv2<R, RA, RB, NTZ, true, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz);
+      k_zconv2<R, RA, RB, NTZ, true, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz, g.Hx);
     else
-      k_zconv2<R, RA, RB, NTZ, false, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz);
+      k_zconv2<R, RA, RB, NTZ, false, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz, g.Hx);
     return;
   }
-  dim3 grid((g.Hx + W - 1) / W, g.Py, 1);
+  // full kx tiles; up to W/4 leftover columns run as ky tiles in the same grid
+  const int rem = g.Hx % W;
+  const int nfull = rem > 0 && rem <= W / 4 && W <= g.Py ? g.Hx / W : (g.Hx + W - 1) / W;
+  const int ncols = nfull * W >= g.Hx ? 0 : g.Hx - nfull * W;
+  dim3 grid(nfull + ncols, g.Py, 1);
   if (offsets_fit_int(g))
-    k_zconv2<R, RA, RB, NTZ, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz);
+    k_zconv2<R, RA, RB, NTZ, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz, nfull);
   else
-    k_zconv2<R, RA, RB, NTZ, false><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz);
+    k_zconv2<R, RA, RB, NTZ, false><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz, nfull);
 }
 
 // Power-of-two z lengths with a fused-middle kernel: L = RA * RB

@@ -65,6 +65,36 @@ struct RowsOut {
   }
 };
 
+// rows of a spectrum array with a run-time step between the W entries of a
+// row: element (line, pos) at base[comp * comp_stride + pos * row_stride +
+// (t0 + w) * wstride], t0 + w < tn (the fused z kernel's tiles along kx, or
+// along ky of one kx column)
+template <typename C, typename IX = int64_t>
+struct RowsInW {
+  const C* base;
+  IX comp_stride, row_stride, wstride;
+  int lgW, t0, tn, nrows;  // pos >= nrows reads as zero
+  __device__ __forceinline__ C load(int line, int pos) const {
+    const int w = line & ((1 << lgW) - 1), comp = line >> lgW;
+    const int t = t0 + w;
+    if (pos >= nrows || t >= tn) return cmk<C>(0, 0);
+    return base[static_cast<IX>(comp) * comp_stride + static_cast<IX>(pos) * row_stride + static_cast<IX>(t) * wstride];
+  }
+};
+
+template <typename C, typename IX = int64_t>
+struct RowsOutW {
+  C* base;
+  IX comp_stride, row_stride, wstride;
+  int lgW, t0, tn, nrows;  // pos >= nrows is not written
+  __device__ __forceinline__ void store(int line, int pos, C v) const {
+    const int w = line & ((1 << lgW) - 1), comp = line >> lgW;
+    const int t = t0 + w;
+    if (pos >= nrows || t >= tn) return;
+    base[static_cast<IX>(comp) * comp_stride + static_cast<IX>(pos) * row_stride + static_cast<IX>(t) * wstride] = v;
+  }
+};
+
 // columns of a column-major spectrum (films): element (line, pos) at
 // base[(comp * Hx + kx) * ld + pos], kx = kx0 + w, comp = line >> lgW.
 template <typename C, typename IX = int64_t>

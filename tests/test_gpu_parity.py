@@ -151,6 +151,23 @@ def test_column_major_3d(mesh, form):
     assert rel_maxnorm(g.m(), o.get_m()) <= (1e-11 if form == 0 else TOL32)
 
 
+@pytest.mark.parametrize("form", [0, 1])
+@pytest.mark.parametrize("mesh", [(32, 12, 16), (64, 10, 16)])
+def test_zconv_leftover_columns(mesh, form):
+    """Power-of-two nx gives Hx = nx + 1 spectrum columns (33, 65): the fused z
+    convolution tiles all but the last along kx and the last along ky in the
+    same launch; field against the oracle."""
+    from oracle.oracle import demag_tensor
+
+    nx, ny, nz = mesh
+    cfg = random_config(37 + nx + ny, nx, ny, nz, "", terms=("demag",))
+    T = demag_tensor(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, idx = build_oracle(cfg, tensor=T)
+    fo, _ = o.term_field(idx["demag"])
+    fg, _ = GpuSim(cfg, form=form, tensor=T).term_field("demag")
+    assert rel_maxnorm(fg, fo) <= (TOL64 if form == 0 else TOL32)
+
+
 def test_long_lines_rk4_and_dopri_fp64():
     """Stepping through the global-memory line stages, gated in the adaptive
     stepper's graph (y = 7500 film with exchange, anisotropy and Zeeman)."""

@@ -471,10 +471,14 @@ enum YLMode { YL_FWD = 0, YL_INV = 1, YL_CONV2D = 2 };
 //   YL_INV:    Y rows 0..Py-1           -> X rows y < ny
 //   YL_CONV2D: X rows y < ny, forward y, tensor product (kz = 0), inverse y -> X
 // XT (YL_CONV2D of films): X column-major, see DemagGeom::xT.
+// Row-major: blocks blockIdx.x >= nfull take one leftover column each
+// (kx = nfull W + blockIdx.x - nfull; Hx = 16 m + 1 for nx = 2^k) instead of
+// a W-wide tile of mostly absent columns; fnl1 divides by ncompc.
 template <typename R, int MODE, int NT, bool I32, bool XT = false>
 __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_ylines(const cplx_t<R>* in, cplx_t<R>* out, const R* __restrict__ Nhat,
                                                   DemagGeom g, int lgW, int ncompc, FastDiv fnl,
-                                                  const cplx_t<R>* __restrict__ twy, int half) {
+                                                  const cplx_t<R>* __restrict__ twy, int half, int nfull,
+                                                  FastDiv fnl1) {
   using C = cplx_t<R>;
   using IX = std::conditional_t<I32, int, int64_t>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -483,8 +487,14 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_ylines(const cpl
   if (g.gate && !*g.gate) return;
   const int Py = g.Py, LS = XT ? padded_line_stride(Py) : Py | 1, Hx = g.Hx, ny = g.ny, nz = g.nz;
   const int W = 1 << lgW;
-  const int kx0 = blockIdx.x * W, z = blockIdx.y, c0 = blockIdx.z * ncompc;
-  const int nlines = ncompc * W;
+  const bool left = !XT && static_cast<int>(blockIdx.x) >= nfull;
+  if (left) {
+    lgW = 0;
+    fnl = fnl1;
+  }
+  const int kx0 = left ? nfull * W + (static_cast<int>(blockIdx.x) - nfull) : blockIdx.x * W;
+  const int z = blockIdx.y, c0 = blockIdx.z * ncompc;
+  const int nlines = ncompc << lgW;
   const int rin = MODE == YL_INV ? Py : ny, rout = MODE == YL_FWD ? Py : ny;
   RowsIn<C, IX> src{in + static_cast<int64_t>(c0 * nz + z) * rin * Hx, static_cast<IX>(static_cast<int64_t>(nz) * rin * Hx),
                     static_cast<IX>(Hx), lgW, kx0, Hx, rin};
@@ -1278,20 +1288,24 @@ static void launch_ylines(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* ou
   const bool xt = MODE == YL_CONV2D ? g.xT != 0 : g.yT != 0;
   const int W = Wforce > 0 ? Wforce : lines_tile<R>(g.Hx, g.Py, ncompc, nbuf);
   const int half = ncompc * W * (xt ? padded_line_stride(g.Py) : g.Py | 1);
-  dim3 grid((g.Hx + W - 1) / W, g.nz, 3 / ncompc);
+  // full tiles; up to W/4 leftover columns (row-major) run as one-column blocks
+  const int rem = g.Hx % W;
+  const int nfull = !xt && rem > 0 && rem <= W / 4 ? g.Hx / W : (g.Hx + W - 1) / W;
+  const int ncols = nfull * W >= g.Hx ? 0 : g.Hx - nfull * W;
+  dim3 grid(nfull + ncols, g.nz, 3 / ncompc);
   const size_t sm = static_cast<size_t>(std::max(1, nbuf)) * sizeof(C) * half;
-  const FastDiv fnl = make_fastdiv(ncompc * W);
+  const FastDiv fnl = make_fastdiv(ncompc * W), fnl1 = make_fastdiv(ncompc);
   if (xt) {
     if (offsets_fit_int(g))
-      k_ylines<R, MODE, kHotNT, true, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
+      k_ylines<R, MODE, kHotNT, true, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1);
     else
-      k_ylines<R, MODE, kHotNT, false, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
+      k_ylines<R, MODE, kHotNT, false, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1);
     return;
   }
   if (offsets_fit_int(g))
-    k_ylines<R, MODE, kHotNT, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
+    k_ylines<R, MODE, kHotNT, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1);
   else
-    k_ylines<R, MODE, kHotNT, false><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half);
+    k_ylines<R, MODE, kHotNT, false><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1);
 }
 
 template <typename R, int RA, int RB>

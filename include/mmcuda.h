@@ -298,9 +298,12 @@ int mm_batch_destroy(mm_batch* b);
  * enqueued on `stream` (cudaStream_t, 0 = legacy default stream).
  * Allocates nothing: the per-block partial sums live in a static device array
  * of the library (3 MiB on every GPU that loads it), so meshes are limited to
- * 2^24 cells (MM_ERR_ARG beyond).  The first call on a device looks the
- * array's device address up (cudaGetSymbolAddress) and should come before any
- * stream capture.  Calls share the array: calls that overlap on the GPU race. */
+ * 2^24 cells (MM_ERR_ARG beyond).  Every call looks the array's device
+ * address up in the current context (cudaGetSymbolAddress, a host-side lookup
+ * that allocates nothing), so a reset or re-created primary context is
+ * followed; the first call on a device (which loads the library's device code
+ * and the array) should come before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU race. */
 int mm_energy_noalloc(const mm_mesh_desc* mesh, const double* m_soa_dev, const double* Ms_dev, double A, double D,
                       double Ku, double ax, double ay, double az, double Hx, double Hy, double Hz,
                       double* energies_dev, void* stream);

@@ -828,13 +828,19 @@ static void set_smem_attrs_nt() {
 
 template <typename R>
 static void set_smem_attrs() {
-  static uint64_t done_mask = 0;  // one bit per device
+  // one bit per device, set only once the attributes are in place; the lock
+  // keeps a second thread from launching before that (devices >= 64 set the
+  // attributes on every call)
+  static std::mutex mu;
+  static uint64_t done_mask = 0;
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 64 && ((done_mask >> dev) & 1ull)) return;
-  if (dev < 64) done_mask |= 1ull << dev;
+  const bool tracked = dev >= 0 && dev < 64;
+  std::lock_guard<std::mutex> lk(mu);
+  if (tracked && ((done_mask >> dev) & 1ull)) return;
   set_smem_attrs_nt<R, kHotNT>();
   if (sizeof(R) == 8) set_smem_attrs_nt<double, kTensorNT>();
+  if (tracked) done_mask |= 1ull << dev;
 }
 
 template <typename R>
@@ -1318,16 +1324,21 @@ static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const
   int W = Wforce > 0 ? Wforce : lines_tile<R>(g.yT ? g.Py : g.Hx, L, 3, 1);
   while (W * RA > NTZ) W /= 2;
   const size_t sm = sizeof(C) * 3 * W * (L | 1);
-  static uint64_t done = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!((done >> dev) & 1ull)) {
-    const int mx = static_cast<int>(kMaxSmem);
-    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    done |= 1ull << dev;
+  {
+    static std::mutex mu;
+    static uint64_t done = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const bool tracked = dev >= 0 && dev < 64;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!tracked || !((done >> dev) & 1ull)) {
+      const int mx = static_cast<int>(kMaxSmem);
+      cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+      cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+      cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+      cudaFuncSetAttribute(k_zconv2<R, RA, RB, NTZ, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+      if (tracked) done |= 1ull << dev;
+    }
   }
   const FastDiv fnl = make_fastdiv(3 * W);
   if (g.yT) {

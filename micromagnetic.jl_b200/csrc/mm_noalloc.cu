@@ -21,7 +21,6 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
-#include <mutex>
 #include <string>
 
 #include "../../include/mmcuda.h"
@@ -124,24 +123,17 @@ __global__ void k_energy_noalloc_final(const double* __restrict__ partials, int 
   }
 }
 
-// Device address of the static scratch, looked up once per device with that
-// device current (the host-side symbol is not a device address).
-std::mutex g_mu;
-double* g_addr[64] = {};
-
+// Device address of the static scratch in the current context.  It is looked
+// up on every call (cudaGetSymbolAddress is a host-side lookup and allocates
+// nothing): a cached address would go stale when the host resets or re-creates
+// the primary context (cudaDeviceReset, CUDA.jl's device_reset!), which reloads
+// the module and its array at another address.  The host-side name of the
+// array is not a device address and is never passed to a kernel.
 int scratch_for_current_device(double** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
   if (e != cudaSuccess) return mm::set_last_error(MM_ERR_CUDA, cudaGetErrorString(e));
-  if (dev < 0 || dev >= 64) return mm::set_last_error(MM_ERR_UNSUPPORTED, "mm_energy_noalloc: device index >= 64");
-  std::lock_guard<std::mutex> g(g_mu);
-  if (!g_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-    if (e != cudaSuccess) return mm::set_last_error(MM_ERR_CUDA, cudaGetErrorString(e));
-    g_addr[dev] = static_cast<double*>(p);
-  }
-  *out = g_addr[dev];
+  *out = static_cast<double*>(p);
   return MM_OK;
 }
 

@@ -118,6 +118,10 @@ int read_header(FILE* f, Header& h) {
   if (h.type < 0) return err(MM_ERR_ARG, "OVF2 file has no data segment");
   if (h.nx < 1 || h.ny < 1 || h.nz < 1) return err(MM_ERR_ARG, "OVF2 header has no valid xnodes/ynodes/znodes");
   if (h.nx > INT32_MAX || h.ny > INT32_MAX || h.nz > INT32_MAX) return err(MM_ERR_ARG, "OVF2 mesh too large");
+  // 3 * xnodes * ynodes * znodes must fit int64: checked by division before
+  // any product is formed (the header is untrusted input)
+  constexpr int64_t kMaxCells = INT64_MAX / 3;
+  if (h.nx > kMaxCells / h.ny || h.nx * h.ny > kMaxCells / h.nz) return err(MM_ERR_ARG, "OVF2 mesh too large");
   if (h.valuedim != 3) return err(MM_ERR_UNSUPPORTED, "OVF2 valuedim other than 3");
   return MM_OK;
 }

@@ -1,9 +1,9 @@
 """Regenerate the golden fixtures in this folder from the reference's own tests.
 
-Run from the repository root, in a container where the MicroMagnetic.jl
-sources are mounted (default ``/root/reference``):
+Run from the repository root with the MicroMagnetic.jl checkout as the
+argument:
 
-    python tests/golden/make_golden.py [reference_root]
+    python tests/golden/make_golden.py <reference_root>
 
 Sources (read as text; nothing of the reference is executed):
   * test/test_fields.txt + test/test_fields.jl:9-59 -> fields_20x5x3.npz
@@ -55,4 +55,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <MicroMagnetic.jl root>")
+    main(sys.argv[1])

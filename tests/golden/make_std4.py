@@ -8,7 +8,8 @@ Ms=8e5, A=1.3e-11, demag; SD relax from (1, 0.25, 0.1) to stopping_dmdt 0.01;
 then LLG (alpha 0.02, gamma 2.211e5, Dormand-Prince tol 1e-6) in the field
 (-24.6, 4.3, 0) mT, <m> at t = i * 10 ps, i = 0..100.
 
-Run from the repository root:  python tests/golden/make_std4.py
+Run from the repository root with the reference checkout as the argument:
+    python tests/golden/make_std4.py <MicroMagnetic.jl root>
 """
 import math
 import os
@@ -19,13 +20,13 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
-REF = "/root/reference/docs/src/micromagnetics/assets/std4_oommf.txt"
+OOMMF_ASSET = "docs/src/micromagnetics/assets/std4_oommf.txt"  # path inside the reference checkout
 MU0 = 4 * math.pi * 1e-7
 mT = 1e-3 / MU0
 
 
-def oommf():
-    d = np.loadtxt(REF)
+def oommf(ref_root):
+    d = np.loadtxt(os.path.join(ref_root, OOMMF_ASSET))
     keep = np.abs(np.round(d[:, 0] / 1e-11) * 1e-11 - d[:, 0]) < 1e-16
     d = d[keep]
     np.savez(os.path.join(HERE, "std4_oommf.npz"), t=d[:, 0], m=d[:, 1:4])
@@ -65,5 +66,7 @@ def oracle():
 
 
 if __name__ == "__main__":
-    oommf()
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_std4.py <MicroMagnetic.jl root>")
+    oommf(sys.argv[1])
     oracle()

@@ -103,3 +103,23 @@ def test_errors(tmp_path):
     assert L.mm_ovf_read(str(trunc).encode(), _lib.dptr(out), 2) == _lib.MM_ERR_ARG
     with pytest.raises(ValueError):
         save_ovf(OVF2(2, 1, 1, 1e-9, 1e-9, 1e-9, "Float16", "x", M), str(tmp_path / "t"))
+
+
+def test_oversized_header_refused(tmp_path):
+    """Node counts whose product (times 3 values a cell) overflows int64 are
+    refused while parsing the header, before any product is formed."""
+    L = _lib.load()
+    ok = str(tmp_path / "ok")
+    save_ovf(OVF2(2, 1, 1, 1e-9, 1e-9, 1e-9, "String", "x", M), ok)
+    text = open(ok + ".ovf").read()
+    for nodes in (("2000000000", "2000000000", "2000000000"), ("2147483647", "2147483647", "2")):
+        bad = text.replace("# xnodes: 2\n", "# xnodes: %s\n" % nodes[0])
+        bad = bad.replace("# ynodes: 1\n", "# ynodes: %s\n" % nodes[1]).replace("# znodes: 1\n", "# znodes: %s\n" % nodes[2])
+        assert bad != text
+        f = tmp_path / "huge.ovf"
+        f.write_text(bad)
+        d = _lib.MeshDesc()
+        assert L.mm_ovf_read_header(str(f).encode(), d, None, None, 0) == _lib.MM_ERR_ARG
+        assert "too large" in _lib.last_error()
+        out = np.empty(6)
+        assert L.mm_ovf_read(str(f).encode(), _lib.dptr(out), 2) == _lib.MM_ERR_ARG

@@ -2,22 +2,29 @@
 """Throughput benchmark of the finite-difference LLG hot path (H_eff + demag +
 RK4) on B200 through libmmcuda's C ABI.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c5|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c5|c2|c1|...]
                     [--impl native|reference]
 
 One JSON line on rank 0.  Metric: LLG cell-steps/s = cells x RK4 steps / s,
 whole job (N replicas of the mesh under torchrun: the path has no exchange
-step between meshes, so ranks run independent replicas, scaling "weak").
+step between meshes, so ranks run independent replicas, scaling "weak"), for
+the FP32 form (`value`) and the FP64 form (`fp64`), with the FP32 form's
+relative max-norm error of m against the FP64 form after the same steps.
 `e2e`: the same metric through the C ABI with pinned host arrays, copying m
 in and out every step; the FP32 form's host arrays are Float32 (sim.spin in
 the reference's Float32 mode), `e2e_f64_host` repeats it with Float64 arrays.
+`--impl reference` times the CPU oracle (FP64 restatement of the reference
+path, all host threads) on the whole mesh of the workload for one RK4 step.
 
 Workloads (seeded synthetic inputs, numpy PCG64):
+  c5  1024x1024x16 cells, 3 nm: exchange A=1.3e-11, Ms=8e5, demag (padded
+      2048x2048x32); random unit m (seed 105); alpha=0.1, gamma=2.211e5; RK4
+      with dt = 5e-14 s.  The default: the configuration the metric is quoted
+      on.  Its line also carries c2 with RK4 and with Dormand-Prince
+      (`extra_workloads`).
   c2  256x256x64 cells, 2 nm: exchange A=1e-11, bulk DMI 3e-3, Ku=5e5 along z,
       Ms=5.8e5, demag; random unit m (seed 102); alpha=0.1, gamma=2.211e5;
-      RK4 with dt = 5e-14 s (the default).
-  c5  1024x1024x16 cells, 3 nm: exchange A=1.3e-11, Ms=8e5, demag (padded
-      2048x2048x32); random unit m (seed 105); alpha=0.1, gamma=2.211e5.
+      RK4 with dt = 5e-14 s (--integrator dopri: Dormand-Prince, tol 1e-6).
   c1  200x50x1, 2.5x2.5x3 nm: A=1.3e-11, Ms=8e5, demag, in-plane Zeeman
       |B| <= 30 mT (seed 101); alpha=0.02, gamma=2.211e5, dt=1e-13.
 """
@@ -121,7 +128,8 @@ def setup_native(w, form, device):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+    """nvidia-smi clock / throttle-reason samples while the timed region runs
+    (one streaming nvidia-smi process sampling every 50 ms)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -130,29 +138,36 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.samples = []
-        self._stop = threading.Event()
+        self._p = None
         self._t = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._p.stdout:
+            row = [x.strip() for x in line.split(",")]
+            if len(row) >= 9:
+                self.samples.append(row)
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                        "--format=csv,noheader,nounits", "-lms", "50"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+            time.sleep(0.2)  # the first sample precedes the timed region's work
+        except Exception:
+            self._p = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._p is not None:
+            time.sleep(0.1)
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except Exception:
+                self._p.kill()
+            self._t.join(timeout=5)
 
     def summary(self):
         if not self.samples:
@@ -329,16 +344,20 @@ def run_adjoint(args, rank, ws, device, dist):
         dist.destroy_process_group()
 
 
-def cpu_baseline(wname, steps=1):
-    """FP64 oracle (CPU restatement of the reference path), all host threads,
-    on a bounded block of the workload's physics."""
+def cpu_baseline(wname, steps=1, full=False):
+    """FP64 oracle (CPU restatement of the reference path), all host threads.
+    full=False: a bounded block of the workload's physics, one warm-up step
+    and `steps` timed steps.  full=True: the whole mesh of the workload, one
+    warm-up field evaluation (page-in of every buffer) and `steps` timed
+    steps."""
     from oracle.oracle import OracleSim, max_threads
 
     w = WORKLOADS[wname]
-    shape = CPU_SAMPLE[wname]
+    shape = (w["nx"], w["ny"], w["nz"]) if full else CPU_SAMPLE[wname]
     nx, ny, nz = shape
     m, H = synth_inputs(w, shape)
     n = nx * ny * nz
+    t_setup = time.perf_counter()
     s = OracleSim(nx, ny, nz, w["dx"], w["dy"], w["dz"])
     s.set_Ms(w["Ms"])
     s.set_m(m)
@@ -352,17 +371,23 @@ def cpu_baseline(wname, steps=1):
         s.add_zeeman(np.asarray(H))
     if w["demag"]:
         s.add_demag()
+    t_setup = time.perf_counter() - t_setup
     heun = w.get("integrator") == "heun"
     step = s.heun if heun else s.rk4
-    step(w["dt"], 1)  # warm-up (plans, pages)
+    if full:
+        s.effective_field()  # warm-up: plans and pages
+    else:
+        step(w["dt"], 1)  # warm-up (plans, pages)
     t0 = time.perf_counter()
     step(w["dt"], steps)
     dt = time.perf_counter() - t0
     evals = 2 if heun else 1
+    what = f"the full {nx}x{ny}x{nz} {wname} mesh" if full else f"{nx}x{ny}x{nz} block of the {wname} physics"
+    warm = "1 warm-up field evaluation" if full else "1 warm-up step"
     return {"value": evals * n * steps / dt, "unit": "cell-evals/s" if heun else "cell-steps/s",
-            "cores": max_threads(), "kind": "port",
-            "sample": f"{nx}x{ny}x{nz} block of the {wname} physics, FP64, {steps} "
-                      f"{'Heun' if heun else 'RK4'} step(s) after 1 warm-up, {dt:.1f} s"}
+            "cores": max_threads(), "kind": "port", "ms_per_step": 1e3 * dt / steps,
+            "sample": f"{what}, FP64, {steps} {'Heun' if heun else 'RK4'} step(s) after {warm}, "
+                      f"{dt:.1f} s timed ({t_setup:.1f} s set-up untimed)"}
 
 
 def dist_init():
@@ -410,26 +435,21 @@ def run_reference(args):
                                                                "workloads only (c1, c2, c5, fig9)"}), flush=True)
         return
     w = WORKLOADS[wname]
-    vals = []
-    for _ in range(max(1, args.warmup // 3)):
-        cpu_baseline(wname, 1)
-    base = None
-    for _ in range(max(1, min(args.steps, 3))):
-        base = cpu_baseline(wname, 1)
-        vals.append(base["value"])
-    v = statistics.median(vals)
+    # the whole mesh of the workload, one timed step (bounded: a full-size
+    # FP64 step of c5 takes about a minute on 16 host cores)
+    base = cpu_baseline(wname, 1, full=True)
+    v = base["value"]
     n = w["nx"] * w["ny"] * w["nz"]
     heun = w.get("integrator") == "heun"
-    evals = 2 if heun else 1
     line = {"metric": ("LLG cell-evals/s (H_eff+demag+Heun, 2 evals per step)" if heun
-                       else "LLG cell-steps/s (H_eff+demag+RK4)"),
+                       else "LLG cell-steps/s (H_eff+demag+RK4), FP32 vs FP64 form at \u22641e-5 err"),
             "value": v, "unit": base["unit"], "n_gpus": args.gpus,
-            "steps": len(vals), "warmup": args.warmup, "ms_per_step": 1e3 * evals * n / v, "higher_is_better": True,
+            "steps": 1, "warmup": 1, "ms_per_step": base["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy PCG64)",
             "config": {"workload": f"{wname}: {w['nx']}x{w['ny']}x{w['nz']} {'Heun' if heun else 'RK4'}",
                        "form": "fp64", "sample": base["sample"]},
             "impl": "reference",
-            "cpu_baseline": {**base, "value": v},
+            "cpu_baseline": dict(base),
             "e2e": {"value": v, "unit": base["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     if dist is not None:
@@ -496,6 +516,8 @@ def run_native(args):
             res["tiles"] = list(tiles)
         if sampler:
             res["clocks"] = sampler.summary()
+        if not heun and "fp32" in (args.only or "fp32 fp64") and "fp64" in (args.only or "fp32 fp64"):
+            res["m_after"] = h.get_m()  # both forms advanced warm-up + steps from the same m0
         if args.quick:
             results[fname] = res
             h.close()
@@ -514,7 +536,7 @@ def run_native(args):
             # form's host arrays are Float32 (sim.spin in the reference's
             # Float32 mode: mm_set_m_f32 / mm_get_m_f32); the Float64-array
             # boundary is reported beside it
-            k2 = max(3, args.steps // 10)
+            k2 = args.steps
 
             def e2e(f32):
                 dt_np, ct = (np.float32, ctypes.c_float) if f32 else (np.float64, ctypes.c_double)
@@ -556,6 +578,11 @@ def run_native(args):
         if dist is not None:
             dist.destroy_process_group()
         return
+    fp32_err = None
+    if "m_after" in results.get("fp32", {}) and "m_after" in results.get("fp64", {}):
+        a, b = results["fp32"].pop("m_after"), results["fp64"].pop("m_after")
+        fp32_err = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    extra = extra_workloads(device) if (wname == "c5" and ws == 1 and not args.no_extra) else None
     if rank == 0:
         r = results["fp32"]
         peak, peak_kind = measured_peak()
@@ -575,7 +602,7 @@ def run_native(args):
                 r[k]["unit"] = unit
         line = {
             "metric": ("LLG cell-evals/s (H_eff+demag+Heun, 2 evals per step)" if heun
-                       else "LLG cell-steps/s (H_eff+demag+RK4)"),
+                       else "LLG cell-steps/s (H_eff+demag+RK4), FP32 vs FP64 form at \u22641e-5 err"),
             "value": evals * r["value"], "unit": unit, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": (evals * r["value"] / w["published"]) if w.get("published") else None,
@@ -591,7 +618,9 @@ def run_native(args):
             "e2e_f64_host": r["e2e_f64_host"],
             "gpu_launches": r["launches_per_step"] * args.steps,
             "fp64": ({"value": evals * results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
-                      "fp32_over_fp64": r["value"] / results["fp64"]["value"]} if "fp64" in results else None),
+                      "fp32_over_fp64": r["value"] / results["fp64"]["value"],
+                      "fp32_rel_err_vs_fp64": fp32_err, "err_after_steps": args.warmup + args.steps}
+                     if "fp64" in results else None),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "peak_kind": peak_kind,
                          "traffic": traffic},
@@ -600,6 +629,8 @@ def run_native(args):
             "kernels": {k: {"ms": round(v["ms"], 5), "GBps": round(v["GBps"] or 0, 1)} for k, v in r["kernels"].items()},
             "clocks": r.get("clocks"),
         }
+        if extra:
+            line["extra_workloads"] = extra
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(wname, 1)
         print(json.dumps(line), flush=True)
@@ -607,23 +638,61 @@ def run_native(args):
         dist.destroy_process_group()
 
 
-def run_dopri(args, w, wname, n, forms, rank, ws, device, dist):
-    """Dormand-Prince (tol 1e-6) through mm_run_until: cell-steps/s over
-    accepted steps, the step control running on the device."""
+def time_steps(w, form, device, steps, warmup, step_fn="mm_rk4_run"):
+    """CUDA-event time of `steps` fixed steps of one handle after `warmup`."""
+    import torch
+
+    h, _ = setup_native(w, form, device)
+    stream = torch.cuda.ExternalStream(h.stream(), device=device)
+    h.call(step_fn, w["dt"], warmup)
+    h.call("mm_synchronize")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    h.call(step_fn, w["dt"], steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    h.close()
+    n = w["nx"] * w["ny"] * w["nz"]
+    return {"value": n * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps}
+
+
+def extra_workloads(device):
+    """c2 (256x256x64, bulk DMI + anisotropy + demag) with RK4 and with
+    Dormand-Prince (tol 1e-6, its own integrator), both forms, beside the c5
+    headline."""
+    from mmcuda import _lib
+
+    w = WORKLOADS["c2"]
+    out = {"c2_rk4": {}, "c2_dopri": {}}
+    for fname, form in (("fp32", _lib.MM_FP32), ("fp64", _lib.MM_FP64)):
+        out["c2_rk4"][fname] = time_steps(w, form, device, 50, 5)
+        out["c2_dopri"][fname] = dopri_forms(w, {fname: form}, 10, 3, 1, device, None)[fname]
+    for k in out:
+        out[k]["fp32_over_fp64"] = out[k]["fp32"]["value"] / out[k]["fp64"]["value"]
+    out["c2_rk4"]["workload"] = "c2: 256x256x64 exch + bulk DMI + anis + demag, RK4 dt=5e-14"
+    out["c2_dopri"]["workload"] = "c2: 256x256x64 exch + bulk DMI + anis + demag, Dormand-Prince tol 1e-6"
+    return out
+
+
+def dopri_forms(w, forms, steps, warmup, ws, device, dist):
+    """Accepted cell-steps/s of Dormand-Prince (tol 1e-6) through mm_run_until
+    for each form, the step control running on the device."""
     import torch
     from mmcuda import _lib
 
+    n = w["nx"] * w["ny"] * w["nz"]
     out = {}
-    for fname in ((args.only,) if args.only else ("fp32", "fp64")):
-        h, _ = setup_native(w, forms[fname], device)
+    for fname, form in forms.items():
+        h, _ = setup_native(w, form, device)
         h.call("mm_dopri_set_tol", 1e-6)
         st = _lib.Stats()
         L = _lib.load()
         _lib.check(L.mm_run_until(h.h, 1e-15, ctypes.byref(st)))  # initial step + first attempts
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             _lib.check(L.mm_advance_step(h.h, ctypes.byref(st)))
         t0, n0, a0, r0 = st.t, st.nsteps, st.attempts, st.rejected
-        span = args.steps * st.step_next
+        span = steps * st.step_next
         stream = torch.cuda.ExternalStream(h.stream(), device=device)
         if dist is not None:
             dist.barrier()
@@ -637,10 +706,18 @@ def run_dopri(args, w, wname, n, forms, rank, ws, device, dist):
         if dist is not None:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-        steps = st.nsteps - n0
-        out[fname] = {"value": ws * n * steps / (ms / 1e3), "ms_per_step": ms / max(1, steps), "accepted": steps,
+        acc = st.nsteps - n0
+        out[fname] = {"value": ws * n * acc / (ms / 1e3), "ms_per_step": ms / max(1, acc), "accepted": acc,
                       "attempts": st.attempts - a0, "rejected": st.rejected - r0, "t_span": span}
         h.close()
+    return out
+
+
+def run_dopri(args, w, wname, n, forms, rank, ws, device, dist):
+    """Dormand-Prince (tol 1e-6) through mm_run_until: cell-steps/s over
+    accepted steps, the step control running on the device."""
+    sel = {k: v for k, v in forms.items() if not args.only or k == args.only}
+    out = dopri_forms(w, sel, args.steps, args.warmup, ws, device, dist)
     if rank == 0:
         r = out.get("fp32") or out.get("fp64")
         line = {"metric": "LLG cell-steps/s (H_eff+demag+Dormand-Prince)", "value": r["value"], "unit": "cell-steps/s",
@@ -659,9 +736,10 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(ADJOINT))
+    ap.add_argument("--workload", default="c5", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(ADJOINT))
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="c5: skip the c2 RK4 / Dormand-Prince extra keys")
     ap.add_argument("--only", choices=["fp32", "fp64"], help="time one form only (profiling runs)")
     ap.add_argument("--quick", action="store_true", help="timed steps only: no e2e, kernel timing or CPU leg")
     ap.add_argument("--integrator", default=None, choices=["rk4", "heun", "dopri"],

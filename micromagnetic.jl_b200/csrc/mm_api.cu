@@ -459,8 +459,9 @@ class Engine : public EngineBase {
     MM_CUDA(cudaMalloc(&T, sizeof(double) * 6 * N));
     if (T6N_host) {
       cudaMemcpyAsync(T, T6N_host, sizeof(double) * 6 * N, cudaMemcpyHostToDevice, st_);
-    } else {
-      newell_tensor_device(nx, ny, nz, dx, dy, dz, Nx, Ny, Nz, T, st_);
+    } else if ((rc = newell_tensor_device(nx, ny, nz, dx, dy, dz, Nx, Ny, Nz, T, st_))) {
+      cudaFree(T);
+      return fail(MM_ERR_CUDA, "Newell tensor assembly failed: %s", cudaGetErrorString(static_cast<cudaError_t>(rc)));
     }
     rc = plan->set_tensor(T, st_);
     cudaStreamSynchronize(st_);

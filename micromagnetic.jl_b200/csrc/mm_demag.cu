@@ -10,6 +10,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "mm_dd.cuh"
 #include "mm_demag.cuh"
 #include "mm_fft.cuh"
 #include "mm_lines.cuh"
@@ -686,68 +687,123 @@ __global__ void k_cast(const double* __restrict__ a, RO* __restrict__ b, int64_t
     b[i] = static_cast<RO>(a[i]);
 }
 
-// ------------------------------------------------------ Newell (FP64) -----
-// newell_f / newell_g: src/micro/demag.jl:133-192; dipole far field
-// src/atomistic/demag.jl:106-120; switch at R > 60 cells, demag.jl:196-201.
-__device__ double dev_newell_f(double x, double y, double z) {
-  const double x2 = x * x, y2 = y * y, z2 = z * z;
-  const double R = sqrt(x2 + y2 + z2);
-  if (R == 0.0) return 0.0;
-  double f = 1.0 / 6 * (2 * x2 - y2 - z2) * R;
-  if (x2 > 0) f -= x * y * z * atan(y * z / (x * R));
-  if (x2 + z2 > 0) f += 0.5 * y * (z2 - x2) * asinh(y / sqrt(x2 + z2));
-  if (x2 + y2 > 0) f += 0.5 * z * (y2 - x2) * asinh(z / sqrt(x2 + y2));
+// ------------------------------------------------------ Newell tensor -----
+// newell_f / newell_g: src/micro/demag.jl:133-192 (Newell, Williams & Dunlop,
+// J. Geophys. Res. 98 (1993) 9551); 27-point second differences
+// demag_tensor_xx / _xy demag.jl:194-296; dipole far field
+// src/atomistic/demag.jl:106-138 beyond R > 60 cells (demag.jl:196-201,
+// 247-252); macro-PBC image sums demag.jl:298-386.
+//
+// The second differences cancel up to R^6 (5e10 at R = 60) of the function
+// values, so an FP64 evaluation carries relative errors up to ~1e-6 in the
+// tensor entries near the dipole switch (its rounding, and 1-ulp differences
+// between libm implementations, show in H_demag at ~1e-9).  Here f and g are
+// evaluated in double-double arithmetic at the exact coordinates
+// (X + a) * dx (X an integer offset, dx the normalised cell size), the
+// differences, image sums and dipole terms are summed in double-double, and
+// each entry is rounded to FP64 once: the tensor of the given normalised
+// cell is then correct to the last bit or so.  The near field is evaluated
+// once per grid point (every point serves up to 27 entries) and stored; f is
+// even in each argument, g odd in its first two and even in the third.
+using dd::DD;
+
+__device__ DD ddf(DD x, DD y, DD z) {
+  const DD x2 = dd::mul(x, x), y2 = dd::mul(y, y), z2 = dd::mul(z, z);
+  const DD R = dd::sqrt(dd::add(dd::add(x2, y2), z2));
+  if (dd::is_zero(R)) return dd::mk(0.0);
+  DD f = dd::div(dd::mul(dd::sub(dd::sub(dd::scale2(x2, 2.0), y2), z2), R), 6.0);
+  if (dd::positive(x2))
+    f = dd::sub(f, dd::mul(dd::mul(dd::mul(x, y), z), dd::atan(dd::div(dd::mul(y, z), dd::mul(x, R)))));
+  const DD xz = dd::add(x2, z2), xy = dd::add(x2, y2);
+  if (dd::positive(xz))
+    f = dd::add(f, dd::mul(dd::scale2(dd::mul(y, dd::sub(z2, x2)), 0.5), dd::asinh(dd::div(y, dd::sqrt(xz)))));
+  if (dd::positive(xy))
+    f = dd::add(f, dd::mul(dd::scale2(dd::mul(z, dd::sub(y2, x2)), 0.5), dd::asinh(dd::div(z, dd::sqrt(xy)))));
   return f;
 }
 
-__device__ double dev_newell_g(double x, double y, double z) {
-  const double x2 = x * x, y2 = y * y, z2 = z * z;
-  const double R = sqrt(x2 + y2 + z2);
-  if (R == 0.0) return 0.0;
-  double g = -1.0 / 3 * x * y * R;
-  if (z2 > 0) g -= 1.0 / 6 * z2 * z * atan(x * y / (z * R));
-  if (y2 > 0) g -= 0.5 * y2 * z * atan(x * z / (y * R));
-  if (x2 > 0) g -= 0.5 * x2 * z * atan(y * z / (x * R));
-  if (x2 + y2 > 0) g += x * y * z * asinh(z / sqrt(x2 + y2));
-  if (y2 + z2 > 0) g += 1.0 / 6 * y * (3 * z2 - y2) * asinh(x / sqrt(y2 + z2));
-  if (x2 + z2 > 0) g += 1.0 / 6 * x * (3 * z2 - x2) * asinh(y / sqrt(x2 + z2));
+__device__ DD ddg(DD x, DD y, DD z) {
+  const DD x2 = dd::mul(x, x), y2 = dd::mul(y, y), z2 = dd::mul(z, z);
+  const DD R = dd::sqrt(dd::add(dd::add(x2, y2), z2));
+  if (dd::is_zero(R)) return dd::mk(0.0);
+  DD g = dd::neg(dd::div(dd::mul(dd::mul(x, y), R), 3.0));
+  if (dd::positive(z2))
+    g = dd::sub(g, dd::div(dd::mul(dd::mul(z2, z), dd::atan(dd::div(dd::mul(x, y), dd::mul(z, R)))), 6.0));
+  if (dd::positive(y2))
+    g = dd::sub(g, dd::scale2(dd::mul(dd::mul(y2, z), dd::atan(dd::div(dd::mul(x, z), dd::mul(y, R)))), 0.5));
+  if (dd::positive(x2))
+    g = dd::sub(g, dd::scale2(dd::mul(dd::mul(x2, z), dd::atan(dd::div(dd::mul(y, z), dd::mul(x, R)))), 0.5));
+  const DD xy = dd::add(x2, y2), yz = dd::add(y2, z2), xz = dd::add(x2, z2);
+  const DD z3 = dd::scale2(z2, 3.0);
+  if (dd::positive(xy)) g = dd::add(g, dd::mul(dd::mul(dd::mul(x, y), z), dd::asinh(dd::div(z, dd::sqrt(xy)))));
+  if (dd::positive(yz))
+    g = dd::add(g, dd::div(dd::mul(dd::mul(y, dd::sub(z3, y2)), dd::asinh(dd::div(x, dd::sqrt(yz)))), 6.0));
+  if (dd::positive(xz))
+    g = dd::add(g, dd::div(dd::mul(dd::mul(x, dd::sub(z3, x2)), dd::asinh(dd::div(y, dd::sqrt(xz)))), 6.0));
   return g;
 }
 
-template <bool G>
-__device__ double dev_newell_tensor(double x, double y, double z, double dx, double dy, double dz) {
-  const double R = sqrt(x * x + y * y + z * z) / fmax(dx, fmax(dy, dz));
-  if (R > 60) {
-    const double r2 = x * x + y * y + z * z;
-    const double d = G ? -3 * x * y : -(2 * x * x - y * y - z * z);
-    return (r2 == 0 ? 0.0 : d / (r2 * r2 * sqrt(r2))) * dx * dy * dz / (4 * kPi);
-  }
-  // 27-point second difference, 1-D weights w(0) = 2, w(+-1) = -1
-  double s = 0.0;
-  for (int a = -1; a <= 1; ++a)
-    for (int b = -1; b <= 1; ++b)
-      for (int c = -1; c <= 1; ++c) {
-        const double w = (a == 0 ? 2.0 : -1.0) * (b == 0 ? 2.0 : -1.0) * (c == 0 ? 2.0 : -1.0);
-        s += w * (G ? dev_newell_g(x + a * dx, y + b * dy, z + c * dz)
-                    : dev_newell_f(x + a * dx, y + b * dy, z + c * dz));
-      }
-  return s / (4.0 * kPi * dx * dy * dz);
-}
+struct NewellGrid {
+  double dx, dy, dz;  // normalised cell (max = 1)
+  int ex, ey, ez;     // grid extents: offsets 0..ex etc. are stored
+  DD* F;              // [6][ez+1][ey+1][ex+1]
+};
 
-__device__ double dev_tensor_comp(int c, double x, double y, double z, double dx, double dy, double dz) {
+// f or g of component c (xx yy zz xy xz yz) at the integer offset (X, Y, Z),
+// arguments permuted as demag_tensor_yy / zz / xz / yz do
+__device__ DD newell_fn(int c, int64_t X, int64_t Y, int64_t Z, const NewellGrid& G) {
+  const DD x = dd::two_prod(static_cast<double>(X), G.dx), y = dd::two_prod(static_cast<double>(Y), G.dy),
+           z = dd::two_prod(static_cast<double>(Z), G.dz);
   switch (c) {
-    case 0: return dev_newell_tensor<false>(x, y, z, dx, dy, dz);
-    case 1: return dev_newell_tensor<false>(y, x, z, dy, dx, dz);
-    case 2: return dev_newell_tensor<false>(z, y, x, dz, dy, dx);
-    case 3: return dev_newell_tensor<true>(x, y, z, dx, dy, dz);
-    case 4: return dev_newell_tensor<true>(x, z, y, dx, dz, dy);
-    default: return dev_newell_tensor<true>(y, z, x, dy, dz, dx);
+    case 0: return ddf(x, y, z);
+    case 1: return ddf(y, x, z);
+    case 2: return ddf(z, y, x);
+    case 3: return ddg(x, y, z);
+    case 4: return ddg(x, z, y);
+    default: return ddg(y, z, x);
   }
 }
 
-// tensors_kernel_*!  src/micro/demag.jl:298-386 (sum over macro-PBC images)
-__global__ void k_newell(double* __restrict__ out, int nx, int ny, int nz, double dx, double dy,
-                         double dz, int Nx, int Ny, int Nz) {
+__global__ void k_newell_grid(NewellGrid G) {
+  const int64_t nxg = G.ex + 1, nyg = G.ey + 1, nzg = G.ez + 1;
+  const int64_t n = 6 * nxg * nyg * nzg;
+  const int64_t gid = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (gid >= n) return;
+  const int64_t X = gid % nxg, Y = (gid / nxg) % nyg, Z = (gid / (nxg * nyg)) % nzg;
+  const int c = static_cast<int>(gid / (nxg * nyg * nzg));
+  G.F[gid] = newell_fn(c, X, Y, Z, G);
+}
+
+// grid value with the parity of component c; offsets beyond the grid (not
+// reached by the near field) are evaluated directly
+__device__ DD newell_at(int c, int64_t X, int64_t Y, int64_t Z, const NewellGrid& G) {
+  const int64_t ax = X < 0 ? -X : X, ay = Y < 0 ? -Y : Y, az = Z < 0 ? -Z : Z;
+  if (ax > G.ex || ay > G.ey || az > G.ez) return newell_fn(c, X, Y, Z, G);
+  const DD v = G.F[((static_cast<int64_t>(c) * (G.ez + 1) + az) * (G.ey + 1) + ay) * (G.ex + 1) + ax];
+  const bool flip = (odd_axis(c, 0) && X < 0) ^ (odd_axis(c, 1) && Y < 0) ^ (odd_axis(c, 2) && Z < 0);
+  return flip ? dd::neg(v) : v;
+}
+
+// dipolar_tensor_xx / _xy (atomistic/demag.jl:106-138) * V / (4 pi), permuted
+// per component, in double-double
+__device__ DD newell_dipole(int c, DD x, DD y, DD z, const DD& V4pi) {
+  const DD x2 = dd::mul(x, x), y2 = dd::mul(y, y), z2 = dd::mul(z, z);
+  const DD r2 = dd::add(dd::add(x2, y2), z2);
+  DD num;
+  switch (c) {
+    case 0: num = dd::neg(dd::sub(dd::sub(dd::scale2(x2, 2.0), y2), z2)); break;
+    case 1: num = dd::neg(dd::sub(dd::sub(dd::scale2(y2, 2.0), x2), z2)); break;
+    case 2: num = dd::neg(dd::sub(dd::sub(dd::scale2(z2, 2.0), y2), x2)); break;
+    case 3: num = dd::mul(dd::mul(x, y), -3.0); break;
+    case 4: num = dd::mul(dd::mul(x, z), -3.0); break;
+    default: num = dd::mul(dd::mul(y, z), -3.0); break;
+  }
+  return dd::mul(dd::div(num, dd::mul(dd::mul(r2, r2), dd::sqrt(r2))), V4pi);
+}
+
+// tensors_kernel_*!  src/micro/demag.jl:298-386: one thread per (component,
+// cell offset), summing the macro-PBC images
+__global__ void k_newell(double* __restrict__ out, int nx, int ny, int nz, int Nx, int Ny, int Nz, NewellGrid G) {
   const int64_t N = static_cast<int64_t>(nx) * ny * nz;
   const int64_t gid = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   if (gid >= 6 * N) return;
@@ -755,28 +811,72 @@ __global__ void k_newell(double* __restrict__ out, int nx, int ny, int nz, doubl
   const int64_t I = gid - c * N;
   const int i = static_cast<int>(I % nx), j = static_cast<int>((I / nx) % ny),
             k = static_cast<int>(I / (static_cast<int64_t>(nx) * ny));
-  double sum = 0.0;
+  const double mx = fmax(G.dx, fmax(G.dy, G.dz));
+  const DD V = dd::mul(dd::two_prod(G.dx, G.dy), G.dz);
+  const DD pi4 = dd::scale2(DD{dd::kPiHi, dd::kPiLo}, 4.0);
+  const DD inv_near = dd::div(dd::mk(1.0), dd::mul(pi4, V));  // 1 / (4 pi dx dy dz)
+  const DD V4pi = dd::div(V, pi4);
+  DD sum = dd::mk(0.0);
   for (int p = -Nx; p <= Nx; ++p)
     for (int q = -Ny; q <= Ny; ++q)
       for (int r = -Nz; r <= Nz; ++r) {
-        const double x = (i + static_cast<double>(p) * nx) * dx;
-        const double y = (j + static_cast<double>(q) * ny) * dy;
-        const double z = (k + static_cast<double>(r) * nz) * dz;
-        sum += dev_tensor_comp(c, x, y, z, dx, dy, dz);
+        const int64_t X = i + static_cast<int64_t>(p) * nx, Y = j + static_cast<int64_t>(q) * ny,
+                      Z = k + static_cast<int64_t>(r) * nz;
+        // the switch as the reference evaluates it: FP64 coordinates, no contraction
+        const double xd = __dmul_rn(static_cast<double>(X), G.dx), yd = __dmul_rn(static_cast<double>(Y), G.dy),
+                     zd = __dmul_rn(static_cast<double>(Z), G.dz);
+        const double Rc = __ddiv_rn(__dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(xd, xd), __dmul_rn(yd, yd)),
+                                                          __dmul_rn(zd, zd))),
+                                    mx);
+        if (Rc > 60) {
+          const DD x = dd::two_prod(static_cast<double>(X), G.dx), y = dd::two_prod(static_cast<double>(Y), G.dy),
+                   z = dd::two_prod(static_cast<double>(Z), G.dz);
+          sum = dd::add(sum, newell_dipole(c, x, y, z, V4pi));
+          continue;
+        }
+        // 27-point second difference, 1-D weights w(0) = 2, w(+-1) = -1
+        DD s = dd::mk(0.0);
+        for (int a = -1; a <= 1; ++a)
+          for (int b = -1; b <= 1; ++b)
+            for (int e = -1; e <= 1; ++e) {
+              const double w = (a == 0 ? 2.0 : -1.0) * (b == 0 ? 2.0 : -1.0) * (e == 0 ? 2.0 : -1.0);
+              const DD v = newell_at(c, X + a, Y + b, Z + e, G);
+              s = dd::add(s, DD{v.hi * w, v.lo * w});
+            }
+        sum = dd::add(sum, dd::mul(s, inv_near));
       }
-  out[gid] = sum;
+  out[gid] = dd::to_double(sum);
 }
 
 int newell_tensor_device(int nx, int ny, int nz, double dx, double dy, double dz, int Nx, int Ny,
                          int Nz, double* out_dev, cudaStream_t st) {
   const double mx = std::max(dx, std::max(dy, dz));
-  const int64_t N = static_cast<int64_t>(nx) * ny * nz;
-  const int64_t tot = 6 * N;
+  NewellGrid G;
+  G.dx = dx / mx;
+  G.dy = dy / mx;
+  G.dz = dz / mx;
+  // near-field offsets |X| dx <= 60 (R <= 60 cells), plus the stencil's +-1,
+  // within the offsets the mesh and its images reach
+  auto extent = [](double d, int n, int Nimg) {
+    const double e = std::floor(60.0 / d) + 2.0;
+    const double reach = static_cast<double>(n - 1) + static_cast<double>(Nimg) * n + 1.0;
+    return static_cast<int>(std::min(e, reach));
+  };
+  G.ex = extent(G.dx, nx, Nx);
+  G.ey = extent(G.dy, ny, Ny);
+  G.ez = extent(G.dz, nz, Nz);
+  const int64_t ng = 6LL * (G.ex + 1) * (G.ey + 1) * (G.ez + 1);
+  G.F = nullptr;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&G.F), sizeof(DD) * ng);
+  if (e != cudaSuccess) return static_cast<int>(e);
   const int T = 128;
-  const int64_t blocks = (tot + T - 1) / T;
-  k_newell<<<static_cast<unsigned>(blocks), T, 0, st>>>(out_dev, nx, ny, nz, dx / mx, dy / mx, dz / mx,
-                                                        Nx, Ny, Nz);
-  return static_cast<int>(cudaGetLastError());
+  k_newell_grid<<<static_cast<unsigned>((ng + T - 1) / T), T, 0, st>>>(G);
+  const int64_t tot = 6 * static_cast<int64_t>(nx) * ny * nz;
+  k_newell<<<static_cast<unsigned>((tot + T - 1) / T), T, 0, st>>>(out_dev, nx, ny, nz, Nx, Ny, Nz, G);
+  e = cudaGetLastError();
+  const cudaError_t es = cudaStreamSynchronize(st);
+  cudaFree(G.F);
+  return static_cast<int>(e != cudaSuccess ? e : es);
 }
 
 

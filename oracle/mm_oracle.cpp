@@ -9,6 +9,8 @@
 // (paths relative to the MicroMagnetic.jl project root).  Array conventions
 // follow the reference: m, H are AoS [mx1,my1,mz1,mx2,...], cell id
 // (k*ny + j)*nx + i with x fastest (src/micro/mesh.jl:24-29, 0-based here).
+#include <quadmath.h>
+
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -206,28 +208,53 @@ double dipole_xy(double x, double y, double z) {
   return -3 * x * y / (R * R * std::sqrt(R));
 }
 
-// 27-point second difference with 1-D weights w(0)=2, w(+-1)=-1 (the
-// 8/-4/2/-1 pattern of demag.jl:206-234).
+// 27-point second difference in the reference's own order and FP64
+// arithmetic: demag_tensor_xx / demag_tensor_xy (demag.jl:194-296):
+// 8 f(0), then -4 f at the six face offsets, +2 f at the twelve edge offsets,
+// -f at the eight corners, accumulated left to right.
 template <typename F>
 double newell_sum(F fn, double x, double y, double z, double dx, double dy, double dz) {
-  double s = 0.0;
-  for (int a = -1; a <= 1; ++a)
-    for (int b = -1; b <= 1; ++b)
-      for (int c = -1; c <= 1; ++c) {
-        double w = (a == 0 ? 2.0 : -1.0) * (b == 0 ? 2.0 : -1.0) * (c == 0 ? 2.0 : -1.0);
-        s += w * fn(x + a * dx, y + b * dy, z + c * dz);
-      }
-  return s;
+  double t = 8.0 * fn(x, y, z);
+  t -= 4.0 * fn(x + dx, y, z);
+  t -= 4.0 * fn(x - dx, y, z);
+  t -= 4.0 * fn(x, y - dy, z);
+  t -= 4.0 * fn(x, y + dy, z);
+  t -= 4.0 * fn(x, y, z - dz);
+  t -= 4.0 * fn(x, y, z + dz);
+  t += 2.0 * fn(x + dx, y + dy, z);
+  t += 2.0 * fn(x + dx, y - dy, z);
+  t += 2.0 * fn(x - dx, y - dy, z);
+  t += 2.0 * fn(x - dx, y + dy, z);
+  t += 2.0 * fn(x + dx, y, z + dz);
+  t += 2.0 * fn(x + dx, y, z - dz);
+  t += 2.0 * fn(x - dx, y, z + dz);
+  t += 2.0 * fn(x - dx, y, z - dz);
+  t += 2.0 * fn(x, y - dy, z - dz);
+  t += 2.0 * fn(x, y - dy, z + dz);
+  t += 2.0 * fn(x, y + dy, z + dz);
+  t += 2.0 * fn(x, y + dy, z - dz);
+  t -= fn(x + dx, y + dy, z + dz);
+  t -= fn(x + dx, y + dy, z - dz);
+  t -= fn(x + dx, y - dy, z + dz);
+  t -= fn(x + dx, y - dy, z - dz);
+  t -= fn(x - dx, y + dy, z + dz);
+  t -= fn(x - dx, y + dy, z - dz);
+  t -= fn(x - dx, y - dy, z + dz);
+  t -= fn(x - dx, y - dy, z - dz);
+  return t;
+}
+
+// R in cells as demag_tensor_xx computes it (demag.jl:196)
+double cells_R(double x, double y, double z, double dx, double dy, double dz) {
+  return std::sqrt(x * x + y * y + z * z) / std::max(dx, std::max(dy, dz));
 }
 
 double tensor_xx(double x, double y, double z, double dx, double dy, double dz) {
-  double R = std::sqrt(x * x + y * y + z * z) / std::max(dx, std::max(dy, dz));
-  if (R > 60) return dipole_xx(x, y, z) * dx * dy * dz / (4 * kPi);
+  if (cells_R(x, y, z, dx, dy, dz) > 60) return dipole_xx(x, y, z) * dx * dy * dz / (4 * kPi);
   return newell_sum(newell_f, x, y, z, dx, dy, dz) / (4.0 * kPi * dx * dy * dz);
 }
 double tensor_xy(double x, double y, double z, double dx, double dy, double dz) {
-  double R = std::sqrt(x * x + y * y + z * z) / std::max(dx, std::max(dy, dz));
-  if (R > 60) return dipole_xy(x, y, z) * dx * dy * dz / (4 * kPi);
+  if (cells_R(x, y, z, dx, dy, dz) > 60) return dipole_xy(x, y, z) * dx * dy * dz / (4 * kPi);
   return newell_sum(newell_g, x, y, z, dx, dy, dz) / (4.0 * kPi * dx * dy * dz);
 }
 // component c: 0 xx, 1 yy, 2 zz, 3 xy, 4 xz, 5 yz (demag.jl:188-296)
@@ -239,6 +266,128 @@ double tensor_comp(int c, double x, double y, double z, double dx, double dy, do
     case 3: return tensor_xy(x, y, z, dx, dy, dz);
     case 4: return tensor_xy(x, z, y, dx, dz, dy);
     default: return tensor_xy(y, z, x, dy, dz, dx);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Accurate tensor (the default): the same Newell formulas evaluated in IEEE
+// binary128 (__float128, libquadmath's sqrtq / atanq / asinhq) at the exact
+// coordinates X * dx (X an integer offset: the product of an int32 and a
+// double is exact in binary128).  The 27-point differences cancel up to
+// R^6 (5e10 at R = 60 cells) of the function values; with a 113-bit
+// significand the near-field entries keep ~1e-23 relative accuracy, so each
+// rounds correctly to FP64.  The far-field dipole terms (no cancellation)
+// keep the reference's FP64 formula; image sums are accumulated in binary128
+// and rounded once.  The switch R > 60 is the reference's FP64 test.
+// ---------------------------------------------------------------------------
+using q128 = __float128;
+bool g_reference_tensor = false;  // orc_set_reference_tensor
+
+q128 qf(q128 x, q128 y, q128 z) {
+  const q128 x2 = x * x, y2 = y * y, z2 = z * z;
+  const q128 R = sqrtq(x2 + y2 + z2);
+  if (R == 0) return 0;
+  q128 f = (2 * x2 - y2 - z2) * R / 6;
+  if (x2 > 0) f -= x * y * z * atanq(y * z / (x * R));
+  if (x2 + z2 > 0) f += y * (z2 - x2) * asinhq(y / sqrtq(x2 + z2)) / 2;
+  if (x2 + y2 > 0) f += z * (y2 - x2) * asinhq(z / sqrtq(x2 + y2)) / 2;
+  return f;
+}
+
+q128 qg(q128 x, q128 y, q128 z) {
+  const q128 x2 = x * x, y2 = y * y, z2 = z * z;
+  const q128 R = sqrtq(x2 + y2 + z2);
+  if (R == 0) return 0;
+  q128 g = -x * y * R / 3;
+  if (z2 > 0) g -= z2 * z * atanq(x * y / (z * R)) / 6;
+  if (y2 > 0) g -= y2 * z * atanq(x * z / (y * R)) / 2;
+  if (x2 > 0) g -= x2 * z * atanq(y * z / (x * R)) / 2;
+  if (x2 + y2 > 0) g += x * y * z * asinhq(z / sqrtq(x2 + y2));
+  if (y2 + z2 > 0) g += y * (3 * z2 - y2) * asinhq(x / sqrtq(y2 + z2)) / 6;
+  if (x2 + z2 > 0) g += x * (3 * z2 - x2) * asinhq(y / sqrtq(x2 + z2)) / 6;
+  return g;
+}
+
+// f or g of component c at integer offsets, arguments permuted as
+// demag_tensor_yy / zz / xz / yz (demag.jl:236-296) do
+q128 q_newell(int c, int64_t X, int64_t Y, int64_t Z, double dx, double dy, double dz) {
+  const q128 x = static_cast<q128>(X) * dx, y = static_cast<q128>(Y) * dy, z = static_cast<q128>(Z) * dz;
+  switch (c) {
+    case 0: return qf(x, y, z);
+    case 1: return qf(y, x, z);
+    case 2: return qf(z, y, x);
+    case 3: return qg(x, y, z);
+    case 4: return qg(x, z, y);
+    default: return qg(y, z, x);
+  }
+}
+
+// Real-space tensor out[c*N + I] (6 x N, xx yy zz xy xz yz) for normalised
+// cell sizes, with macro-PBC images (tensors_kernel_*!, demag.jl:298-386).
+// accurate = false: the reference's FP64 arithmetic (tensor_comp).
+void newell_table(int nx, int ny, int nz, double dx, double dy, double dz, int Nx, int Ny, int Nz, bool accurate,
+                  double* out) {
+  const int64_t N = static_cast<int64_t>(nx) * ny * nz;
+  // near-field function table over offsets 0..e (f even in each argument,
+  // g odd in its first two): R <= 60 cells plus the stencil's +-1
+  auto extent = [](double d, int n, int Nimg) {
+    return static_cast<int>(std::min(std::floor(60.0 / d) + 2.0, static_cast<double>(n - 1) + Nimg * 1.0 * n + 1.0));
+  };
+  const int ex = extent(dx, nx, Nx), ey = extent(dy, ny, Ny), ez = extent(dz, nz, Nz);
+  const int64_t gx = ex + 1, gy = ey + 1, gz = ez + 1;
+  const bool odd[6][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+  std::vector<q128> F;
+  if (accurate) {
+    F.resize(static_cast<size_t>(6 * gx * gy * gz));
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t t = 0; t < 6 * gx * gy * gz; ++t) {
+      const int64_t X = t % gx, Y = (t / gx) % gy, Z = (t / (gx * gy)) % gz;
+      const int c = static_cast<int>(t / (gx * gy * gz));
+      F[static_cast<size_t>(t)] = q_newell(c, X, Y, Z, dx, dy, dz);
+    }
+  }
+  auto at = [&](int c, int64_t X, int64_t Y, int64_t Z) -> q128 {
+    const int64_t ax = X < 0 ? -X : X, ay = Y < 0 ? -Y : Y, az = Z < 0 ? -Z : Z;
+    if (ax > ex || ay > ey || az > ez) return q_newell(c, X, Y, Z, dx, dy, dz);
+    const q128 v = F[static_cast<size_t>(((c * gz + az) * gy + ay) * gx + ax)];
+    const bool flip = (odd[c][0] && X < 0) != ((odd[c][1] && Y < 0) != (odd[c][2] && Z < 0));
+    return flip ? -v : v;
+  };
+  const q128 qpi = 4 * atanq(static_cast<q128>(1));
+  const q128 inv_near = 1 / (4 * qpi * static_cast<q128>(dx) * dy * dz);
+  for (int c = 0; c < 6; ++c) {
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t I = 0; I < N; ++I) {
+      const int i = static_cast<int>(I % nx), j = static_cast<int>((I / nx) % ny),
+                k = static_cast<int>(I / (static_cast<int64_t>(nx) * ny));
+      double sum = 0.0;
+      q128 qsum = 0;
+      for (int p = -Nx; p <= Nx; ++p)
+        for (int q = -Ny; q <= Ny; ++q)
+          for (int r = -Nz; r <= Nz; ++r) {
+            const int64_t X = i + static_cast<int64_t>(p) * nx, Y = j + static_cast<int64_t>(q) * ny,
+                          Z = k + static_cast<int64_t>(r) * nz;
+            const double x = static_cast<double>(X) * dx, y = static_cast<double>(Y) * dy,
+                         z = static_cast<double>(Z) * dz;
+            if (!accurate) {
+              sum += tensor_comp(c, x, y, z, dx, dy, dz);
+              continue;
+            }
+            if (cells_R(x, y, z, dx, dy, dz) > 60) {
+              qsum += tensor_comp(c, x, y, z, dx, dy, dz);
+              continue;
+            }
+            q128 s = 0;
+            for (int a = -1; a <= 1; ++a)
+              for (int b = -1; b <= 1; ++b)
+                for (int e = -1; e <= 1; ++e) {
+                  const int w = (a == 0 ? 2 : -1) * (b == 0 ? 2 : -1) * (e == 0 ? 2 : -1);
+                  s += w * at(c, X + a, Y + b, Z + e);
+                }
+            qsum += s * inv_near;
+          }
+      out[c * N + I] = accurate ? static_cast<double>(qsum) : sum;
+    }
   }
 }
 
@@ -481,28 +630,19 @@ void demag_init(const Sim& s, Term& tm, int Nx, int Ny, int Nz, const double* te
   const int64_t N = g.n;
   std::vector<double> t(N);
   std::vector<cd> pad(P);
+  // tensors_kernel_*!  demag.jl:298-386 (macro-PBC image sums)
+  std::vector<double> table;
+  if (!tensor_override) {
+    table.resize(static_cast<size_t>(6 * N));
+    newell_table(nx, ny, nz, dx, dy, dz, Nx, Ny, Nz, !g_reference_tensor, table.data());
+  }
   // tensor components and the odd axes of each (fill_tensors calls, demag.jl:56-83)
   const bool odd[6][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
   for (int c = 0; c < 6; ++c) {
     if (tensor_override) {
       std::copy(tensor_override + c * N, tensor_override + (c + 1) * N, t.begin());
     } else {
-      // tensors_kernel_*!  demag.jl:298-386 (macro-PBC image sums)
-#pragma omp parallel for schedule(dynamic, 16)
-      for (int64_t I = 0; I < N; ++I) {
-        int i = static_cast<int>(I % nx), j = static_cast<int>((I / nx) % ny),
-            k = static_cast<int>(I / (static_cast<int64_t>(nx) * ny));
-        double sum = 0.0;
-        for (int p = -Nx; p <= Nx; ++p)
-          for (int q = -Ny; q <= Ny; ++q)
-            for (int r = -Nz; r <= Nz; ++r) {
-              double x = (i + static_cast<double>(p) * nx) * dx;
-              double y = (j + static_cast<double>(q) * ny) * dy;
-              double z = (k + static_cast<double>(r) * nz) * dz;
-              sum += tensor_comp(c, x, y, z, dx, dy, dz);
-            }
-        t[I] = sum;
-      }
+      std::copy(table.begin() + c * N, table.begin() + (c + 1) * N, t.begin());
     }
     // fill_tensors_kernel!  demag.jl:394-412
     std::fill(pad.begin(), pad.end(), cd(0.0, 0.0));
@@ -1298,28 +1438,24 @@ int orc_add_demag(void* h, int Nx, int Ny, int Nz, const double* tensor) {
 
 // Newell real-space tensor (6 x N, order xx yy zz xy xz yz) in normalised
 // cell units, with macro-PBC images: tensors_kernel_*! demag.jl:298-386.
-void orc_demag_tensor(int nx, int ny, int nz, double dx, double dy, double dz, int Nx, int Ny,
-                      int Nz, double* out) {
+// accurate != 0: binary128 near field (the default of add_demag); 0: the
+// reference's FP64 arithmetic.
+void orc_demag_tensor(int nx, int ny, int nz, double dx, double dy, double dz, int Nx, int Ny, int Nz, int accurate,
+                      double* out) {
   const double mx = std::max(dx, std::max(dy, dz));
-  const double ddx = dx / mx, ddy = dy / mx, ddz = dz / mx;
-  const int64_t N = static_cast<int64_t>(nx) * ny * nz;
-  for (int c = 0; c < 6; ++c) {
-#pragma omp parallel for schedule(dynamic, 16)
-    for (int64_t I = 0; I < N; ++I) {
-      int i = static_cast<int>(I % nx), j = static_cast<int>((I / nx) % ny),
-          k = static_cast<int>(I / (static_cast<int64_t>(nx) * ny));
-      double sum = 0.0;
-      for (int p = -Nx; p <= Nx; ++p)
-        for (int q = -Ny; q <= Ny; ++q)
-          for (int r = -Nz; r <= Nz; ++r) {
-            double x = (i + static_cast<double>(p) * nx) * ddx;
-            double y = (j + static_cast<double>(q) * ny) * ddy;
-            double z = (k + static_cast<double>(r) * nz) * ddz;
-            sum += tensor_comp(c, x, y, z, ddx, ddy, ddz);
-          }
-      out[c * N + I] = sum;
-    }
-  }
+  newell_table(nx, ny, nz, dx / mx, dy / mx, dz / mx, Nx, Ny, Nz, accurate != 0, out);
+}
+
+// Tensor arithmetic of the following add_demag calls: 1 = the reference's
+// FP64 arithmetic, 0 = binary128 near field (default).
+void orc_set_reference_tensor(int on) { g_reference_tensor = on != 0; }
+
+// f or g of component c (xx yy zz xy xz yz, permuted as in demag.jl) at
+// x = X dx, y = Y dy, z = Z dz, in binary128, returned as hi + lo doubles
+void orc_newell_fn(int c, int64_t X, int64_t Y, int64_t Z, double dx, double dy, double dz, double* hi_lo) {
+  const q128 v = q_newell(c, X, Y, Z, dx, dy, dz);
+  hi_lo[0] = static_cast<double>(v);
+  hi_lo[1] = static_cast<double>(v - static_cast<q128>(hi_lo[0]));
 }
 
 // Evaluate one term on m (or on the stored m if m == null); field 3N, energy N.

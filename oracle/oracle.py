@@ -51,7 +51,9 @@ def lib():
         L.orc_add_dmi_interfacial.argtypes = [vp, _dp]
         L.orc_add_anis.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.orc_add_demag.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
-        L.orc_demag_tensor.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 3 + [ctypes.c_int] * 3 + [_dp]
+        L.orc_demag_tensor.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 3 + [ctypes.c_int] * 4 + [_dp]
+        L.orc_set_reference_tensor.argtypes = [ctypes.c_int]
+        L.orc_newell_fn.argtypes = [ctypes.c_int] + [ctypes.c_int64] * 3 + [ctypes.c_double] * 3 + [_dp]
         L.orc_term_field.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp]
         L.orc_effective_field.argtypes = [vp, _dp, _dp]
         L.orc_llg_rhs.argtypes = [vp, _dp, _dp]
@@ -96,12 +98,28 @@ def max_threads() -> int:
     return int(lib().orc_max_threads())
 
 
-def demag_tensor(nx, ny, nz, dx, dy, dz, Nx=0, Ny=0, Nz=0) -> np.ndarray:
-    """Real-space Newell tensor, shape (6, N) in order xx yy zz xy xz yz."""
+def demag_tensor(nx, ny, nz, dx, dy, dz, Nx=0, Ny=0, Nz=0, accurate=True) -> np.ndarray:
+    """Real-space Newell tensor, shape (6, N) in order xx yy zz xy xz yz.
+    accurate=True: near field in binary128 (correctly rounded entries);
+    False: the reference's FP64 arithmetic."""
     n = nx * ny * nz
     out = np.zeros((6, n))
-    lib().orc_demag_tensor(nx, ny, nz, dx, dy, dz, Nx, Ny, Nz, _ptr(out))
+    lib().orc_demag_tensor(nx, ny, nz, dx, dy, dz, Nx, Ny, Nz, 1 if accurate else 0, _ptr(out))
     return out
+
+
+def reference_tensor_arithmetic(on: bool) -> None:
+    """Newell tensor of the following add_demag calls in the reference's FP64
+    arithmetic (True) or with the binary128 near field (False, the default)."""
+    lib().orc_set_reference_tensor(1 if on else 0)
+
+
+def newell_fn(c, X, Y, Z, dx, dy, dz):
+    """f (c = 0..2) or g (c = 3..5) of tensor component c at the integer
+    offset (X, Y, Z) times the normalised cell, in binary128: (hi, lo)."""
+    out = np.zeros(2)
+    lib().orc_newell_fn(c, X, Y, Z, dx, dy, dz, _ptr(out))
+    return out[0], out[1]
 
 
 class OracleSim:

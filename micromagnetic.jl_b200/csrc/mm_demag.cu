@@ -73,6 +73,39 @@ static int smem_budget_bytes() {
 }
 
 
+// Largest power-of-two radix of the FP32 shared-memory passes (16 or 32;
+// MMCUDA_MAXRADIX overrides).  A radix-32 butterfly holds 32 complex values a
+// thread, above the 80-register budget of the 3-blocks-per-SM passes: those
+// stages run with spilled registers.
+static int fp32_max_radix() {
+  static const int v = [] {
+    const char* e = getenv("MMCUDA_MAXRADIX");
+    const int r = e ? atoi(e) : 16;
+    return r == 32 ? 32 : 16;
+  }();
+  return v;
+}
+
+// The register-resident x and y passes (mm_wreg.cu) where they apply, unless
+// MMCUDA_WREG=0 keeps the shared-memory kernels
+static bool wreg_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MMCUDA_WREG");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// The register-resident z convolution (mm_zpair.cu) where it applies, unless
+// MMCUDA_ZPAIR=0 keeps the shared-memory kernels
+static bool zpair_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MMCUDA_ZPAIR");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 // 3-D column-major spectra (DemagGeom::yT) unless MMCUDA_COLS3D=0 keeps the
 // row-major layout; both run the same arithmetic on every line
 static bool cols3d_enabled() {
@@ -940,6 +973,7 @@ static void set_smem_attrs() {
   if (tracked && ((done_mask >> dev) & 1ull)) return;
   set_smem_attrs_nt<R, kHotNT>();
   if (sizeof(R) == 8) set_smem_attrs_nt<double, kTensorNT>();
+  if (sizeof(R) == 4) wreg_set_attrs();
   if (tracked) done_mask |= 1ull << dev;
 }
 
@@ -1002,14 +1036,18 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
   const bool zc2 = (g.Pz & (g.Pz - 1)) == 0 && g.Pz >= 4 && (g.Pz <= 128 || (sizeof(R) == 4 && g.Pz == 256));
   if (g.Pz > 1 && !long_y && cols_ok && zc2 && cols3d_enabled()) {
     FftPlan1 py;
-    make_fft_plan(g.Py, py, sizeof(R) == 4 ? 32 : 8);
+    make_fft_plan(g.Py, py, sizeof(R) == 4 ? fp32_max_radix() : 8);
     if (lines_tile<R>(g.Hx, g.Py, 1, std::max(1, line_fft_buffers(py))) < 8) g.yT = g.xT = 1;
   }
+  g.wreg = 0;
+  if (sizeof(R) == 4 && g.Pz > 1 && !long_x && !long_y && zc2 && wreg_enabled() &&
+      wreg_applies(nx, ny, nz, g.Px, g.Py))
+    g.wreg = g.yT = g.xT = 1;
   if ((long_x && !make_fft_plan(g.Lc, gplx, 8)) || (long_y && !make_fft_plan(g.Py, gply, 8))) {
     snprintf(err, nerr, "demag: no radix plan");
     return -1;
   }
-  const int maxr = sizeof(R) == 4 ? 32 : 8;
+  const int maxr = sizeof(R) == 4 ? fp32_max_radix() : 8;
   if (!make_fft_plan(g.Lc > 0 ? g.Lc : 1, g.plx, maxr) || !make_fft_plan(g.Py, g.ply, maxr) ||
       !make_fft_plan(g.Pz, g.plz, maxr)) {
     snprintf(err, nerr, "demag: no radix plan");
@@ -1485,6 +1523,12 @@ template <typename R>
 static void launch_zconv(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st,
                          int Wforce = 0) {
   using C = cplx_t<R>;
+  if constexpr (sizeof(R) == 4) {
+    if (zpair_enabled() && zpair_applies(g)) {
+      launch_zpair_f32(g, Y, Nhat, st);
+      return;
+    }
+  }
   if (try_zconv2<R>(g, Y, Nhat, twz, st, Wforce)) return;
   const int W = Wforce > 0 ? Wforce : lines_tile<R>(g.Hx, g.Pz, 3, 2);
   const int half = 3 * W * (g.Pz | 1);
@@ -1502,6 +1546,12 @@ static bool run_pass(const DemagPlan<R>& p, DemagGeom g, int which, const R* m, 
   using C = cplx_t<R>;
   constexpr int NT = kHotNT;
   const int64_t xlines = 3LL * g.ny * g.nz, ncz = 3LL * g.nz;
+  if constexpr (sizeof(R) == 4) {
+    if (g.wreg && which != 2) {
+      launch_wreg_f32(which, g, m, mu0Ms, p.X, p.Y, Hd, p.twx, p.twy, st);
+      return true;
+    }
+  }
   switch (which) {
     case 0:
       if (p.long_x) {
@@ -1615,6 +1665,7 @@ int DemagPlan<R>::autotune(const R* m, const R* mu0Ms, R* Hd, cudaStream_t st) {
   for (int which = 1; which <= 3; ++which) {
     if (fused2d && which != 2) continue;
     if (long_y && (which != 2 || g.Pz == 1)) continue;  // global-memory stages have no tile
+    if (g.wreg && which != 2) continue;                  // register passes have no tile
     // the static rule's W is the incumbent; another W must be 3 % faster
     // (timing noise, e.g. under a profiler, then cannot move the choice)
     tile[which] = 0;

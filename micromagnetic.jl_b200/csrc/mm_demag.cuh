@@ -36,6 +36,10 @@ struct DemagGeom {
   // x pass to the forward y pass (xT is set), and row-major again from the
   // inverse y pass to the inverse x pass
   int yT;
+  // FP32 power-of-two meshes (nx, ny = 32 Q, Px = 2 nx, Py = 2 ny, 3-D): the
+  // x and y passes run register-resident (mm_wreg.cu) with X column-major in
+  // both directions (yT and xT are set too)
+  int wreg;
   const int* gate;  // device flag: kernels return at once when *gate == 0 (null: always run)
 };
 
@@ -92,6 +96,18 @@ class DemagPlan {
  private:
   size_t bytes_ = 0;
 };
+
+// Register-resident z convolution for Pz = 32 (nz <= 16), FP32 form
+// (mm_zpair.cu): in place on Y, either spectrum layout.
+bool zpair_applies(const DemagGeom& g);
+void launch_zpair_f32(const DemagGeom& g, float2* Y, const float* Nhat, cudaStream_t st);
+
+// Register-resident x and y passes, FP32 form (mm_wreg.cu): which = 0 fwd-x
+// (m, Ms -> X), 1 fwd-y (X -> Y), 3 inv-y (Y -> X), 4 inv-x (X -> H).
+bool wreg_applies(int nx, int ny, int nz, int Px, int Py);
+void wreg_set_attrs();
+void launch_wreg_f32(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,
+                     const float2* twx, const float2* twy, cudaStream_t st);
 
 // FP64 Newell tensor (real space) with macro-PBC images, on the device:
 // out[c*N + I], c = xx yy zz xy xz yz.  dx,dy,dz are the raw cell sizes.

@@ -1,0 +1,269 @@
+// mm_wreg.cu -- register-resident x and y passes of the demag convolution for
+// power-of-two meshes, FP32 form (internal).
+//
+// Applies when nx = Lc and ny are 32 Q with Q in {4, 8, 16, 32} (padded
+// Px = 2 nx, Py = 2 ny), on 3-D meshes.  Every line is transformed by a group
+// of Q lanes holding 32 values each (mm_wfft.cuh); shared memory only carries
+// the warp transposes and the block's staging of coalesced HBM segments, and
+// each block synchronises three or four times.  Layout (DemagGeom::wreg):
+//   X  [3][Hx][nz][ny] column-major in both directions (the x passes stage
+//      tiles of RB consecutive rows through shared memory so that a column
+//      segment of RB rows is one coalesced HBM access);
+//   Y  [3][Hx][nz][Py] column-major, as for DemagGeom::yT.
+// The zero padding is pruned: the x transform of real rows packs pairs
+// (x[2n], x[2n+1]) into the Lc-point complex transform, half of whose inputs
+// are zero; the forward y transform of ny inputs into Py = 2 ny outputs is
+// two ny-point transforms by output parity s,
+//     Y[2k + s] = DFT_ny(x[n] w_Py^(n s))[k],
+// and the inverse keeps y < ny as u0[y] + w_Py^(-y) u1[y], us the ny-point
+// inverse transform of Y[2k + s].  (src/micro/demag.jl:102-131.)
+#include "mm_demag.cuh"
+#include "mm_wfft.cuh"
+
+namespace mm {
+
+namespace {
+
+constexpr int kWrNT = 128;  // x passes: 4 warps
+constexpr int kWyNT = 256;  // y passes: 8 warps, 4 lines x 2 halves (Q = 32)
+
+// rows of one x-pass block: 4 warps x (32 / Q) groups
+template <int Q> constexpr int x_rows() { return 4 * (32 / Q); }
+
+// ---------------------------------------------------------------- x forward
+// Rows of m * mu0Ms (zero padded to Px = 2 Lc) -> X column-major.
+template <int Q>
+__global__ void __launch_bounds__(kWrNT) k_xfwd_w(const float* __restrict__ m, const float* __restrict__ Ms,
+                                                 float2* __restrict__ X, DemagGeom g, const float2* __restrict__ twx) {
+  constexpr int RB = x_rows<Q>(), L = 32 * Q;
+  __shared__ __align__(16) float2 sm[4 * wtile_size<Q>()];
+  if (g.gate && !*g.gate) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gq = lane / Q, q = lane % Q;
+  const int rows = g.ny * g.nz, Hx = g.Hx, nx = g.nx;
+  const int64_t N = static_cast<int64_t>(rows) * nx;
+  const int line0 = blockIdx.x * RB;  // rows % RB == 0: one component a block
+  const int c = line0 / rows, row0 = line0 - c * rows;
+  const int rl = warp * (32 / Q) + gq;
+  const int64_t rb = static_cast<int64_t>(row0 + rl) * nx;
+  const float2* m2 = reinterpret_cast<const float2*>(m + c * N + rb);
+  const float2* s2 = reinterpret_cast<const float2*>(Ms + rb);
+  float2 v[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j < 16) {  // z[n] = (x[2n], x[2n+1]), nonzero for n < Lc / 2
+      const float2 a = m2[q + Q * j], b = s2[q + Q * j];
+      v[j] = make_float2(a.x * b.x, a.y * b.y);
+    } else {
+      v[j] = make_float2(0.f, 0.f);
+    }
+  }
+  wfft<Q, false, 2>(v, sm + warp * wtile_size<Q>(), twx);
+  __syncthreads();  // every warp is done with its transpose tile
+#pragma unroll
+  for (int r = 0; r < 32; ++r) sm[(q + Q * (r / Q) + 32 * (r % Q)) * RB + rl] = v[r];
+  __syncthreads();
+  // X[k] = E + w_Px^k O, E = (Z[k] + conj Z[Lc-k]) / 2, O = (Z[k] - conj Z[Lc-k]) / 2i
+  for (int e = threadIdx.x; e < Hx * RB; e += kWrNT) {
+    const int k = e / RB, r = e - k * RB;
+    const float2 zk = sm[(k == L ? 0 : k) * RB + r];
+    float2 zc = sm[(k == 0 ? 0 : L - k) * RB + r];
+    zc.y = -zc.y;
+    const float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+    const float2 od = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
+    X[(static_cast<int64_t>(c) * Hx + k) * rows + row0 + r] = cadd(ev, cmul(__ldg(twx + k), od));
+  }
+}
+
+// ---------------------------------------------------------------- x inverse
+// X column-major -> real rows (c2r, unnormalised), keeps x < nx.
+template <int Q>
+__global__ void __launch_bounds__(kWrNT) k_xinv_w(const float2* __restrict__ X, float* __restrict__ H, DemagGeom g,
+                                                 const float2* __restrict__ twx) {
+  constexpr int RB = x_rows<Q>(), L = 32 * Q;
+  __shared__ __align__(16) float2 sm[4 * wtile_size<Q>()];
+  if (g.gate && !*g.gate) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gq = lane / Q, q = lane % Q;
+  const int rows = g.ny * g.nz, Hx = g.Hx, nx = g.nx;
+  const int64_t N = static_cast<int64_t>(rows) * nx;
+  const int line0 = blockIdx.x * RB;
+  const int c = line0 / rows, row0 = line0 - c * rows;
+  const int rl = warp * (32 / Q) + gq;
+  for (int e = threadIdx.x; e < Hx * RB; e += kWrNT) {
+    const int k = e / RB, r = e - k * RB;
+    sm[e] = X[(static_cast<int64_t>(c) * Hx + k) * rows + row0 + r];
+  }
+  __syncthreads();
+  // Z'[k] = (A + B) + i (A - B) conj(w_Px^k), A = X[k], B = conj X[Lc - k]
+  float2 v[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const int k = q + Q * j;
+    const float2 a = sm[k * RB + rl];
+    float2 b = sm[(L - k) * RB + rl];
+    b.y = -b.y;
+    float2 w = __ldg(twx + k);
+    w.y = -w.y;
+    const float2 d = cmul(csub(a, b), w);
+    v[j] = make_float2(a.x + b.x - d.y, a.y + b.y + d.x);
+  }
+  __syncthreads();  // the staging tile becomes the transpose tiles
+  wfft<Q, true, 2>(v, sm + warp * wtile_size<Q>(), twx);
+  // z[n] = (x[2n], x[2n+1]) for n < Lc / 2: registers with k2 = r % Q < Q / 2
+  float2* h2 = reinterpret_cast<float2*>(H + c * N + static_cast<int64_t>(row0 + rl) * nx);
+#pragma unroll
+  for (int r = 0; r < 32; ++r) {
+    if (r % Q < Q / 2) h2[q + Q * (r / Q) + 32 * (r % Q)] = v[r];
+  }
+}
+
+// ---------------------------------------------------------------- y forward
+// X column (ny values) -> Y column (Py = 2 ny values); line = (c Hx + kx) nz + z.
+// Unit u = group in the block: line (u >> 1), half s = u & 1.
+template <int Q>
+__global__ void __launch_bounds__(kWyNT) k_yfwd_w(const float2* __restrict__ X, float2* __restrict__ Y, DemagGeom g,
+                                                 const float2* __restrict__ twy, int nlines) {
+  constexpr int NL = 4 * (32 / Q), Py = 64 * Q;  // lines a block, padded length
+  extern __shared__ __align__(16) float2 smy[];
+  if (g.gate && !*g.gate) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gq = lane / Q, q = lane % Q;
+  const int u = warp * (32 / Q) + gq, s = u & 1, ll = u >> 1;
+  const int line0 = blockIdx.x * NL;
+  const int line = line0 + ll;
+  const bool live = line < nlines;
+  const float2* xc = X + static_cast<int64_t>(line) * (Py / 2);
+  float2 v[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    float2 a = live ? xc[q + Q * j] : make_float2(0.f, 0.f);
+    if (s) a = cmul(a, __ldg(twy + q + Q * j));
+    v[j] = a;
+  }
+  wfft<Q, false, 2>(v, smy + warp * wtile_size<Q>(), twy);
+  __syncthreads();  // transposes done: the tiles become the block's output columns
+  float2* col = smy + ll * Py;
+#pragma unroll
+  for (int r = 0; r < 32; ++r) col[2 * (q + Q * (r / Q) + 32 * (r % Q)) + s] = v[r];
+  __syncthreads();
+  const int nl = min(NL, nlines - line0);
+  const float4* src = reinterpret_cast<const float4*>(smy);
+  float4* dst = reinterpret_cast<float4*>(Y + static_cast<int64_t>(line0) * Py);
+  for (int e = threadIdx.x; e < nl * Py / 2; e += kWyNT) dst[e] = src[e];
+}
+
+// ---------------------------------------------------------------- y inverse
+// Y column (Py values) -> X column (y < ny).
+template <int Q>
+__global__ void __launch_bounds__(kWyNT) k_yinv_w(const float2* __restrict__ Y, float2* __restrict__ X, DemagGeom g,
+                                                 const float2* __restrict__ twy, int nlines) {
+  constexpr int NL = 4 * (32 / Q), Py = 64 * Q, ny = 32 * Q;
+  extern __shared__ __align__(16) float2 smy[];
+  if (g.gate && !*g.gate) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gq = lane / Q, q = lane % Q;
+  const int u = warp * (32 / Q) + gq, s = u & 1, ll = u >> 1;
+  const int line0 = blockIdx.x * NL;
+  const int nl = min(NL, nlines - line0);
+  {
+    const float4* src = reinterpret_cast<const float4*>(Y + static_cast<int64_t>(line0) * Py);
+    float4* dst = reinterpret_cast<float4*>(smy);
+    for (int e = threadIdx.x; e < nl * Py / 2; e += kWyNT) dst[e] = src[e];
+  }
+  __syncthreads();
+  float2 v[32];
+  const float2* col = smy + ll * Py;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = ll < nl ? col[2 * (q + Q * j) + s] : make_float2(0.f, 0.f);
+  __syncthreads();  // the staged columns become the transpose tiles
+  wfft<Q, true, 2>(v, smy + warp * wtile_size<Q>(), twy);
+  if (s) {
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+      float2 w = __ldg(twy + q + Q * (r / Q) + 32 * (r % Q));
+      w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+  }
+  __syncthreads();
+  float2* half = smy + (ll * 2 + s) * ny;
+#pragma unroll
+  for (int r = 0; r < 32; ++r) half[q + Q * (r / Q) + 32 * (r % Q)] = v[r];
+  __syncthreads();
+  float2* xo = X + static_cast<int64_t>(line0) * ny;
+  for (int e = threadIdx.x; e < nl * ny; e += kWyNT) {
+    const int l = e / ny, y = e - l * ny;
+    const float2 a = smy[(2 * l) * ny + y], b = smy[(2 * l + 1) * ny + y];
+    xo[e] = make_float2(a.x + b.x, a.y + b.y);
+  }
+}
+
+template <int Q>
+void launch_q(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,
+              const float2* twx, const float2* twy, cudaStream_t st) {
+  const int rows = g.ny * g.nz;
+  const int ylines = 3 * g.Hx * g.nz;
+  constexpr int NL = 4 * (32 / Q);
+  const size_t ysm = static_cast<size_t>(8) * wtile_size<Q>() * sizeof(float2);
+  switch (which) {
+    case 0:
+      k_xfwd_w<Q><<<3 * rows / x_rows<Q>(), kWrNT, 0, st>>>(m, Ms, X, g, twx);
+      break;
+    case 1:
+      k_yfwd_w<Q><<<(ylines + NL - 1) / NL, kWyNT, ysm, st>>>(X, Y, g, twy, ylines);
+      break;
+    case 3:
+      k_yinv_w<Q><<<(ylines + NL - 1) / NL, kWyNT, ysm, st>>>(Y, X, g, twy, ylines);
+      break;
+    case 4:
+      k_xinv_w<Q><<<3 * rows / x_rows<Q>(), kWrNT, 0, st>>>(X, H, g, twx);
+      break;
+    default:
+      break;
+  }
+}
+
+template <int Q>
+void set_attrs_q() {
+  const int b = 8 * wtile_size<Q>() * static_cast<int>(sizeof(float2));
+  cudaFuncSetAttribute(k_yfwd_w<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  cudaFuncSetAttribute(k_yinv_w<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+}
+
+int wq(int n) {
+  switch (n) {
+    case 128: return 4;
+    case 256: return 8;
+    case 512: return 16;
+    case 1024: return 32;
+    default: return 0;
+  }
+}
+
+}  // namespace
+
+bool wreg_applies(int nx, int ny, int nz, int Px, int Py) {
+  return nz > 1 && wq(nx) && wq(ny) && Px == 2 * nx && Py == 2 * ny;
+}
+
+void wreg_set_attrs() {
+  set_attrs_q<4>();
+  set_attrs_q<8>();
+  set_attrs_q<16>();
+  set_attrs_q<32>();
+}
+
+void launch_wreg_f32(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,
+                     const float2* twx, const float2* twy, cudaStream_t st) {
+  // the x passes run on rows (Q of nx), the y passes on columns (Q of ny)
+  const int q = (which == 0 || which == 4) ? wq(g.nx) : wq(g.ny);
+  switch (q) {
+    case 4: launch_q<4>(which, g, m, Ms, X, Y, H, twx, twy, st); break;
+    case 8: launch_q<8>(which, g, m, Ms, X, Y, H, twx, twy, st); break;
+    case 16: launch_q<16>(which, g, m, Ms, X, Y, H, twx, twy, st); break;
+    default: launch_q<32>(which, g, m, Ms, X, Y, H, twx, twy, st); break;
+  }
+}
+
+}  // namespace mm

@@ -1551,6 +1551,13 @@ int orc_run_until(void* h, double t_end, double* stats) {
   return ok;
 }
 
+// integrator.y_current of the adaptive stepper (advance_step does not copy it
+// into sim.spin; run_until does)
+void orc_get_y_current(void* h, double* y) {
+  Sim* s = static_cast<Sim*>(h);
+  std::copy(s->y_current.begin(), s->y_current.end(), y);
+}
+
 // One advance_step(sim, ::AdaptiveRK) (used by relax with the LLG driver).
 int orc_dopri_advance(void* h, double* stats) {
   Sim* s = static_cast<Sim*>(h);

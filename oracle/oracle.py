@@ -43,6 +43,7 @@ def lib():
         L.orc_set_Ms.argtypes = [vp, _dp]
         L.orc_set_m.argtypes = [vp, _dp]
         L.orc_get_m.argtypes = [vp, _dp]
+        L.orc_get_y_current.argtypes = [vp, _dp]
         L.orc_set_pins.argtypes = [vp, ctypes.POINTER(ctypes.c_uint8)]
         L.orc_set_llg.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int]
         L.orc_add_zeeman.argtypes = [vp, _dp]
@@ -253,6 +254,12 @@ class OracleSim:
         st = np.zeros(6)
         ok = lib().orc_run_until(self.h, float(t_end), _ptr(st))
         return ok, dict(t=st[0], step=st[1], step_next=st[2], nsteps=int(st[3]), nfevals=int(st[4]), attempts=int(st[5]))
+
+    def get_y_current(self):
+        """The adaptive stepper's state (integrator.y_current)."""
+        out = np.zeros(3 * self.n)
+        lib().orc_get_y_current(self.h, _ptr(out))
+        return out
 
     def dopri_advance(self):
         st = np.zeros(6)

@@ -128,7 +128,9 @@ def test_c2_dormand_prince_step():
     assert ok and sg["nsteps"] == so["nsteps"] == 1
     assert abs(sg["step"] - so["step"]) <= 1e-12 * so["step"]
     assert abs(sg["t"] - so["t"]) <= 1e-12 * so["t"]
-    assert rel_maxnorm(h.get_m(), o.get_m()) <= TOL_STEPS
+    # advance_step leaves sim.spin alone (adaptive_rk.jl:93-148): the state is
+    # the integrator's y_current
+    assert rel_maxnorm(h.get_m(), o.get_y_current()) <= TOL_STEPS
     h.close()
 
 
@@ -172,7 +174,7 @@ def test_c4_adjoint_mesh_fields():
 def test_c5_column_major_full_size():
     """1024x1024x16 at 3 nm: column-major spectra of the padded
     2048x2048x32 grid at full size; H_eff, dm/dt and one RK4 step."""
-    _check_workload("c5", steps=(1,), form32=False)
+    _check_workload("c5", steps=(1,), form32=True)
 
 
 def _film_handle(s, form):

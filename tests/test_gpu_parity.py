@@ -458,3 +458,41 @@ def test_fp32_form_rk4_random_state_short_horizon():
     g64.rk4(1e-14, 50)
     g32.rk4(1e-14, 50)
     assert rel_maxnorm(g32.m(), g64.m()) <= TOL32
+
+
+@pytest.mark.parametrize("mesh", [(128, 128, 16), (256, 128, 16), (128, 512, 16), (512, 256, 16), (1024, 128, 16),
+                                  (128, 1024, 16), (256, 256, 64)])
+def test_register_passes_fp32(mesh):
+    """FP32 power-of-two meshes (nx, ny = 128 .. 1024, nz = 16 or 64) run the
+    register-resident x and y passes (every lane group size Q = 4 .. 32) and,
+    for nz = 16, the register-resident z convolution: the demag field and
+    H_eff against the FP64 form of the same mesh, two RK4 steps against the
+    oracle."""
+    from oracle.oracle import demag_tensor
+
+    nx, ny, nz = mesh
+    cfg = random_config(41 + nx + ny + nz, nx, ny, nz, "", terms=("exch", "demag"), spatial=False)
+    T = demag_tensor(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    g64 = GpuSim(cfg, form=0, tensor=T)
+    g32 = GpuSim(cfg, form=1, tensor=T)
+    assert rel_maxnorm(g32.term_field("demag")[0], g64.term_field("demag")[0]) <= TOL32
+    assert rel_maxnorm(g32.field(), g64.field()) <= TOL32
+    o, _ = build_oracle(cfg, tensor=T)
+    o.rk4(2e-14, 2)
+    g32.rk4(2e-14, 2)
+    assert rel_maxnorm(g32.m(), o.get_m()) <= TOL32
+
+
+@pytest.mark.parametrize("mesh", [(100, 60, 16), (40, 900, 16)])
+def test_zpair_layouts_fp32(mesh):
+    """Pz = 32 (nz = 16) on meshes outside the register x / y passes: the
+    register-resident z convolution on row-major spectra (100 x 60) and on
+    column-major spectra (padded y = 1800): demag field against FP64."""
+    from oracle.oracle import demag_tensor
+
+    nx, ny, nz = mesh
+    cfg = random_config(43 + nx + ny, nx, ny, nz, "", terms=("demag",))
+    T = demag_tensor(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    f64 = GpuSim(cfg, form=0, tensor=T).term_field("demag")[0]
+    f32 = GpuSim(cfg, form=1, tensor=T).term_field("demag")[0]
+    assert rel_maxnorm(f32, f64) <= TOL32

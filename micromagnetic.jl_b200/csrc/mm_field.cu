@@ -125,9 +125,19 @@ void launch_nbmask(int nx, int ny, int nz, int pbc, const R* Ms, uint8_t* nbm, c
 // kernels of src/micro/kernels.jl (zeeman 14-20, anisotropy 54-75, exchange
 // 226-304, bulk DMI 306-344, interfacial DMI 426-466) and the demag energy of
 // src/micro/demag.jl:435-456; terms with Ms == 0 contribute nothing.
-template <typename R, bool ENERGY, bool EXTRA = false>
+// The cell and its six neighbours from a shared-memory halo tile instead of
+// global memory: component c of the cell at p[c*cs + c0], the x neighbours
+// at c0 -+ 1, the y neighbours at c0 -+ sx, the z neighbours at c0 + dm and
+// c0 + dp (the tile's planes k-1 and k+1).  Tile cells of absent neighbours
+// are never read: their mask bit drops the term.
+template <typename R> struct TileNb {
+  const R* p;
+  int cs, c0, sx, dm, dp;
+};
+
+template <typename R, bool ENERGY, bool EXTRA = false, bool TILE = false>
 __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __restrict__ y, int I, int i, int j,
-                                          int k, R m[3], R h[3], double* e) {
+                                          int k, R m[3], R h[3], double* e, const TileNb<R>& tn = TileNb<R>{}) {
   const int64_t N = a.N;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int nxy = nx * ny;
@@ -145,19 +155,32 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
   nb[3] = j < ny - 1 ? I + nx : (py ? I - (ny - 1) * nx : I);
   nb[4] = k > 0 ? I - nxy : (pz ? I + (nz - 1) * nxy : I);
   nb[5] = k < nz - 1 ? I + nxy : (pz ? I - (nz - 1) * nxy : I);
-  m[0] = y[I];
-  m[1] = y[N + I];
-  m[2] = y[2 * N + I];
+  if constexpr (TILE) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) m[c] = tn.p[c * tn.cs + tn.c0];
+  } else {
+    m[0] = y[I];
+    m[1] = y[N + I];
+    m[2] = y[2 * N + I];
+  }
   const R Ms = a.Ms[I];
   unsigned nbm = 0;
   R mn[6][3];
   if (local) {
     nbm = a.nbm[I];
+    if constexpr (TILE) {
+      const int off[6] = {-1, 1, -tn.sx, tn.sx, tn.dm, tn.dp};
 #pragma unroll
-    for (int d = 0; d < 6; ++d) {
-      mn[d][0] = __ldg(y + nb[d]);
-      mn[d][1] = __ldg(y + N + nb[d]);
-      mn[d][2] = __ldg(y + 2 * N + nb[d]);
+      for (int d = 0; d < 6; ++d)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) mn[d][c] = tn.p[c * tn.cs + tn.c0 + off[d]];
+    } else {
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        mn[d][0] = __ldg(y + nb[d]);
+        mn[d][1] = __ldg(y + N + nb[d]);
+        mn[d][2] = __ldg(y + 2 * N + nb[d]);
+      }
     }
   }
   R An[6] = {R(0), R(0), R(0), R(0), R(0), R(0)}, AI = R(0);
@@ -419,6 +442,93 @@ __constant__ RkTableau c_rk[RK_NMETHODS] = MM_RK_TABLES;
 static const RkTableau h_rk[RK_NMETHODS] = MM_RK_TABLES;
 const RkTableau& rk_tableau(int method) { return h_rk[method]; }
 
+// The RK4 / Heun stage update of one cell from its field h at the stage input
+// m: advance_step(::RungeKutta) src/integrator/rk.jl:23-52 and
+// advance_step(::ModifiedEuler) src/integrator/heun.jl:28-49.  mN, mL: the
+// step's start state (hi, lo); av: the accumulator.
+template <typename R>
+__device__ __forceinline__ void rk4_update(const FieldArgs<R>& a, const StageArgs<R>& s, int I, const R m[3],
+                                           const R h[3], const R mN[3], const R mL[3], const R av[3]) {
+  constexpr bool kF32 = sizeof(R) == 4;
+  const int64_t N = a.N;
+  if (s.scheme == 1) {
+    // advance_step(::ModifiedEuler)  src/integrator/heun.jl:28-49:
+    // k1 = f(m); y = m + h k1; k2 = f(y); m = normalise(m + (h/2) k1 + (h/2) k2)
+    R f[3];
+    llg_rhs(a, I, m, h, f);
+    if (s.stage == 1) {
+      const R hh = static_cast<R>(s.h);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        s.acc[c * N + I] = f[c];
+        s.ynext[c * N + I] = kF32 ? mN[c] + (mL[c] + hh * f[c]) : mN[c] + hh * f[c];
+      }
+    } else {
+      const R h2 = static_cast<R>(0.5 * s.h);
+      R mv[3];
+      if constexpr (kF32) {
+        float lo[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          mv[c] = mN[c];
+          lo[c] = mL[c];
+          df_add(mv[c], lo[c], h2 * av[c] + h2 * f[c]);
+        }
+        df_normalise(mv, lo);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s.m_lo[c * N + I] = lo[c];
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) mv[c] = mN[c] + h2 * av[c] + h2 * f[c];
+        plain_normalise(mv);
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s.m[c * N + I] = mv[c];
+    }
+  } else {
+    // advance_step(::RungeKutta)  src/integrator/rk.jl:23-52
+    R f[3];
+    llg_rhs(a, I, m, h, f);
+    const int st = s.stage;
+    if (st < 4) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const R kc = f[c];
+        s.acc[c * N + I] = st == 1 ? kc : av[c] + 2 * kc;
+      }
+      const R cf = static_cast<R>(st == 3 ? s.h : 0.5 * s.h);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        R v;
+        if (kF32) v = mN[c] + (mL[c] + cf * f[c]);
+        else v = mN[c] + cf * f[c];
+        s.ynext[c * N + I] = v;
+      }
+    } else {
+      const R c6 = static_cast<R>(1.0 / 6 * s.h);
+      R mv[3];
+      if constexpr (kF32) {
+        float lo[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          mv[c] = mN[c];
+          lo[c] = mL[c];
+          df_add(mv[c], lo[c], c6 * (av[c] + f[c]));
+        }
+        df_normalise(mv, lo);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s.m_lo[c * N + I] = lo[c];
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) mv[c] = mN[c] + c6 * (av[c] + f[c]);
+        plain_normalise(mv);
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s.m[c * N + I] = mv[c];
+    }
+  }
+}
+
 template <typename R, int MODE, bool EXTRA>
 __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage(FieldArgs<R> a, const R* __restrict__ y, StageArgs<R> s) {
   constexpr bool kF32 = sizeof(R) == 4;
@@ -464,81 +574,8 @@ __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage
       s.out[I] = f[0];
       s.out[N + I] = f[1];
       s.out[2 * N + I] = f[2];
-    } else if (MODE == SM_RK4 && s.scheme == 1) {
-      // advance_step(::ModifiedEuler)  src/integrator/heun.jl:28-49:
-      // k1 = f(m); y = m + h k1; k2 = f(y); m = normalise(m + (h/2) k1 + (h/2) k2)
-      R f[3];
-      llg_rhs(a, I, m, h, f);
-      if (s.stage == 1) {
-        const R hh = static_cast<R>(s.h);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          s.acc[c * N + I] = f[c];
-          s.ynext[c * N + I] = kF32 ? mN[c] + (mL[c] + hh * f[c]) : mN[c] + hh * f[c];
-        }
-      } else {
-        const R h2 = static_cast<R>(0.5 * s.h);
-        R mv[3];
-        if constexpr (kF32) {
-          float lo[3];
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            mv[c] = mN[c];
-            lo[c] = mL[c];
-            df_add(mv[c], lo[c], h2 * av[c] + h2 * f[c]);
-          }
-          df_normalise(mv, lo);
-#pragma unroll
-          for (int c = 0; c < 3; ++c) s.m_lo[c * N + I] = lo[c];
-        } else {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) mv[c] = mN[c] + h2 * av[c] + h2 * f[c];
-          plain_normalise(mv);
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) s.m[c * N + I] = mv[c];
-      }
     } else if (MODE == SM_RK4) {
-      // advance_step(::RungeKutta)  src/integrator/rk.jl:23-52
-      R f[3];
-      llg_rhs(a, I, m, h, f);
-      const int st = s.stage;
-      if (st < 4) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const R kc = f[c];
-          s.acc[c * N + I] = st == 1 ? kc : av[c] + 2 * kc;
-        }
-        const R cf = static_cast<R>(st == 3 ? s.h : 0.5 * s.h);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          R v;
-          if (kF32) v = mN[c] + (mL[c] + cf * f[c]);
-          else v = mN[c] + cf * f[c];
-          s.ynext[c * N + I] = v;
-        }
-      } else {
-        const R c6 = static_cast<R>(1.0 / 6 * s.h);
-        R mv[3];
-        if constexpr (kF32) {
-          float lo[3];
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            mv[c] = mN[c];
-            lo[c] = mL[c];
-            df_add(mv[c], lo[c], c6 * (av[c] + f[c]));
-          }
-          df_normalise(mv, lo);
-#pragma unroll
-          for (int c = 0; c < 3; ++c) s.m_lo[c * N + I] = lo[c];
-        } else {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) mv[c] = mN[c] + c6 * (av[c] + f[c]);
-          plain_normalise(mv);
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) s.m[c * N + I] = mv[c];
-      }
+      rk4_update(a, s, I, m, h, mN, mL, av);
     } else if (MODE == SM_DOPRI) {
       // rk_step_bs23! / rk_step_dopri54! / rk_step_cashkarp54! /
       // rk_step_fehlberg54!  src/integrator/adaptive_rk_steps.jl:11-229
@@ -662,6 +699,85 @@ __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage
   }
 }
 
+// RK4 / Heun stage on halo tiles (handles without the further terms): a
+// block of BX x BY threads walks kStageTileZ consecutive z planes of its
+// BX x BY column, keeping the planes k-1, k, k+1 of the stage input as
+// (BX+2) x (BY+2) tiles in shared memory (a rolling window of three; each
+// plane is loaded once per block, with coalesced row segments), so the six
+// neighbours of every cell come from shared memory.  Same arithmetic as
+// k_stage.
+constexpr int kStageTileZ = 8;
+
+template <typename R>
+__global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2)
+    k_stage_tile(FieldArgs<R> a, const R* __restrict__ y, StageArgs<R> s) {
+  constexpr bool kF32 = sizeof(R) == 4;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  R* T = reinterpret_cast<R*>(smraw);
+  const int bx = blockDim.x, by = blockDim.y, TX = bx + 2, TY = by + 2, TP = TX * TY;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int64_t N = a.N;
+  const bool px = a.pbc & 1, py = a.pbc & 2, pz = a.pbc & 4;
+  const int i0 = blockIdx.x * bx, j0 = blockIdx.y * by, k0 = blockIdx.z * kStageTileZ;
+  const int k1 = min(nz, k0 + kStageTileZ);
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * bx + tx, nth = bx * by;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool live = i < nx && j < ny;
+  auto slot = [](int p) { return (p + 3) % 3; };
+  // plane p (-1 <= p <= nz) of the stage input into its slot; cells outside
+  // the mesh (and not wrapped by periodic boundaries) are zero
+  auto load_plane = [&](int p) {
+    R* dst = T + slot(p) * 3 * TP;
+    int pk = p;
+    if (pk < 0 || pk >= nz) pk = pz ? (pk < 0 ? pk + nz : pk - nz) : -1;
+    for (int e = tid; e < TP; e += nth) {
+      const int hy = e / TX, hx = e - hy * TX;
+      int gi = i0 + hx - 1, gj = j0 + hy - 1;
+      if (gi == -1 && px) gi = nx - 1;
+      else if (gi == nx && px) gi = 0;
+      if (gj == -1 && py) gj = ny - 1;
+      else if (gj == ny && py) gj = 0;
+      const bool ok = pk >= 0 && gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+      const int64_t g = ok ? (static_cast<int64_t>(pk) * ny + gj) * nx + gi : 0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) dst[c * TP + e] = ok ? y[c * N + g] : R(0);
+    }
+  };
+  load_plane(k0 - 1);
+  load_plane(k0);
+  for (int k = k0; k < k1; ++k) {
+    load_plane(k + 1);
+    const int I = (k * ny + j) * nx + i;
+    R mN[3], mL[3], av[3];
+    if (live) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        mN[c] = s.m[c * N + I];
+        mL[c] = kF32 ? s.m_lo[c * N + I] : R(0);
+        av[c] = s.stage > 1 ? s.acc[c * N + I] : R(0);
+      }
+    }
+    __syncthreads();
+    if (live) {
+      const int sk = slot(k) * 3 * TP;
+      TileNb<R> tn{T + sk, TP, (ty + 1) * TX + tx + 1, TX, slot(k - 1) * 3 * TP - sk, slot(k + 1) * 3 * TP - sk};
+      R m[3], h[3];
+      cell_heff<R, false, false, true>(a, y, I, i, j, k, m, h, nullptr, tn);
+      rk4_update(a, s, I, m, h, mN, mL, av);
+    }
+    __syncthreads();  // before plane k + 2 replaces plane k - 1
+  }
+}
+
+// halo-tiled RK4 / Heun stages unless MMCUDA_STAGETILE=0
+static bool stage_tile_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MMCUDA_STAGETILE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 template <typename R>
 void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<R>& sa, cudaStream_t st) {
   const StageGrid g = stage_grid(fa.nx, fa.ny, fa.nz);
@@ -674,6 +790,12 @@ void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<
       case SM_ENERGY: k_stage<R, SM_ENERGY, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
       default: k_stage<R, SM_DOPRI, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
     }
+    return;
+  }
+  const size_t tsm = 3 * 3 * static_cast<size_t>(g.block.x + 2) * (g.block.y + 2) * sizeof(R);
+  if (mode == SM_RK4 && stage_tile_enabled() && tsm <= 48 * 1024) {
+    const dim3 grid(g.grid.x, g.grid.y, (fa.nz + kStageTileZ - 1) / kStageTileZ);
+    k_stage_tile<R><<<grid, g.block, tsm, st>>>(fa, y, sa);
     return;
   }
   switch (mode) {

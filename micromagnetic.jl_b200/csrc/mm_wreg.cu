@@ -29,14 +29,23 @@ constexpr int kWyNT = 256;  // y passes: 8 warps, 4 lines x 2 halves (Q = 32)
 
 // rows of one x-pass block: 4 warps x (32 / Q) groups
 template <int Q> constexpr int x_rows() { return 4 * (32 / Q); }
+// Staging stride (complex values between consecutive k of the block's RB
+// rows): lanes of a half warp touch 16 distinct 8-byte banks, i.e. the stride
+// is odd for Q >= 16 (one group of 16 lanes) and 2 or 4 mod 16 for Q = 8 or 4
+// (lane groups side by side).
+template <int Q> constexpr int x_stride() { return x_rows<Q>() + (x_rows<Q>() >= 8 ? x_rows<Q>() / 8 : 1); }
+// shared memory of an x-pass block: the transpose tiles or the staged rows
+template <int Q> constexpr int x_smem() {
+  return 4 * wtile_size<Q>() > (32 * Q + 1) * x_stride<Q>() ? 4 * wtile_size<Q>() : (32 * Q + 1) * x_stride<Q>();
+}
 
 // ---------------------------------------------------------------- x forward
 // Rows of m * mu0Ms (zero padded to Px = 2 Lc) -> X column-major.
 template <int Q>
 __global__ void __launch_bounds__(kWrNT) k_xfwd_w(const float* __restrict__ m, const float* __restrict__ Ms,
                                                  float2* __restrict__ X, DemagGeom g, const float2* __restrict__ twx) {
-  constexpr int RB = x_rows<Q>(), L = 32 * Q;
-  __shared__ __align__(16) float2 sm[4 * wtile_size<Q>()];
+  constexpr int RB = x_rows<Q>(), L = 32 * Q, S = x_stride<Q>();
+  __shared__ __align__(16) float2 sm[x_smem<Q>()];
   if (g.gate && !*g.gate) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gq = lane / Q, q = lane % Q;
@@ -61,13 +70,13 @@ __global__ void __launch_bounds__(kWrNT) k_xfwd_w(const float* __restrict__ m, c
   wfft<Q, false, 2>(v, sm + warp * wtile_size<Q>(), twx);
   __syncthreads();  // every warp is done with its transpose tile
 #pragma unroll
-  for (int r = 0; r < 32; ++r) sm[(q + Q * (r / Q) + 32 * (r % Q)) * RB + rl] = v[r];
+  for (int r = 0; r < 32; ++r) sm[(q + Q * (r / Q) + 32 * (r % Q)) * S + rl] = v[r];
   __syncthreads();
   // X[k] = E + w_Px^k O, E = (Z[k] + conj Z[Lc-k]) / 2, O = (Z[k] - conj Z[Lc-k]) / 2i
   for (int e = threadIdx.x; e < Hx * RB; e += kWrNT) {
     const int k = e / RB, r = e - k * RB;
-    const float2 zk = sm[(k == L ? 0 : k) * RB + r];
-    float2 zc = sm[(k == 0 ? 0 : L - k) * RB + r];
+    const float2 zk = sm[(k == L ? 0 : k) * S + r];
+    float2 zc = sm[(k == 0 ? 0 : L - k) * S + r];
     zc.y = -zc.y;
     const float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
     const float2 od = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
@@ -80,8 +89,8 @@ __global__ void __launch_bounds__(kWrNT) k_xfwd_w(const float* __restrict__ m, c
 template <int Q>
 __global__ void __launch_bounds__(kWrNT) k_xinv_w(const float2* __restrict__ X, float* __restrict__ H, DemagGeom g,
                                                  const float2* __restrict__ twx) {
-  constexpr int RB = x_rows<Q>(), L = 32 * Q;
-  __shared__ __align__(16) float2 sm[4 * wtile_size<Q>()];
+  constexpr int RB = x_rows<Q>(), L = 32 * Q, S = x_stride<Q>();
+  __shared__ __align__(16) float2 sm[x_smem<Q>()];
   if (g.gate && !*g.gate) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gq = lane / Q, q = lane % Q;
@@ -92,7 +101,7 @@ __global__ void __launch_bounds__(kWrNT) k_xinv_w(const float2* __restrict__ X, 
   const int rl = warp * (32 / Q) + gq;
   for (int e = threadIdx.x; e < Hx * RB; e += kWrNT) {
     const int k = e / RB, r = e - k * RB;
-    sm[e] = X[(static_cast<int64_t>(c) * Hx + k) * rows + row0 + r];
+    sm[k * S + r] = X[(static_cast<int64_t>(c) * Hx + k) * rows + row0 + r];
   }
   __syncthreads();
   // Z'[k] = (A + B) + i (A - B) conj(w_Px^k), A = X[k], B = conj X[Lc - k]
@@ -100,8 +109,8 @@ __global__ void __launch_bounds__(kWrNT) k_xinv_w(const float2* __restrict__ X, 
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     const int k = q + Q * j;
-    const float2 a = sm[k * RB + rl];
-    float2 b = sm[(L - k) * RB + rl];
+    const float2 a = sm[k * S + rl];
+    float2 b = sm[(L - k) * S + rl];
     b.y = -b.y;
     float2 w = __ldg(twx + k);
     w.y = -w.y;
@@ -122,7 +131,7 @@ __global__ void __launch_bounds__(kWrNT) k_xinv_w(const float2* __restrict__ X, 
 // X column (ny values) -> Y column (Py = 2 ny values); line = (c Hx + kx) nz + z.
 // Unit u = group in the block: line (u >> 1), half s = u & 1.
 template <int Q>
-__global__ void __launch_bounds__(kWyNT) k_yfwd_w(const float2* __restrict__ X, float2* __restrict__ Y, DemagGeom g,
+__global__ void __launch_bounds__(kWyNT, 3) k_yfwd_w(const float2* __restrict__ X, float2* __restrict__ Y, DemagGeom g,
                                                  const float2* __restrict__ twy, int nlines) {
   constexpr int NL = 4 * (32 / Q), Py = 64 * Q;  // lines a block, padded length
   extern __shared__ __align__(16) float2 smy[];
@@ -143,20 +152,24 @@ __global__ void __launch_bounds__(kWyNT) k_yfwd_w(const float2* __restrict__ X, 
   }
   wfft<Q, false, 2>(v, smy + warp * wtile_size<Q>(), twy);
   __syncthreads();  // transposes done: the tiles become the block's output columns
-  float2* col = smy + ll * Py;
+  // Y[2k + s] of line ll staged as half column (ll, s), k contiguous
+  float2* half = smy + (2 * ll + s) * (Py / 2);
 #pragma unroll
-  for (int r = 0; r < 32; ++r) col[2 * (q + Q * (r / Q) + 32 * (r % Q)) + s] = v[r];
+  for (int r = 0; r < 32; ++r) half[q + Q * (r / Q) + 32 * (r % Q)] = v[r];
   __syncthreads();
   const int nl = min(NL, nlines - line0);
-  const float4* src = reinterpret_cast<const float4*>(smy);
   float4* dst = reinterpret_cast<float4*>(Y + static_cast<int64_t>(line0) * Py);
-  for (int e = threadIdx.x; e < nl * Py / 2; e += kWyNT) dst[e] = src[e];
+  for (int e = threadIdx.x; e < nl * Py / 2; e += kWyNT) {
+    const int l = e / (Py / 2), k = e - l * (Py / 2);
+    const float2 a = smy[(2 * l) * (Py / 2) + k], b = smy[(2 * l + 1) * (Py / 2) + k];
+    dst[e] = make_float4(a.x, a.y, b.x, b.y);
+  }
 }
 
 // ---------------------------------------------------------------- y inverse
 // Y column (Py values) -> X column (y < ny).
 template <int Q>
-__global__ void __launch_bounds__(kWyNT) k_yinv_w(const float2* __restrict__ Y, float2* __restrict__ X, DemagGeom g,
+__global__ void __launch_bounds__(kWyNT, 3) k_yinv_w(const float2* __restrict__ Y, float2* __restrict__ X, DemagGeom g,
                                                  const float2* __restrict__ twy, int nlines) {
   constexpr int NL = 4 * (32 / Q), Py = 64 * Q, ny = 32 * Q;
   extern __shared__ __align__(16) float2 smy[];
@@ -167,15 +180,20 @@ __global__ void __launch_bounds__(kWyNT) k_yinv_w(const float2* __restrict__ Y, 
   const int line0 = blockIdx.x * NL;
   const int nl = min(NL, nlines - line0);
   {
+    // Y[2k + s] of line l staged as half column (l, s), k contiguous
     const float4* src = reinterpret_cast<const float4*>(Y + static_cast<int64_t>(line0) * Py);
-    float4* dst = reinterpret_cast<float4*>(smy);
-    for (int e = threadIdx.x; e < nl * Py / 2; e += kWyNT) dst[e] = src[e];
+    for (int e = threadIdx.x; e < nl * Py / 2; e += kWyNT) {
+      const int l = e / (Py / 2), k = e - l * (Py / 2);
+      const float4 p = src[e];
+      smy[(2 * l) * (Py / 2) + k] = make_float2(p.x, p.y);
+      smy[(2 * l + 1) * (Py / 2) + k] = make_float2(p.z, p.w);
+    }
   }
   __syncthreads();
   float2 v[32];
-  const float2* col = smy + ll * Py;
+  const float2* col = smy + (2 * ll + s) * (Py / 2);
 #pragma unroll
-  for (int j = 0; j < 32; ++j) v[j] = ll < nl ? col[2 * (q + Q * j) + s] : make_float2(0.f, 0.f);
+  for (int j = 0; j < 32; ++j) v[j] = ll < nl ? col[q + Q * j] : make_float2(0.f, 0.f);
   __syncthreads();  // the staged columns become the transpose tiles
   wfft<Q, true, 2>(v, smy + warp * wtile_size<Q>(), twy);
   if (s) {

@@ -255,9 +255,11 @@ def run_batch(args, rank, ws, device, dist):
         if dist is not None:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
+        launches, merged = b.launches()
         out[fname] = {"value": total * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
                       "instances": len(batch_specs(wname)), "cells": total, "rank0_instances": len(handles),
-                      "launches_per_step": sum(h.rk4_launches() for h in handles)}
+                      "launches_per_step": launches, "merged_instances": merged,
+                      "launches_per_step_unmerged": sum(h.rk4_launches() for h in handles)}
         b.close()
         for h in handles:
             h.close()
@@ -267,7 +269,8 @@ def run_batch(args, rank, ws, device, dist):
                 "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
                 "dtype": "f32" if "fp32" in out else "f64", "data": "synthetic (seeded numpy PCG64)",
-                "config": {"workload": f"{wname}: {r['instances']} meshes, {r['cells']} cells, one graph per step",
+                "config": {"workload": f"{wname}: {r['instances']} meshes, {r['cells']} cells, one graph per step, "
+                                       f"{r['launches_per_step']} launches per step",
                            "parallelism": f"meshes partitioned over {ws} rank(s) by FFT cost, no collective"},
                 "forms": out}
         print(json.dumps(line), flush=True)

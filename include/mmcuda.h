@@ -275,8 +275,11 @@ int mm_rk4_launches_per_step(mm_handle* h, int* launches);
 
 /* ---- batches: several meshes (ensembles, NEB images) stepped together ----
  * The reference evaluates NEB images one after another (src/neb/neb.jl:220-232).
- * A batch captures one RK4 step of every handle (same device, same dt) as
- * parallel branches of one CUDA graph and replays it once per step; work
+ * A batch captures one RK4 step of every handle (same device, same dt) in one
+ * CUDA graph and replays it once per step: the demag passes and stage
+ * kernels of meshes that take the shared-memory FFT paths are launched once
+ * per pass for all of them (mm_batch_launches), other meshes run as parallel
+ * branches of the graph; work
  * queued on the handles before mm_batch_rk4_run precedes the batch and work
  * queued after it follows.  The handles stay owned by the caller and must
  * outlive the batch. */
@@ -284,6 +287,13 @@ typedef struct mm_batch mm_batch;
 int mm_batch_create(mm_handle* const* handles, int n, mm_batch** out);
 int mm_batch_rk4_run(mm_batch* b, double dt, int64_t nsteps);
 int mm_batch_get_stream(mm_batch* b, void** stream);
+/* Measurement hook (no reference counterpart): kernel launches of one batched
+ * RK4 step and the number of handles whose passes were merged into shared
+ * launches (each pass kernel launched once for all of them, its blocks
+ * looking their mesh up); valid after the first mm_batch_rk4_run.  The other
+ * handles run as parallel graph branches.  MMCUDA_BATCH_MERGE=0 disables the
+ * merging. */
+int mm_batch_launches(mm_batch* b, int* launches_per_step, int* merged_handles);
 int mm_batch_destroy(mm_batch* b);
 
 /* ---- energies without device allocation ----------------------------------

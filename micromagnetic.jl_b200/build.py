@@ -19,7 +19,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin", "g++",
+FLAGS = ["-O3", "-std=c++20", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin", "g++",
          "--expt-relaxed-constexpr", "-I", CSRC, "-I", INCLUDE]
 
 
@@ -47,13 +47,24 @@ def _compile(src, verbose):
     return obj, r.stderr
 
 
+def _stale(src):
+    """The object of src is missing or older than src or any header."""
+    obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+    if not os.path.exists(obj):
+        return True
+    hdrs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    hdrs.append(os.path.join(INCLUDE, "mmcuda.h"))
+    return os.path.getmtime(obj) < max(os.path.getmtime(f) for f in [src] + hdrs)
+
+
 def build(force=False, jobs=4, verbose=False):
     if not force and not needs_build():
         return LIB
     os.makedirs(OBJ_DIR, exist_ok=True)
+    todo = [s for s in sources() if force or verbose or _stale(s)]
     with concurrent.futures.ThreadPoolExecutor(max_workers=jobs) as ex:
-        results = list(ex.map(lambda s: _compile(s, verbose), sources()))
-    objs = [o for o, _ in results]
+        results = list(ex.map(lambda s: _compile(s, verbose), todo))
+    objs = [os.path.join(OBJ_DIR, os.path.basename(s) + ".o") for s in sources()]
     if verbose:
         for _, log in results:
             sys.stderr.write(log)

@@ -16,6 +16,7 @@
 
 #include "../../include/mmcuda.h"
 #include "mm_demag.cuh"
+#include "mm_launch.cuh"
 #include "mm_field.cuh"
 #include "mm_integ.cuh"
 
@@ -109,6 +110,8 @@ class EngineBase {
   // step counters advanced after a batch ran n steps
   virtual int rk4_prepare() = 0;
   virtual void rk4_enqueue(double dt) = 0;
+  // every launch of rk4_enqueue is a descriptor kernel (mm_launch.cuh)
+  virtual bool rk4_batchable() const = 0;
   virtual void rk4_count(int64_t n, double dt) = 0;
   virtual uint64_t params_version() const = 0;
   virtual cudaStream_t stream() const = 0;
@@ -733,6 +736,11 @@ class Engine : public EngineBase {
     return MM_OK;
   }
   void rk4_enqueue(double dt) override { enqueue_rk4_step(dt); }
+  bool rk4_batchable() const override {
+    if (mask & TB_THERMAL) return false;
+    if (!stage_descriptor_used<R>(fargs(~0u))) return false;
+    return !((mask & TB_DEMAG) && demag) || demag->batchable();
+  }
   void rk4_count(int64_t n, double dt) override {
     rk_n += n;
     rk_t = static_cast<double>(rk_n) * dt;
@@ -1350,6 +1358,11 @@ struct mm_handle {
 // A set of handles on one device stepped together: one RK4 step of every
 // instance is captured as parallel branches (fork/join over the handles' own
 // streams) of a single CUDA graph, launched once per step on the batch stream.
+// Handles whose RK4 step launches descriptor kernels only are merged pass by
+// pass: their steps are recorded (mm_launch.cuh) and the records of the same
+// kernel across meshes become one launch over all of them (blocks look their
+// mesh up), scheduled so that each mesh keeps its own order.  Other handles
+// run as parallel branches of the same graph.
 struct mm_batch {
   std::vector<mm_handle*> hs;
   int device = 0;
@@ -1359,9 +1372,13 @@ struct mm_batch {
   cudaGraphExec_t graph = nullptr;
   double dt = 0.0;
   std::vector<uint64_t> versions;
+  void* merged_args = nullptr;  // device: per merged launch, the meshes' Args and block offsets
+  int launches = 0;             // kernel launches of one step
+  int merged = 0;               // handles in the merged launches
   ~mm_batch() {
     cudaSetDevice(device);
     if (graph) cudaGraphExecDestroy(graph);
+    if (merged_args) cudaFree(merged_args);
     for (cudaEvent_t e : joins) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
     if (done) cudaEventDestroy(done);
@@ -1370,6 +1387,15 @@ struct mm_batch {
 };
 
 using mm::fail;
+
+// merged pass launches in batches unless MMCUDA_BATCH_MERGE=0
+static bool batch_merge_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MMCUDA_BATCH_MERGE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
 
 #define MM_HANDLE(h)                                                          \
   do {                                                                        \
@@ -1624,6 +1650,13 @@ int mm_batch_create(mm_handle* const* handles, int n, mm_batch** out) {
   return MM_OK;
 }
 
+int mm_batch_launches(mm_batch* b, int* launches_per_step, int* merged_handles) {
+  if (!b) return fail(MM_ERR_ARG, "null batch");
+  if (launches_per_step) *launches_per_step = b->launches;
+  if (merged_handles) *merged_handles = b->merged;
+  return MM_OK;
+}
+
 int mm_batch_destroy(mm_batch* b) {
   delete b;
   return MM_OK;
@@ -1653,17 +1686,101 @@ int mm_batch_rk4_run(mm_batch* b, double dt, int64_t nsteps) {
     if (stale) {
       if (b->graph) cudaGraphExecDestroy(b->graph);
       b->graph = nullptr;
+      if (b->merged_args) cudaFree(b->merged_args);
+      b->merged_args = nullptr;
+      // record the steps of the handles whose launches can be merged
+      std::vector<int> rec_h, branch_h;
+      for (int i = 0; i < n; ++i)
+        (batch_merge_enabled() && b->hs[i]->eng->rk4_batchable() ? rec_h : branch_h).push_back(i);
+      if (rec_h.size() < 2) {
+        branch_h.insert(branch_h.end(), rec_h.begin(), rec_h.end());
+        rec_h.clear();
+      }
+      std::vector<std::vector<mm::LaunchRec>> recs(rec_h.size());
+      for (size_t j = 0; j < rec_h.size(); ++j) {
+        mm::LaunchRecorder rec;
+        mm::launch_recorder() = &rec;
+        b->hs[rec_h[j]]->eng->rk4_enqueue(dt);
+        mm::launch_recorder() = nullptr;
+        recs[j] = std::move(rec.recs);
+      }
+      // greedy merge: the kernel that is next for the most meshes launches
+      // for all of them; every mesh's records stay in order
+      struct Merged {
+        const mm::LaunchRec* first;
+        std::vector<const mm::LaunchRec*> parts;
+        int blocks = 0;
+        size_t smem = 0, off_args = 0, off_begins = 0;
+      };
+      std::vector<Merged> plan;
+      std::vector<size_t> next(recs.size(), 0);
+      for (;;) {
+        std::vector<std::pair<const void*, int>> cnt;
+        for (size_t j = 0; j < recs.size(); ++j) {
+          if (next[j] >= recs[j].size()) continue;
+          const void* k = recs[j][next[j]].kind;
+          auto it = std::find_if(cnt.begin(), cnt.end(), [&](const auto& p) { return p.first == k; });
+          if (it == cnt.end()) cnt.push_back({k, 1});
+          else ++it->second;
+        }
+        if (cnt.empty()) break;
+        const void* kind = std::max_element(cnt.begin(), cnt.end(),
+                                            [](const auto& a, const auto& c) { return a.second < c.second; })->first;
+        Merged mg;
+        mg.first = nullptr;
+        for (size_t j = 0; j < recs.size(); ++j) {
+          if (next[j] >= recs[j].size() || recs[j][next[j]].kind != kind) continue;
+          const mm::LaunchRec* r = &recs[j][next[j]++];
+          if (!mg.first) mg.first = r;
+          mg.parts.push_back(r);
+          mg.blocks += r->blocks;
+          mg.smem = std::max(mg.smem, r->smem);
+        }
+        plan.push_back(std::move(mg));
+      }
+      // one device buffer: per merged launch its Args array and block offsets
+      size_t bytes = 0;
+      for (Merged& mg : plan) {
+        mg.off_args = bytes;
+        bytes += (mg.first->args_size * mg.parts.size() + 255) / 256 * 256;
+        mg.off_begins = bytes;
+        bytes += (sizeof(int) * mg.parts.size() + 255) / 256 * 256;
+      }
+      if (bytes) {
+        std::vector<unsigned char> host(bytes, 0);
+        for (Merged& mg : plan) {
+          int beg = 0;
+          for (size_t q = 0; q < mg.parts.size(); ++q) {
+            std::memcpy(host.data() + mg.off_args + q * mg.first->args_size, mg.parts[q]->args.data(),
+                        mg.first->args_size);
+            std::memcpy(host.data() + mg.off_begins + q * sizeof(int), &beg, sizeof(int));
+            beg += mg.parts[q]->blocks;
+          }
+        }
+        MM_CUDA(cudaMalloc(&b->merged_args, bytes));
+        MM_CUDA(cudaMemcpy(b->merged_args, host.data(), bytes, cudaMemcpyHostToDevice));
+      }
       cudaGraph_t g;
       MM_CUDA(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
       MM_CUDA(cudaEventRecord(b->fork, b->st));
-      for (int i = 0; i < n; ++i) {
+      int launches = 0;
+      for (int i : branch_h) {
         cudaStream_t hs = b->hs[i]->eng->stream();
         MM_CUDA(cudaStreamWaitEvent(hs, b->fork, 0));
         b->hs[i]->eng->rk4_enqueue(dt);
         MM_CUDA(cudaEventRecord(b->joins[i], hs));
-        MM_CUDA(cudaStreamWaitEvent(b->st, b->joins[i], 0));
+        launches += b->hs[i]->eng->rk4_launches();
       }
+      unsigned char* base = static_cast<unsigned char*>(b->merged_args);
+      for (const Merged& mg : plan) {
+        MM_CUDA(mg.first->many(base + mg.off_args, reinterpret_cast<const int*>(base + mg.off_begins),
+                               static_cast<int>(mg.parts.size()), mg.blocks, mg.smem, b->st));
+        ++launches;
+      }
+      for (int i : branch_h) MM_CUDA(cudaStreamWaitEvent(b->st, b->joins[i], 0));
       MM_CUDA(cudaStreamEndCapture(b->st, &g));
+      b->launches = launches;
+      b->merged = static_cast<int>(rec_h.size());
       MM_CUDA(cudaGraphInstantiate(&b->graph, g, 0));
       cudaGraphDestroy(g);
       b->dt = dt;

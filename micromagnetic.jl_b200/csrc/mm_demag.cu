@@ -3,6 +3,7 @@
 #include <tuple>
 #include <mutex>
 #include <map>
+#include <set>
 #include <array>
 #include <cstdlib>
 #include <cmath>
@@ -13,6 +14,7 @@
 #include "mm_dd.cuh"
 #include "mm_demag.cuh"
 #include "mm_fft.cuh"
+#include "mm_launch.cuh"
 #include "mm_lines.cuh"
 
 namespace mm {
@@ -126,10 +128,25 @@ enum XMode { XM_MAGN = 0, XM_TENSOR = 1 };
 // Forward x pass: real rows (zero padded / mirrored to Px) -> half spectrum.
 // line = c*rows + row;  X[line*Hx + k].
 template <typename R, int MODE, int NT>
-__global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_fwd_x(
-    const R* __restrict__ m, const R* __restrict__ Ms, const double* __restrict__ Tr, int tsign,
-    cplx_t<R>* __restrict__ X, DemagGeom g, int lines_total, int nl, const cplx_t<R>* __restrict__ twx,
-    int half, FastDiv fnl) {
+struct FwdX {
+  static constexpr int kNT = NT, kMinB = (PassCfg<R, NT>::minb);
+  struct Args {
+    const R* __restrict__ m;
+    const R* __restrict__ Ms;
+    const double* __restrict__ Tr;
+    int tsign;
+    cplx_t<R>* __restrict__ X;
+    DemagGeom g;
+    int lines_total;
+    int nl;
+    const cplx_t<R>* __restrict__ twx;
+    int half;
+    FastDiv fnl;
+    dim3 grid;
+  };
+  static __device__ __forceinline__ void body(const Args& args, uint3 blockIdx) {
+    const auto& [m, Ms, Tr, tsign, X, g, lines_total, nl, twx, half, fnl, grid] = args;
+
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
@@ -191,7 +208,9 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_fwd_x(
       X[static_cast<int64_t>(line0 + l) * Hx + k] = spectrum(l, k);
     }
   }
-}
+  }
+};
+
 
 // Px == 1 (nx == 1): the x "transform" is the identity.
 template <typename R, int MODE>
@@ -210,9 +229,22 @@ __global__ void k_fwd_x1(const R* __restrict__ m, const R* __restrict__ Ms, cons
 
 // Inverse x pass: half spectrum -> real rows (unnormalised c2r), keeps nx.
 template <typename R, int NT>
-__global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_inv_x(
-    const cplx_t<R>* __restrict__ X, R* __restrict__ H, DemagGeom g, int lines_total, int nl,
-    const cplx_t<R>* __restrict__ twx, int half, FastDiv fnl) {
+struct InvX {
+  static constexpr int kNT = NT, kMinB = (PassCfg<R, NT>::minb);
+  struct Args {
+    const cplx_t<R>* __restrict__ X;
+    R* __restrict__ H;
+    DemagGeom g;
+    int lines_total;
+    int nl;
+    const cplx_t<R>* __restrict__ twx;
+    int half;
+    FastDiv fnl;
+    dim3 grid;
+  };
+  static __device__ __forceinline__ void body(const Args& args, uint3 blockIdx) {
+    const auto& [X, H, g, lines_total, nl, twx, half, fnl, grid] = args;
+
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
@@ -275,7 +307,9 @@ __global__ void __launch_bounds__(NT, (PassCfg<R, NT>::minb)) k_inv_x(
       if (u + 1 < nx) out[u + 1] = z.y;
     }
   }
-}
+  }
+};
+
 
 template <typename R>
 __global__ void k_inv_x1(const cplx_t<R>* __restrict__ X, R* __restrict__ H, int lines_total,
@@ -509,10 +543,27 @@ enum YLMode { YL_FWD = 0, YL_INV = 1, YL_CONV2D = 2 };
 // (kx = nfull W + blockIdx.x - nfull; Hx = 16 m + 1 for nx = 2^k) instead of
 // a W-wide tile of mostly absent columns; fnl1 divides by ncompc.
 template <typename R, int MODE, int NT, bool I32, bool XT = false>
-__global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_ylines(const cplx_t<R>* in, cplx_t<R>* out, const R* __restrict__ Nhat,
-                                                  DemagGeom g, int lgW, int ncompc, FastDiv fnl,
-                                                  const cplx_t<R>* __restrict__ twy, int half, int nfull,
-                                                  FastDiv fnl1) {
+struct YLines {
+  static constexpr int kNT = NT, kMinB = (sizeof(R) == 4 ? 3 : 2);
+  struct Args {
+    const cplx_t<R>* in;
+    cplx_t<R>* out;
+    const R* __restrict__ Nhat;
+    DemagGeom g;
+    int lgW0;
+    int ncompc;
+    FastDiv fnl0;
+    const cplx_t<R>* __restrict__ twy;
+    int half;
+    int nfull;
+    FastDiv fnl1;
+    dim3 grid;
+  };
+  static __device__ __forceinline__ void body(const Args& args, uint3 blockIdx) {
+    const auto& [in, out, Nhat, g, lgW0, ncompc, fnl0, twy, half, nfull, fnl1, grid] = args;
+    int lgW = lgW0;  // a leftover column takes one-column tiles
+    FastDiv fnl = fnl0;
+
   using C = cplx_t<R>;
   using IX = std::conditional_t<I32, int, int64_t>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -562,14 +613,29 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 3 : 2) k_ylines(const cpl
   } else {
     line_fft<MODE == YL_INV, NT>(src, dst, a, b, LS, nlines, fnl, g.ply, twy, 1);
   }
-}
+  }
+};
+
 
 // z lines (forward z, tensor product, inverse z, in place on Y) of one ky row
 // over a W-wide kx tile.  grid: (tiles, Py); consecutive blockIdx.y take ky
 // and Py - ky so the two reads of each tensor entry are close in time (L2).
 template <typename R, int NT, bool I32>
-__global__ void __launch_bounds__(NT, 2) k_zconv(cplx_t<R>* Y, const R* __restrict__ Nhat, DemagGeom g, int lgW,
-                                                 FastDiv fnl, const cplx_t<R>* __restrict__ twz, int half) {
+struct ZConv {
+  static constexpr int kNT = NT, kMinB = 2;
+  struct Args {
+    cplx_t<R>* Y;
+    const R* __restrict__ Nhat;
+    DemagGeom g;
+    int lgW;
+    FastDiv fnl;
+    const cplx_t<R>* __restrict__ twz;
+    int half;
+    dim3 grid;
+  };
+  static __device__ __forceinline__ void body(const Args& args, uint3 blockIdx) {
+    const auto& [Y, Nhat, g, lgW, fnl, twz, half, grid] = args;
+
   using C = cplx_t<R>;
   using IX = std::conditional_t<I32, int, int64_t>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -589,7 +655,9 @@ __global__ void __launch_bounds__(NT, 2) k_zconv(cplx_t<R>* Y, const R* __restri
   C* res = line_fft_to_smem<false, NT>(src, a, b, LS, nlines, fnl, g.plz, twz, 1);
   tensor_product<R, false, NT>(res, LS, lgW, Pz, g.fPz, kx0, ky, Nhat, Hx, Py, Pz);
   line_fft_from_smem<true, NT>(res, res == a ? b : a, dst, LS, nlines, fnl, g.plz, twz, 1);
-}
+  }
+};
+
 
 // z convolution for Pz = RA * RB (powers of two): forward radix-RA stage from
 // the Y rows into shared memory; then, per butterfly i < RA and in registers,
@@ -914,6 +982,22 @@ int newell_tensor_device(int nx, int ny, int nz, double dx, double dy, double dz
 
 
 // ============================================================ host side ====
+LaunchRecorder*& launch_recorder() {
+  thread_local LaunchRecorder* r = nullptr;
+  return r;
+}
+
+void smem_optin(const void* kernel) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({kernel, dev})) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
+  done.insert({kernel, dev});
+}
+
 template <typename C>
 static C* upload_twiddles(int L, size_t& bytes, cudaStream_t st) {
   std::vector<C> h(L);
@@ -933,9 +1017,9 @@ static C* upload_twiddles(int L, size_t& bytes, cudaStream_t st) {
 template <typename R, int NT>
 static void set_smem_attrs_nt() {
   const int mx = static_cast<int>(kMaxSmem);
-  cudaFuncSetAttribute(k_fwd_x<R, XM_MAGN, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_fwd_x<R, XM_TENSOR, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_inv_x<R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<FwdX<R, XM_MAGN, NT>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<FwdX<R, XM_TENSOR, NT>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<InvX<R, NT>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_ypass<R, YM_FWD, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_ypass<R, YM_INV, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_ypass<R, YM_CONV2D, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
@@ -943,20 +1027,20 @@ static void set_smem_attrs_nt() {
   cudaFuncSetAttribute(k_ypass<R, YM_TENSOR_Q, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_zpass<R, ZM_CONV, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_zpass<R, ZM_TENSOR_Q, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_FWD, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_INV, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_zconv<R, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_FWD, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_INV, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_CONV2D, NT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_FWD, NT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_FWD, NT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_INV, NT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_ylines<R, YL_INV, NT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_zconv<R, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_FWD, NT, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_INV, NT, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_CONV2D, NT, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<ZConv<R, NT, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_FWD, NT, false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_INV, NT, false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_CONV2D, NT, false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_CONV2D, NT, true, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_CONV2D, NT, false, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_FWD, NT, true, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_FWD, NT, false, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_INV, NT, true, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<YLines<R, YL_INV, NT, false, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_one<ZConv<R, NT, false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
 
 template <typename R>
@@ -1355,7 +1439,7 @@ static void launch_fwd_x(const DemagGeom& g, const R* m, const R* Ms, const doub
   const int blocks = (lines + nl - 1) / nl;
   const int half = nl * (g.Lc | 1);
   const size_t sm = 2 * sizeof(C) * half;
-  k_fwd_x<R, MODE, NT><<<blocks, NT, sm, st>>>(m, Ms, Tr, tsign, X, g, lines, nl, twx, half, make_fastdiv(nl));
+  launch_k<FwdX<R, MODE, NT>>(dim3(blocks), sm, st, {m, Ms, Tr, tsign, X, g, lines, nl, twx, half, make_fastdiv(nl), dim3()});
 }
 
 template <typename R, int MODE, int NT>
@@ -1441,15 +1525,15 @@ static void launch_ylines(const DemagGeom& g, const cplx_t<R>* in, cplx_t<R>* ou
   const FastDiv fnl = make_fastdiv(ncompc * W), fnl1 = make_fastdiv(ncompc);
   if (xt) {
     if (offsets_fit_int(g))
-      k_ylines<R, MODE, kHotNT, true, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1);
+      launch_k<YLines<R, MODE, kHotNT, true, true>>(grid, sm, st, {in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1, dim3()});
     else
-      k_ylines<R, MODE, kHotNT, false, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1);
+      launch_k<YLines<R, MODE, kHotNT, false, true>>(grid, sm, st, {in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1, dim3()});
     return;
   }
   if (offsets_fit_int(g))
-    k_ylines<R, MODE, kHotNT, true><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1);
+    launch_k<YLines<R, MODE, kHotNT, true>>(grid, sm, st, {in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1, dim3()});
   else
-    k_ylines<R, MODE, kHotNT, false><<<grid, kHotNT, sm, st>>>(in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1);
+    launch_k<YLines<R, MODE, kHotNT, false>>(grid, sm, st, {in, out, Nhat, g, ilog2(W), ncompc, fnl, twy, half, nfull, fnl1, dim3()});
 }
 
 template <typename R, int RA, int RB>
@@ -1535,9 +1619,9 @@ static void launch_zconv(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const 
   dim3 grid((g.Hx + W - 1) / W, g.Py, 1);
   const size_t sm = 2 * sizeof(C) * half;
   if (offsets_fit_int(g))
-    k_zconv<R, kHotNT, true><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz, half);
+    launch_k<ZConv<R, kHotNT, true>>(grid, sm, st, {Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz, half, dim3()});
   else
-    k_zconv<R, kHotNT, false><<<grid, kHotNT, sm, st>>>(Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz, half);
+    launch_k<ZConv<R, kHotNT, false>>(grid, sm, st, {Y, Nhat, g, ilog2(W), make_fastdiv(3 * W), twz, half, dim3()});
 }
 
 template <typename R>
@@ -1606,7 +1690,7 @@ static bool run_pass(const DemagPlan<R>& p, DemagGeom g, int which, const R* m, 
         const int nl = std::max(1, PassCfg<R, NT>::cap / g.Lc);
         const int half = nl * (g.Lc | 1);
         const size_t sm = 2 * sizeof(C) * half;
-        k_inv_x<R, NT><<<(lines + nl - 1) / nl, NT, sm, st>>>(p.X, Hd, g, lines, nl, p.twx, half, make_fastdiv(nl));
+        launch_k<InvX<R, NT>>(dim3((lines + nl - 1) / nl), sm, st, {p.X, Hd, g, lines, nl, p.twx, half, make_fastdiv(nl), dim3()});
       }
       return true;
     }
@@ -1726,6 +1810,19 @@ double DemagPlan<R>::pass_bytes(int which) const {
     case 3: return fused2d ? 0.0 : (nX + nY) * cw;
     case 4: return nX * cw + 3.0 * N * w;
     default: return 0.0;
+  }
+}
+
+template <typename R>
+bool DemagPlan<R>::batchable() const {
+  // the paths of run_pass that launch FwdX, YLines, ZConv and InvX only
+  if (long_x || long_y || g.Px == 1 || g.wreg) return false;
+  if (fused2d) return true;
+  if (sizeof(R) == 4 && zpair_enabled() && zpair_applies(g)) return false;
+  switch (g.Pz) {
+    case 4: case 8: case 16: case 32: case 64: case 128: return false;  // k_zconv2
+    case 256: return sizeof(R) != 4;
+    default: return true;
   }
 }
 

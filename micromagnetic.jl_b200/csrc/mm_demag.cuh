@@ -61,6 +61,9 @@ class DemagPlan {
   void apply(const R* m, const R* mu0Ms, R* Hd, cudaStream_t st, const int* gate = nullptr);
   // Number of kernel launches of one apply().
   int launches_per_apply() const;
+  // Every launch of apply() is a descriptor kernel (mm_launch.cuh), so that a
+  // batch can merge the passes of several meshes into one launch each.
+  bool batchable() const;
   // One pass alone (0 fwd-x, 1 fwd-y, 2 conv, 3 inv-y, 4 inv-x), for timing;
   // false when this geometry does not use it.
   bool launch_pass(int which, const R* m, const R* mu0Ms, R* Hd, cudaStream_t st);

@@ -2,6 +2,7 @@
 #include <cmath>
 
 #include "mm_field.cuh"
+#include "mm_launch.cuh"
 
 namespace mm {
 
@@ -709,18 +710,33 @@ __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage
 constexpr int kStageTileZ = 8;
 
 template <typename R>
-__global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2)
-    k_stage_tile(FieldArgs<R> a, const R* __restrict__ y, StageArgs<R> s) {
+struct StageTile {
+  static constexpr int kNT = kStageThreads, kMinB = sizeof(R) == 4 ? 3 : 2;
+  struct Args {
+    FieldArgs<R> a;
+    const R* y;
+    StageArgs<R> s;
+    int bx, by;  // the block's cells along x and y (bx * by = kNT)
+    dim3 grid;
+  };
+  static __device__ __forceinline__ void body(const Args& args, uint3 blockIdx);
+};
+
+template <typename R>
+__device__ __forceinline__ void StageTile<R>::body(const Args& args, uint3 blockIdx) {
+  const FieldArgs<R>& a = args.a;
+  const StageArgs<R>& s = args.s;
+  const R* __restrict__ y = args.y;
   constexpr bool kF32 = sizeof(R) == 4;
   extern __shared__ __align__(16) unsigned char smraw[];
   R* T = reinterpret_cast<R*>(smraw);
-  const int bx = blockDim.x, by = blockDim.y, TX = bx + 2, TY = by + 2, TP = TX * TY;
+  const int bx = args.bx, by = args.by, TX = bx + 2, TY = by + 2, TP = TX * TY;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int64_t N = a.N;
   const bool px = a.pbc & 1, py = a.pbc & 2, pz = a.pbc & 4;
   const int i0 = blockIdx.x * bx, j0 = blockIdx.y * by, k0 = blockIdx.z * kStageTileZ;
   const int k1 = min(nz, k0 + kStageTileZ);
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * bx + tx, nth = bx * by;
+  const int tid = threadIdx.x, tx = tid % bx, ty = tid / bx, nth = bx * by;
   const int i = i0 + tx, j = j0 + ty;
   const bool live = i < nx && j < ny;
   auto slot = [](int p) { return (p + 3) % 3; };
@@ -769,13 +785,57 @@ __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2)
   }
 }
 
-// halo-tiled RK4 / Heun stages unless MMCUDA_STAGETILE=0
+// Halo-tiled RK4 / Heun stages only with MMCUDA_STAGETILE=1: measured slower
+// than the one-plane-per-block kernel (c5 0.59 vs 0.38 ms, c2 0.16 vs 0.10 ms
+// a stage) -- each block waits for every plane's tile before computing it.
 static bool stage_tile_enabled() {
   static const bool on = [] {
     const char* e = getenv("MMCUDA_STAGETILE");
-    return !(e && e[0] == '0');
+    return e && e[0] == '1';
   }();
   return on;
+}
+
+// RK4 / Heun stage, one cell a thread and one z plane a block (k_stage's
+// SM_RK4 mode without the further terms) as a descriptor, so that batches can
+// merge it; blocks are 1-D, the cell tile bx x by comes with the arguments.
+template <typename R>
+struct StagePlain {
+  static constexpr int kNT = kStageThreads, kMinB = sizeof(R) == 4 ? 3 : 2;
+  struct Args {
+    FieldArgs<R> a;
+    const R* y;
+    StageArgs<R> s;
+    int bx, by;
+    dim3 grid;
+  };
+  static __device__ __forceinline__ void body(const Args& args, uint3 blockIdx) {
+    const FieldArgs<R>& a = args.a;
+    const StageArgs<R>& s = args.s;
+    constexpr bool kF32 = sizeof(R) == 4;
+    const int64_t N = a.N;
+    const int tid = threadIdx.x, bx = args.bx;
+    const int i = blockIdx.x * bx + tid % bx;
+    const int j = blockIdx.y * args.by + tid / bx;
+    const int k = blockIdx.z;
+    if (i >= a.nx || j >= a.ny) return;
+    const int I = (k * a.ny + j) * a.nx + i;
+    R mN[3], mL[3], av[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      mN[c] = s.m[c * N + I];
+      mL[c] = kF32 ? s.m_lo[c * N + I] : R(0);
+      av[c] = s.stage > 1 ? s.acc[c * N + I] : R(0);
+    }
+    R m[3], h[3];
+    cell_heff<R, false, false>(a, args.y, I, i, j, k, m, h, nullptr);
+    rk4_update(a, s, I, m, h, mN, mL, av);
+  }
+};
+
+template <typename R>
+bool stage_descriptor_used(const FieldArgs<R>& fa) {
+  return !((fa.mask & kExtraBits) || ((fa.mask & TB_DMI_BULK) && fa.x.bD[0]));
 }
 
 template <typename R>
@@ -795,13 +855,17 @@ void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<
   const size_t tsm = 3 * 3 * static_cast<size_t>(g.block.x + 2) * (g.block.y + 2) * sizeof(R);
   if (mode == SM_RK4 && stage_tile_enabled() && tsm <= 48 * 1024) {
     const dim3 grid(g.grid.x, g.grid.y, (fa.nz + kStageTileZ - 1) / kStageTileZ);
-    k_stage_tile<R><<<grid, g.block, tsm, st>>>(fa, y, sa);
+    launch_k<StageTile<R>>(grid, tsm, st,
+                           {fa, y, sa, static_cast<int>(g.block.x), static_cast<int>(g.block.y), dim3()});
+    return;
+  }
+  if (mode == SM_RK4) {
+    launch_k<StagePlain<R>>(g.grid, 0, st, {fa, y, sa, static_cast<int>(g.block.x), static_cast<int>(g.block.y), dim3()});
     return;
   }
   switch (mode) {
     case SM_FIELD: k_stage<R, SM_FIELD, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
     case SM_RHS: k_stage<R, SM_RHS, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-    case SM_RK4: k_stage<R, SM_RK4, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
     case SM_ENERGY: k_stage<R, SM_ENERGY, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
     default: k_stage<R, SM_DOPRI, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
   }
@@ -1187,6 +1251,7 @@ void launch_adj_field(const FieldArgs<R>& fa_lin, const R* w, const R* q, const 
 
 #define MM_INST(R)                                                                                       \
   template void launch_stage<R>(int, const FieldArgs<R>&, const R*, const StageArgs<R>&, cudaStream_t); \
+  template bool stage_descriptor_used<R>(const FieldArgs<R>&);                                            \
   template void launch_nbmask<R>(int, int, int, int, const R*, uint8_t*, cudaStream_t);                 \
   template void launch_aos_to_soa<R, double>(const double*, R*, R*, int64_t, int*, cudaStream_t);           \
   template void launch_aos_to_soa<R, float>(const float*, R*, R*, int64_t, int*, cudaStream_t);             \

@@ -139,6 +139,11 @@ void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<
 
 int stage_blocks(int64_t N);
 
+// launch_stage(SM_RK4, fa, ...) runs a descriptor kernel (mm_launch.cuh) for
+// these field arguments (no further terms)
+template <typename R>
+bool stage_descriptor_used(const FieldArgs<R>& fa);
+
 struct StageGrid {
   dim3 grid, block;
   int nblocks;

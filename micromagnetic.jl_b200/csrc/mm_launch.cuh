@@ -1,0 +1,93 @@
+// mm_launch.cuh -- kernels as descriptors, launched for one mesh or for many
+// meshes at once (internal).
+//
+// A descriptor K holds the kernel's arguments (K::Args, with the grid it was
+// sized for), its block size K::kNT, its occupancy hint K::kMinB and a device
+// body K::body(args, block index).  k_one<K> runs the body on one mesh's grid;
+// k_many<K> runs it over the concatenated grids of several meshes -- block b
+// finds its mesh i (begins[i] <= b < begins[i+1]) and its block index within
+// that mesh's grid -- so one launch covers a pass of every mesh of a batch.
+//
+// launch_k<K>() launches k_one<K>, or, while a LaunchRecorder is active on the
+// calling thread, appends a record (the arguments as bytes and the grid) that
+// the batch builder later merges with the same pass of other meshes.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <vector>
+
+namespace mm {
+
+template <class K>
+__global__ void __launch_bounds__(K::kNT, K::kMinB) k_one(const typename K::Args a) {
+  K::body(a, blockIdx);
+}
+
+template <class K>
+__global__ void __launch_bounds__(K::kNT, K::kMinB) k_many(const typename K::Args* __restrict__ A,
+                                                           const int* __restrict__ begins, int n) {
+  int lo = 0, hi = n - 1;
+  const int b = static_cast<int>(blockIdx.x);
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (begins[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  const typename K::Args& a = A[lo];
+  const unsigned local = static_cast<unsigned>(b - begins[lo]);
+  uint3 bid;
+  bid.x = local % a.grid.x;
+  bid.y = (local / a.grid.x) % a.grid.y;
+  bid.z = local / (a.grid.x * a.grid.y);
+  K::body(a, bid);
+}
+
+// One recorded launch: which kernel (its multi-mesh launcher), its arguments
+// and its launch shape.
+struct LaunchRec {
+  const void* kind;  // identity of the descriptor (k_many<K>)
+  // launches k_many<K> over n meshes whose Args (device) and block offsets
+  // (device) are given; total blocks, dynamic shared memory
+  cudaError_t (*many)(const void* args_dev, const int* begins_dev, int n, int blocks, size_t smem, cudaStream_t st);
+  size_t args_size;
+  std::vector<unsigned char> args;
+  int blocks;   // grid.x * grid.y * grid.z
+  size_t smem;  // dynamic shared memory
+};
+
+struct LaunchRecorder {
+  std::vector<LaunchRec> recs;
+};
+LaunchRecorder*& launch_recorder();  // the calling thread's active recorder (null: launch)
+// Raises the dynamic shared-memory limit of a kernel to the opt-in maximum,
+// once per (kernel, current device).
+void smem_optin(const void* kernel);
+
+template <class K>
+cudaError_t launch_many(const void* args_dev, const int* begins_dev, int n, int blocks, size_t smem, cudaStream_t st) {
+  if (smem > 48 * 1024) smem_optin(reinterpret_cast<const void*>(&k_many<K>));
+  k_many<K><<<blocks, K::kNT, smem, st>>>(static_cast<const typename K::Args*>(args_dev), begins_dev, n);
+  return cudaGetLastError();
+}
+
+template <class K>
+void launch_k(dim3 grid, size_t smem, cudaStream_t st, typename K::Args a) {
+  a.grid = grid;
+  if (LaunchRecorder* r = launch_recorder()) {
+    LaunchRec rec;
+    rec.kind = reinterpret_cast<const void*>(&k_many<K>);
+    rec.many = &launch_many<K>;
+    rec.args_size = sizeof(a);
+    rec.args.resize(sizeof(a));
+    std::memcpy(rec.args.data(), &a, sizeof(a));
+    rec.blocks = static_cast<int>(grid.x * grid.y * grid.z);
+    rec.smem = smem;
+    r->recs.push_back(std::move(rec));
+    return;
+  }
+  if (smem > 48 * 1024) smem_optin(reinterpret_cast<const void*>(&k_one<K>));
+  k_one<K><<<grid, K::kNT, smem, st>>>(a);
+}
+
+}  // namespace mm

@@ -42,7 +42,7 @@ EXPORTS = (
     "mm_add_demag", "mm_add_demag_tensor", "mm_effective_field", "mm_term_field", "mm_energy",
     "mm_llg_rhs", "mm_average_m", "mm_rk4_run", "mm_rk4_state", "mm_dopri_set_tol", "mm_run_until",
     "mm_advance_step", "mm_dopri_reset", "mm_relax", "mm_kernel_time", "mm_rk4_launches_per_step",
-    "mm_energy_noalloc", "mm_batch_create", "mm_batch_rk4_run", "mm_batch_get_stream", "mm_batch_destroy",
+    "mm_energy_noalloc", "mm_batch_create", "mm_batch_rk4_run", "mm_batch_get_stream", "mm_batch_launches", "mm_batch_destroy",
     "mm_heun_run", "mm_set_adaptive_method", "mm_ovf_write", "mm_ovf_read_header", "mm_ovf_read",
     "mm_save_ovf", "mm_load_ovf", "mm_adjoint_record", "mm_adjoint_backward", "mm_add_dmi_bulk_spatial",
     "mm_add_sot", "mm_add_stt_zhang_li", "mm_add_stt_slonczewski", "mm_add_thermal_noise", "mm_demag_tiles",
@@ -143,6 +143,7 @@ def load():
         "mm_batch_create": ([ctypes.POINTER(_vp), i, ctypes.POINTER(_vp)], i),
         "mm_batch_rk4_run": ([_vp, d, i64], i),
         "mm_batch_get_stream": ([_vp, ctypes.POINTER(_vp)], i),
+        "mm_batch_launches": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], i),
         "mm_batch_destroy": ([_vp], i),
     }
     for name, (args, res) in sig.items():
@@ -194,6 +195,12 @@ class Batch:
         s = _vp()
         check(load().mm_batch_get_stream(self.b, ctypes.byref(s)))
         return int(s.value or 0)
+
+    def launches(self):
+        """(kernel launches of one batched RK4 step, handles in merged launches)."""
+        n, k = ctypes.c_int(), ctypes.c_int()
+        check(load().mm_batch_launches(self.b, ctypes.byref(n), ctypes.byref(k)))
+        return n.value, k.value
 
     def close(self):
         if getattr(self, "b", None) and _lib is not None:

@@ -37,6 +37,10 @@ def test_batch_equals_individual_steps(form):
     batch.rk4_run(2e-14, 7)
     for a, b in pairs:
         assert rel_maxnorm(b.m(), a.m()) == 0.0
+    # the meshes' passes share launches: far fewer than one chain per mesh
+    launches, merged = batch.launches()
+    per_mesh = sum(b.h.rk4_launches() for _, b in pairs)
+    assert merged == len(pairs) and launches < per_mesh / 2, (launches, merged, per_mesh)
     batch.close()
 
 

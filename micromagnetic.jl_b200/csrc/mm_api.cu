@@ -1704,39 +1704,58 @@ int mm_batch_rk4_run(mm_batch* b, double dt, int64_t nsteps) {
         mm::launch_recorder() = nullptr;
         recs[j] = std::move(rec.recs);
       }
-      // greedy merge: the kernel that is next for the most meshes launches
-      // for all of them; every mesh's records stay in order
+      // the merged kernels keep the mesh's arguments in static shared
+      // memory: meshes whose passes need nearly all of a block's shared
+      // memory stay on their own branch
+      for (size_t j = 0; j < recs.size();) {
+        bool fits = true;
+        for (const mm::LaunchRec& r : recs[j]) fits = fits && r.smem + 4096 <= 227 * 1024;
+        if (fits) {
+          ++j;
+          continue;
+        }
+        branch_h.push_back(rec_h[j]);
+        rec_h.erase(rec_h.begin() + j);
+        recs.erase(recs.begin() + j);
+      }
+      // Meshes with the same sequence of kernels (e.g. films on the fused y
+      // convolution, 3-D meshes on the z convolution) form a family; each
+      // family runs on its own graph branch, its k-th launch merged over
+      // all its meshes, so the families overlap as independent meshes did.
       struct Merged {
         const mm::LaunchRec* first;
         std::vector<const mm::LaunchRec*> parts;
         int blocks = 0;
         size_t smem = 0, off_args = 0, off_begins = 0;
+        int family = 0;
       };
       std::vector<Merged> plan;
-      std::vector<size_t> next(recs.size(), 0);
-      for (;;) {
-        std::vector<std::pair<const void*, int>> cnt;
-        for (size_t j = 0; j < recs.size(); ++j) {
-          if (next[j] >= recs[j].size()) continue;
-          const void* k = recs[j][next[j]].kind;
-          auto it = std::find_if(cnt.begin(), cnt.end(), [&](const auto& p) { return p.first == k; });
-          if (it == cnt.end()) cnt.push_back({k, 1});
-          else ++it->second;
+      std::vector<std::vector<size_t>> families;  // members (indices into recs)
+      for (size_t j = 0; j < recs.size(); ++j) {
+        auto same = [&](size_t o) {
+          if (recs[o].size() != recs[j].size()) return false;
+          for (size_t q = 0; q < recs[j].size(); ++q)
+            if (recs[o][q].kind != recs[j][q].kind) return false;
+          return true;
+        };
+        auto f = std::find_if(families.begin(), families.end(), [&](const auto& fam) { return same(fam[0]); });
+        if (f == families.end()) families.push_back({j});
+        else f->push_back(j);
+      }
+      for (size_t fi = 0; fi < families.size(); ++fi) {
+        const auto& fam = families[fi];
+        for (size_t q = 0; q < recs[fam[0]].size(); ++q) {
+          Merged mg;
+          mg.first = &recs[fam[0]][q];
+          mg.family = static_cast<int>(fi);
+          for (size_t j : fam) {
+            const mm::LaunchRec* r = &recs[j][q];
+            mg.parts.push_back(r);
+            mg.blocks += r->blocks;
+            mg.smem = std::max(mg.smem, r->smem);
+          }
+          plan.push_back(std::move(mg));
         }
-        if (cnt.empty()) break;
-        const void* kind = std::max_element(cnt.begin(), cnt.end(),
-                                            [](const auto& a, const auto& c) { return a.second < c.second; })->first;
-        Merged mg;
-        mg.first = nullptr;
-        for (size_t j = 0; j < recs.size(); ++j) {
-          if (next[j] >= recs[j].size() || recs[j][next[j]].kind != kind) continue;
-          const mm::LaunchRec* r = &recs[j][next[j]++];
-          if (!mg.first) mg.first = r;
-          mg.parts.push_back(r);
-          mg.blocks += r->blocks;
-          mg.smem = std::max(mg.smem, r->smem);
-        }
-        plan.push_back(std::move(mg));
       }
       // one device buffer: per merged launch its Args array and block offsets
       size_t bytes = 0;
@@ -1771,13 +1790,23 @@ int mm_batch_rk4_run(mm_batch* b, double dt, int64_t nsteps) {
         MM_CUDA(cudaEventRecord(b->joins[i], hs));
         launches += b->hs[i]->eng->rk4_launches();
       }
+      // each family on the stream of its first handle (forked from the batch
+      // stream, joined back below)
       unsigned char* base = static_cast<unsigned char*>(b->merged_args);
-      for (const Merged& mg : plan) {
-        MM_CUDA(mg.first->many(base + mg.off_args, reinterpret_cast<const int*>(base + mg.off_begins),
-                               static_cast<int>(mg.parts.size()), mg.blocks, mg.smem, b->st));
-        ++launches;
+      for (size_t fi = 0; fi < families.size(); ++fi) {
+        const int hi = rec_h[families[fi][0]];
+        cudaStream_t fs = b->hs[hi]->eng->stream();
+        MM_CUDA(cudaStreamWaitEvent(fs, b->fork, 0));
+        for (const Merged& mg : plan) {
+          if (mg.family != static_cast<int>(fi)) continue;
+          MM_CUDA(mg.first->many(base + mg.off_args, reinterpret_cast<const int*>(base + mg.off_begins),
+                                 static_cast<int>(mg.parts.size()), mg.blocks, mg.smem, fs));
+          ++launches;
+        }
+        MM_CUDA(cudaEventRecord(b->joins[hi], fs));
       }
       for (int i : branch_h) MM_CUDA(cudaStreamWaitEvent(b->st, b->joins[i], 0));
+      for (const auto& fam : families) MM_CUDA(cudaStreamWaitEvent(b->st, b->joins[rec_h[fam[0]]], 0));
       MM_CUDA(cudaStreamEndCapture(b->st, &g));
       b->launches = launches;
       b->merged = static_cast<int>(rec_h.size());

@@ -34,7 +34,18 @@ __global__ void __launch_bounds__(K::kNT, K::kMinB) k_many(const typename K::Arg
     if (begins[mid] <= b) lo = mid;
     else hi = mid - 1;
   }
-  const typename K::Args& a = A[lo];
+  // the mesh's arguments are copied to shared memory once: the body reads
+  // them often (plans, strides), as k_one reads its parameter bank
+  using Args = typename K::Args;
+  static_assert(sizeof(Args) % 4 == 0, "argument structs are word multiples");
+  __shared__ __align__(16) unsigned char sa[sizeof(Args)];
+  {
+    const unsigned* src = reinterpret_cast<const unsigned*>(A + lo);
+    unsigned* dst = reinterpret_cast<unsigned*>(sa);
+    for (int w = threadIdx.x; w < static_cast<int>(sizeof(Args) / 4); w += K::kNT) dst[w] = src[w];
+  }
+  __syncthreads();
+  const Args& a = *reinterpret_cast<const Args*>(sa);
   const unsigned local = static_cast<unsigned>(b - begins[lo]);
   uint3 bid;
   bid.x = local % a.grid.x;

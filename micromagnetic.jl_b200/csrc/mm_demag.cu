@@ -994,7 +994,11 @@ void smem_optin(const void* kernel) {
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lk(mu);
   if (done.count({kernel, dev})) return;
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem));
+  // the opt-in limit covers static and dynamic shared memory together
+  cudaFuncAttributes fa{};
+  cudaFuncGetAttributes(&fa, kernel);
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(kMaxSmem) - static_cast<int>(fa.sharedSizeBytes));
   done.insert({kernel, dev});
 }
 

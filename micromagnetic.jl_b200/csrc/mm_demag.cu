@@ -98,6 +98,15 @@ static bool wreg_enabled() {
   return on;
 }
 
+// The direct-DFT z convolution for Pz <= 9 (ZSmall) unless MMCUDA_ZSMALL=0
+static bool zsmall_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MMCUDA_ZSMALL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 // The register-resident z convolution (mm_zpair.cu) where it applies, unless
 // MMCUDA_ZPAIR=0 keeps the shared-memory kernels
 static bool zpair_enabled() {
@@ -620,6 +629,86 @@ struct YLines {
 // z lines (forward z, tensor product, inverse z, in place on Y) of one ky row
 // over a W-wide kx tile.  grid: (tiles, Py); consecutive blockIdx.y take ky
 // and Py - ky so the two reads of each tensor entry are close in time (L2).
+// Short z lines (Pz = 3, 5, 7, 9: nz = 2 .. 5) on row-major spectra: one
+// thread per (kx, ky) line holds the three components in registers and runs
+// the forward transform of its nz inputs as a direct DFT (Pz x nz products),
+// the tensor product at every kz and the inverse DFT for the nz kept outputs
+// only -- no shared memory, no barrier.  The twiddles w_Pz^t (t < Pz) come with
+// the arguments.  (demag.jl:114-123 on the z axis.)
+template <typename R, int PZ>
+struct ZSmall {
+  static constexpr int kNT = 256, kMinB = sizeof(R) == 4 ? 2 : 1;
+  static constexpr int NZ = (PZ + 1) / 2;  // nz <= (Pz + 1) / 2 (Pz >= 2 nz - 1)
+  struct Args {
+    cplx_t<R>* Y;
+    const R* __restrict__ Nhat;
+    int Hx, Py, nz, Tyq, Tzq;
+    R twr[PZ], twi[PZ];  // w^t = exp(-2 pi i t / PZ)
+    dim3 grid;
+  };
+  static __device__ __forceinline__ void body(const Args& a, uint3 blockIdx) {
+    using C = cplx_t<R>;
+    const int64_t line = static_cast<int64_t>(blockIdx.x) * kNT + threadIdx.x;
+    const int Hx = a.Hx, Py = a.Py, nz = a.nz;
+    if (line >= static_cast<int64_t>(Hx) * Py) return;
+    const int ky = static_cast<int>(line / Hx), kx = static_cast<int>(line - static_cast<int64_t>(ky) * Hx);
+    const int64_t zs = static_cast<int64_t>(Py) * Hx, cs = zs * nz;
+    C* y0 = a.Y + static_cast<int64_t>(ky) * Hx + kx;
+    C x[3][NZ], v[3][PZ];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int n = 0; n < NZ; ++n) x[c][n] = n < nz ? y0[c * cs + n * zs] : cmk<C>(R(0), R(0));
+    // forward: v[k] = sum_{n < nz} x[n] w^(nk)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < PZ; ++k) {
+        C acc = x[c][0];
+#pragma unroll
+        for (int n = 1; n < NZ; ++n) {
+          if (n >= nz) break;
+          const int t = (n * k) % PZ;
+          acc = cadd(acc, cmul(x[c][n], cmk<C>(a.twr[t], a.twi[t])));
+        }
+        v[c][k] = acc;
+      }
+    // tensor product (xy odd in ky, xz in kz, yz in both)
+    const bool fy = ky > Py / 2;
+    const int kyq = fy ? Py - ky : ky;
+    const R sy = fy ? R(-1) : R(1);
+    const int64_t Ts = static_cast<int64_t>(a.Tzq) * a.Tyq * Hx;
+#pragma unroll
+    for (int k = 0; k < PZ; ++k) {
+      const bool fz = k > PZ / 2;
+      const int kzq = fz ? PZ - k : k;
+      const R sz = fz ? R(-1) : R(1);
+      const int64_t b = (static_cast<int64_t>(kzq) * a.Tyq + kyq) * Hx + kx;
+      const R xx = __ldg(a.Nhat + b), yy = __ldg(a.Nhat + Ts + b), zz = __ldg(a.Nhat + 2 * Ts + b);
+      const R xy = sy * __ldg(a.Nhat + 3 * Ts + b), xz = sz * __ldg(a.Nhat + 4 * Ts + b),
+              yz = sy * sz * __ldg(a.Nhat + 5 * Ts + b);
+      const C p0 = v[0][k], p1 = v[1][k], p2 = v[2][k];
+      v[0][k] = cmk<C>(xx * p0.x + xy * p1.x + xz * p2.x, xx * p0.y + xy * p1.y + xz * p2.y);
+      v[1][k] = cmk<C>(xy * p0.x + yy * p1.x + yz * p2.x, xy * p0.y + yy * p1.y + yz * p2.y);
+      v[2][k] = cmk<C>(xz * p0.x + yz * p1.x + zz * p2.x, xz * p0.y + yz * p1.y + zz * p2.y);
+    }
+    // inverse, kept outputs n < nz: y[n] = sum_k v[k] w^(-nk)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int n = 0; n < NZ; ++n) {
+        if (n >= nz) break;
+        C acc = v[c][0];
+#pragma unroll
+        for (int k = 1; k < PZ; ++k) {
+          const int t = (n * k) % PZ;
+          acc = cadd(acc, cmul(v[c][k], cmk<C>(a.twr[t], -a.twi[t])));
+        }
+        y0[c * cs + n * zs] = acc;
+      }
+  }
+};
+
 template <typename R, int NT, bool I32>
 struct ZConv {
   static constexpr int kNT = NT, kMinB = 2;
@@ -1607,6 +1696,38 @@ static bool try_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cp
   }
 }
 
+template <typename R, int PZ>
+static void launch_zsmall_pz(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, cudaStream_t st) {
+  typename ZSmall<R, PZ>::Args a{};
+  a.Y = Y;
+  a.Nhat = Nhat;
+  a.Hx = g.Hx;
+  a.Py = g.Py;
+  a.nz = g.nz;
+  a.Tyq = g.Tyq;
+  a.Tzq = g.Tzq;
+  for (int t = 0; t < PZ; ++t) {
+    const long double ang = -2.0L * 3.141592653589793238462643383279502884L * t / PZ;
+    a.twr[t] = static_cast<R>(static_cast<double>(cosl(ang)));
+    a.twi[t] = static_cast<R>(static_cast<double>(sinl(ang)));
+  }
+  const int64_t lines = static_cast<int64_t>(g.Hx) * g.Py;
+  launch_k<ZSmall<R, PZ>>(dim3(static_cast<unsigned>((lines + 255) / 256)), 0, st, a);
+}
+
+// the direct-DFT z convolution for Pz = 3, 5, 7, 9 on row-major spectra
+template <typename R>
+static bool try_zsmall(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, cudaStream_t st) {
+  if (g.yT || !zsmall_enabled()) return false;
+  switch (g.Pz) {
+    case 3: launch_zsmall_pz<R, 3>(g, Y, Nhat, st); return true;
+    case 5: launch_zsmall_pz<R, 5>(g, Y, Nhat, st); return true;
+    case 7: launch_zsmall_pz<R, 7>(g, Y, Nhat, st); return true;
+    case 9: launch_zsmall_pz<R, 9>(g, Y, Nhat, st); return true;
+    default: return false;
+  }
+}
+
 template <typename R>
 static void launch_zconv(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st,
                          int Wforce = 0) {
@@ -1618,6 +1739,7 @@ static void launch_zconv(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const 
     }
   }
   if (try_zconv2<R>(g, Y, Nhat, twz, st, Wforce)) return;
+  if (try_zsmall<R>(g, Y, Nhat, st)) return;
   const int W = Wforce > 0 ? Wforce : lines_tile<R>(g.Hx, g.Pz, 3, 2);
   const int half = 3 * W * (g.Pz | 1);
   dim3 grid((g.Hx + W - 1) / W, g.Py, 1);

@@ -17,6 +17,7 @@
 #include "../../include/mmcuda.h"
 #include "mm_demag.cuh"
 #include "mm_launch.cuh"
+#include "mm_persist.cuh"
 #include "mm_field.cuh"
 #include "mm_integ.cuh"
 
@@ -112,6 +113,7 @@ class EngineBase {
   virtual void rk4_enqueue(double dt) = 0;
   // every launch of rk4_enqueue is a descriptor kernel (mm_launch.cuh)
   virtual bool rk4_batchable() const = 0;
+  virtual bool is_fp32() const = 0;
   virtual void rk4_count(int64_t n, double dt) = 0;
   virtual uint64_t params_version() const = 0;
   virtual cudaStream_t stream() const = 0;
@@ -696,6 +698,36 @@ class Engine : public EngineBase {
   double he_dt = 0.0;
   uint64_t he_version = 0;
 
+  // Small meshes run their RK4 steps in the persistent step kernel
+  // (mm_persist.cu): one cooperative launch for up to 256 steps instead of
+  // one graph of about 4 x 6 kernels a step.
+  static constexpr int64_t kPersistCells = int64_t(1) << 17;
+  PersistProgram persist_;
+  double ps_dt = 0.0;
+  uint64_t ps_version = ~0ull;
+
+  int rk4_run_persistent(double dt, int64_t n) {
+    if (!persist_.ready() || ps_dt != dt || ps_version != version) {
+      std::vector<std::vector<LaunchRec>> recs(1);
+      LaunchRecorder rec;
+      launch_recorder() = &rec;
+      enqueue_rk4_step(dt);
+      launch_recorder() = nullptr;
+      recs[0] = std::move(rec.recs);
+      char msg[256] = {0};
+      const int rc = persist_.build(recs, kF32, msg, sizeof(msg));
+      if (rc) return fail(rc == -1 ? MM_ERR_UNSUPPORTED : MM_ERR_CUDA, "%s", msg);
+      ps_dt = dt;
+      ps_version = version;
+    }
+    const int rc = persist_.run(n, st_);
+    if (rc == 1) return fail(MM_ERR_TIMEOUT, "persistent RK4 step: a grid-barrier wait ran out");
+    if (rc) return fail(MM_ERR_CUDA, "persistent RK4 step: %s", cudaGetErrorString(cudaGetLastError()));
+    rk_n += n;
+    rk_t = static_cast<double>(rk_n) * dt;
+    return MM_OK;
+  }
+
   int rk4_run(double dt, int64_t n) override {
     if (int rc = need_ms()) return rc;
     if (n < 0 || !(dt > 0)) return fail(MM_ERR_ARG, "rk4: need dt > 0 and nsteps >= 0");
@@ -703,6 +735,7 @@ class Engine : public EngineBase {
     int rc;
     if (!acc && (rc = alloc(acc, 3 * N))) return rc;
     if (!yB && (rc = alloc(yB, 3 * N))) return rc;
+    if (n > 0 && persist_enabled() && N <= kPersistCells && rk4_batchable()) return rk4_run_persistent(dt, n);
     if (!rk_graph || rk_dt != dt || rk_version != version) {
       if (rk_graph) cudaGraphExecDestroy(rk_graph);
       rk_graph = nullptr;
@@ -736,6 +769,7 @@ class Engine : public EngineBase {
     return MM_OK;
   }
   void rk4_enqueue(double dt) override { enqueue_rk4_step(dt); }
+  bool is_fp32() const override { return kF32; }
   bool rk4_batchable() const override {
     if (mask & TB_THERMAL) return false;
     if (!stage_descriptor_used<R>(fargs(~0u))) return false;
@@ -1375,6 +1409,10 @@ struct mm_batch {
   void* merged_args = nullptr;  // device: per merged launch, the meshes' Args and block offsets
   int launches = 0;             // kernel launches of one step
   int merged = 0;               // handles in the merged launches
+  // small batches whose launches all have a persistent form run in the
+  // persistent step kernel instead of the graph (one launch per 256 steps)
+  mm::PersistProgram persist;
+  bool use_persist = false;
   ~mm_batch() {
     cudaSetDevice(device);
     if (graph) cudaGraphExecDestroy(graph);
@@ -1387,6 +1425,9 @@ struct mm_batch {
 };
 
 using mm::fail;
+
+// batches of at most this many cells run in the persistent step kernel
+static constexpr int64_t kPersistBatchCells = int64_t(1) << 20;
 
 // merged pass launches in batches unless MMCUDA_BATCH_MERGE=0
 static bool batch_merge_enabled() {
@@ -1674,7 +1715,7 @@ int mm_batch_rk4_run(mm_batch* b, double dt, int64_t nsteps) {
   if (cudaSetDevice(b->device) != cudaSuccess) return fail(MM_ERR_CUDA, "cudaSetDevice failed");
   try {
     const int n = static_cast<int>(b->hs.size());
-    bool stale = !b->graph || b->dt != dt || static_cast<int>(b->versions.size()) != n;
+    bool stale = (!b->graph && !b->use_persist) || b->dt != dt || static_cast<int>(b->versions.size()) != n;
     for (int i = 0; i < n && !stale; ++i) stale = b->versions[i] != b->hs[i]->eng->params_version();
     for (int i = 0; i < n; ++i)
       if (int rc = b->hs[i]->eng->rk4_prepare()) return rc;
@@ -1688,6 +1729,44 @@ int mm_batch_rk4_run(mm_batch* b, double dt, int64_t nsteps) {
       b->graph = nullptr;
       if (b->merged_args) cudaFree(b->merged_args);
       b->merged_args = nullptr;
+      b->persist.release();
+      b->use_persist = false;
+      int64_t cells = 0;
+      bool all = mm::persist_enabled() && batch_merge_enabled();
+      for (int i = 0; i < n && all; ++i) {
+        all = b->hs[i]->eng->rk4_batchable() && b->hs[i]->eng->is_fp32() == b->hs[0]->eng->is_fp32();
+        cells += static_cast<int64_t>(b->hs[i]->mesh.nx) * b->hs[i]->mesh.ny * b->hs[i]->mesh.nz;
+      }
+      if (all && cells <= kPersistBatchCells) {
+        std::vector<std::vector<mm::LaunchRec>> recs(n);
+        for (int i = 0; i < n; ++i) {
+          mm::LaunchRecorder rec;
+          mm::launch_recorder() = &rec;
+          b->hs[i]->eng->rk4_enqueue(dt);
+          mm::launch_recorder() = nullptr;
+          recs[i] = std::move(rec.recs);
+        }
+        char msg[256] = {0};
+        b->use_persist = b->persist.build(recs, b->hs[0]->eng->is_fp32(), msg, sizeof(msg)) == 0;
+      }
+    }
+    if (b->use_persist) {
+      b->dt = dt;
+      b->versions.resize(n);
+      for (int i = 0; i < n; ++i) b->versions[i] = b->hs[i]->eng->params_version();
+      b->launches = 1;
+      b->merged = n;
+      const int rc = b->persist.run(nsteps, b->st);
+      if (rc == 1) return fail(MM_ERR_TIMEOUT, "persistent batch step: a grid-barrier wait ran out");
+      if (rc) return fail(MM_ERR_CUDA, "persistent batch step failed");
+      MM_CUDA(cudaEventRecord(b->done, b->st));
+      for (int i = 0; i < n; ++i) {
+        MM_CUDA(cudaStreamWaitEvent(b->hs[i]->eng->stream(), b->done, 0));
+        b->hs[i]->eng->rk4_count(nsteps, dt);
+      }
+      return MM_OK;
+    }
+    if (stale) {
       // record the steps of the handles whose launches can be merged
       std::vector<int> rec_h, branch_h;
       for (int i = 0; i < n; ++i)

@@ -54,10 +54,16 @@ __global__ void __launch_bounds__(K::kNT, K::kMinB) k_many(const typename K::Arg
   K::body(a, bid);
 }
 
+// Index of a descriptor in the persistent step kernel's dispatch
+// (mm_persist.cu), -1 for descriptors it does not run.
+template <class K> struct PersistKind { static constexpr int value = -1; };
+
 // One recorded launch: which kernel (its multi-mesh launcher), its arguments
 // and its launch shape.
 struct LaunchRec {
   const void* kind;  // identity of the descriptor (k_many<K>)
+  int pkind;         // PersistKind<K>::value
+  dim3 grid;
   // launches k_many<K> over n meshes whose Args (device) and block offsets
   // (device) are given; total blocks, dynamic shared memory
   cudaError_t (*many)(const void* args_dev, const int* begins_dev, int n, int blocks, size_t smem, cudaStream_t st);
@@ -88,6 +94,8 @@ void launch_k(dim3 grid, size_t smem, cudaStream_t st, typename K::Args a) {
   if (LaunchRecorder* r = launch_recorder()) {
     LaunchRec rec;
     rec.kind = reinterpret_cast<const void*>(&k_many<K>);
+    rec.pkind = PersistKind<K>::value;
+    rec.grid = grid;
     rec.many = &launch_many<K>;
     rec.args_size = sizeof(a);
     rec.args.resize(sizeof(a));

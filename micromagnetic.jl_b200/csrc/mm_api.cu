@@ -716,7 +716,8 @@ class Engine : public EngineBase {
       recs[0] = std::move(rec.recs);
       char msg[256] = {0};
       const int rc = persist_.build(recs, kF32, msg, sizeof(msg));
-      if (rc) return fail(rc == -1 ? MM_ERR_UNSUPPORTED : MM_ERR_CUDA, "%s", msg);
+      if (rc == -1) return -1;  // a kernel without a persistent form: the caller takes the graph
+      if (rc) return fail(MM_ERR_CUDA, "%s", msg);
       ps_dt = dt;
       ps_version = version;
     }
@@ -735,7 +736,10 @@ class Engine : public EngineBase {
     int rc;
     if (!acc && (rc = alloc(acc, 3 * N))) return rc;
     if (!yB && (rc = alloc(yB, 3 * N))) return rc;
-    if (n > 0 && persist_enabled() && N <= kPersistCells && rk4_batchable()) return rk4_run_persistent(dt, n);
+    if (n > 0 && persist_enabled() && N <= kPersistCells && rk4_batchable()) {
+      const int prc = rk4_run_persistent(dt, n);
+      if (prc != -1) return prc;
+    }
     if (!rk_graph || rk_dt != dt || rk_version != version) {
       if (rk_graph) cudaGraphExecDestroy(rk_graph);
       rk_graph = nullptr;

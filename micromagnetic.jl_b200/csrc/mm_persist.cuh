@@ -10,7 +10,7 @@
 
 namespace mm {
 
-// MMCUDA_PERSIST=0 turns the persistent path off
+// MMCUDA_PERSIST=1 turns the persistent path on (off by default)
 bool persist_enabled();
 
 class PersistProgram {

@@ -1,11 +1,11 @@
-"""The persistent RK4 step kernel (small meshes and small batches): the same
-states as the graph of separate launches, bit for bit, and a bounded grid
+"""The persistent RK4 step kernel (opt-in, MMCUDA_PERSIST=1: small meshes and
+small batches run up to 256 steps a cooperative launch): the same states as
+the default graphs of separate launches, bit for bit, and a bounded grid
 barrier -- a barrier whose wait limit runs out ends the kernel with
 MM_ERR_TIMEOUT instead of hanging it.
 
-The switches are read once per process, so the graph path (MMCUDA_PERSIST=0)
-and the one-spin barrier limit (MMCUDA_BARRIER_SPINS=1) run in child
-processes."""
+The switches are read once per process, so the persistent path and the
+one-spin barrier limit (MMCUDA_BARRIER_SPINS=1) run in child processes."""
 import os
 import subprocess
 import sys
@@ -53,10 +53,10 @@ np.savez(%r, **out)
 
 def test_persistent_equals_graph(tmp_path):
     """RK4 steps of small meshes (films, 3-D, PBC; both forms) in the
-    persistent kernel (this process) and as separate launches (a child with
-    MMCUDA_PERSIST=0): identical states."""
-    path = str(tmp_path / "graph.npz")
-    r = _child(STEP % (MESHES, path), {"MMCUDA_PERSIST": "0"}, tmp_path)
+    persistent kernel (a child with MMCUDA_PERSIST=1) and as separate
+    launches (this process): identical states."""
+    path = str(tmp_path / "persist.npz")
+    r = _child(STEP % (MESHES, path), {"MMCUDA_PERSIST": "1"}, tmp_path)
     assert r.returncode == 0, r.stdout + r.stderr
     ref = np.load(path)
     for mesh in MESHES:
@@ -68,25 +68,32 @@ def test_persistent_equals_graph(tmp_path):
             np.testing.assert_array_equal(g.m(), ref[key])
 
 
-def test_persistent_batch():
+BATCH = """
+import numpy as np
+from helpers import GpuSim, random_config
+from mmcuda import _lib
+rng = np.random.default_rng(5)
+pairs = []
+for f in range(6):
+    nx, ny, nz = int(rng.integers(8, 40)), int(rng.integers(8, 40)), int(rng.integers(1, 5))
+    cfg = random_config(500 + f, nx, ny, nz, "", terms=("exch", "dmi_int", "anis", "zeeman", "demag"))
+    pairs.append((GpuSim(cfg, form=1), GpuSim(cfg, form=1)))
+batch = _lib.Batch([b.h for _, b in pairs])
+for a, _ in pairs:
+    a.rk4(2e-14, 5)
+batch.rk4_run(2e-14, 5)
+assert batch.launches() == (1, len(pairs)), batch.launches()
+for a, b in pairs:
+    np.testing.assert_array_equal(b.m(), a.m())
+print("ok")
+"""
+
+
+def test_persistent_batch(tmp_path):
     """A small batch runs as one persistent launch and gives the states of
     its handles stepped one by one."""
-    from mmcuda import _lib
-
-    rng = np.random.default_rng(5)
-    pairs = []
-    for f in range(6):
-        nx, ny, nz = int(rng.integers(8, 40)), int(rng.integers(8, 40)), int(rng.integers(1, 5))
-        cfg = random_config(500 + f, nx, ny, nz, "", terms=("exch", "dmi_int", "anis", "zeeman", "demag"))
-        pairs.append((GpuSim(cfg, form=1), GpuSim(cfg, form=1)))
-    batch = _lib.Batch([b.h for _, b in pairs])
-    for a, _ in pairs:
-        a.rk4(2e-14, 5)
-    batch.rk4_run(2e-14, 5)
-    assert batch.launches() == (1, len(pairs))
-    for a, b in pairs:
-        np.testing.assert_array_equal(b.m(), a.m())
-    batch.close()
+    r = _child(BATCH, {"MMCUDA_PERSIST": "1"}, tmp_path)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
 
 
 TIMEOUT = """
@@ -102,6 +109,6 @@ print("rc", rc, _lib.last_error())
 def test_barrier_wait_limit_reports_timeout(tmp_path):
     """With a barrier wait limit of one spin the blocks that arrive early give
     up: mm_rk4_run returns MM_ERR_TIMEOUT (-5) and the process ends normally."""
-    r = _child(TIMEOUT, {"MMCUDA_BARRIER_SPINS": "1"}, tmp_path)
+    r = _child(TIMEOUT, {"MMCUDA_PERSIST": "1", "MMCUDA_BARRIER_SPINS": "1"}, tmp_path)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "rc -5" in r.stdout and "grid-barrier" in r.stdout, r.stdout

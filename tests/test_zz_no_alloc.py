@@ -75,3 +75,52 @@ def test_energy_noalloc_rejects_oversized_mesh():
     rc = _lib.load().mm_energy_noalloc(ctypes.byref(big), *args[1:])
     assert rc == -1 and "static scratch limit" in _lib.last_error()
     h.close()
+
+
+@pytest.mark.parametrize("mesh", [(37, 23, 5, ""), (16, 8, 12, "xyz")])
+def test_energy_noalloc_matches_oracle(mesh):
+    """The same energies against the CPU oracle's compute_system_energy
+    restatement (src/micro/field.jl:520-536), term by term."""
+    from oracle.oracle import OracleSim
+
+    nx, ny, nz, pbc = mesh
+    torch, _lib, h, ref, out, args = _setup(*mesh, seed=mesh[0] * 10000 + mesh[1] * 100 + mesh[2])
+    rng = np.random.default_rng(mesh[0] * 10000 + mesh[1] * 100 + mesh[2])
+    n = nx * ny * nz
+    Ms = rng.uniform(4e5, 9e5, n)
+    Ms[rng.random(n) < 0.1] = 0.0
+    m = rng.normal(size=(n, 3))
+    m /= np.linalg.norm(m, axis=1, keepdims=True)
+    m[Ms == 0] = 0.0
+    A, D, Ku, axis, H = 1.2e-11, 2.5e-3, 3e5, (0.3, -0.2, 0.9), (1.5e4, -2.0e4, 3.0e4)
+    o = OracleSim(nx, ny, nz, 2e-9, 2.5e-9, 3e-9, pbc)
+    o.set_Ms(Ms)
+    o.set_m(m.reshape(-1))
+    o.add_zeeman(np.tile(np.asarray(H), n))
+    o.add_exch(Ax=A, Ay=A, Az=A)
+    o.add_dmi_bulk(D, D, D)
+    o.add_anis(np.full(n, Ku), axis)
+    _, per = o.energy(4)  # zeeman, exchange, bulk DMI, anisotropy in the order added
+    L = _lib.load()
+    _lib.check(L.mm_energy_noalloc(*args))
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    for t, e in zip((0, 1, 2, 4), per):
+        assert abs(got[t] - e) <= REL_TOL * abs(e), (t, got[t], e)
+    h.close()
+
+
+def test_energy_noalloc_allocates_nothing():
+    """After the first call (which loads the library's device code and its
+    static array), further calls leave the device's free memory unchanged."""
+    torch, _lib, h, ref, out, args = _setup(37, 23, 5, "", seed=77)
+    L = _lib.load()
+    _lib.check(L.mm_energy_noalloc(*args))
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(4):
+        _lib.check(L.mm_energy_noalloc(*args))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    h.close()

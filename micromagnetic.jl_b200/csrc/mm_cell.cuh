@@ -469,9 +469,9 @@ struct StagePlain {
     const StageArgs<R>& s = args.s;
     constexpr bool kF32 = sizeof(R) == 4;
     const int64_t N = a.N;
-    const int tid = threadIdx.x, bx = args.bx;
-    const int i = blockIdx.x * bx + tid % bx;
-    const int j = blockIdx.y * args.by + tid / bx;
+    const int tid = threadIdx.x, bx = args.bx;  // bx: a power of two
+    const int i = blockIdx.x * bx + (tid & (bx - 1));
+    const int j = blockIdx.y * args.by + (tid >> (__ffs(bx) - 1));
     const int k = blockIdx.z;
     if (i >= a.nx || j >= a.ny) return;
     const int I = (k * a.ny + j) * a.nx + i;

@@ -101,25 +101,31 @@ template <bool INV, typename C> __device__ __forceinline__ void dft16(C* v) {
   }
 }
 
-// cos, sin of 2*pi*k/32, k = 0..15 (mathematical constants)
-__constant__ const double c_w32[16][2] = {
-    {1.00000000000000000000, 0.00000000000000000000},
-    {0.98078528040323043058, 0.19509032201612824808},
-    {0.92387953251128673848, 0.38268343236508978178},
-    {0.83146961230254523567, 0.55557023301960217765},
-    {0.70710678118654757274, 0.70710678118654746172},
-    {0.55557023301960228867, 0.83146961230254523567},
-    {0.38268343236508983729, 0.92387953251128673848},
-    {0.19509032201612833135, 0.98078528040323043058},
-    {0.00000000000000006123, 1.00000000000000000000},
-    {-0.19509032201612819257, 0.98078528040323043058},
-    {-0.38268343236508972627, 0.92387953251128673848},
-    {-0.55557023301960195560, 0.83146961230254545772},
-    {-0.70710678118654746172, 0.70710678118654757274},
-    {-0.83146961230254534669, 0.55557023301960217765},
-    {-0.92387953251128673848, 0.38268343236508989280},
-    {-0.98078528040323043058, 0.19509032201612860891},
-};
+// cos, sin of 2*pi*k/32, k = 0..15 (mathematical constants).  A constexpr
+// function rather than a __constant__ table: the butterflies read it at
+// indices fixed by loop unrolling, which then fold into immediate operands
+// of the right precision instead of constant-bank loads of doubles.
+__host__ __device__ constexpr double w32_cs(int k, int sin_part) {
+  constexpr double t[16][2] = {
+      {1.00000000000000000000, 0.00000000000000000000},
+      {0.98078528040323044913, 0.19509032201612826785},
+      {0.92387953251128675613, 0.38268343236508977173},
+      {0.83146961230254523708, 0.55557023301960222474},
+      {0.70710678118654752440, 0.70710678118654752440},
+      {0.55557023301960222474, 0.83146961230254523708},
+      {0.38268343236508977173, 0.92387953251128675613},
+      {0.19509032201612826785, 0.98078528040323044913},
+      {0.00000000000000000000, 1.00000000000000000000},
+      {-0.19509032201612826785, 0.98078528040323044913},
+      {-0.38268343236508977173, 0.92387953251128675613},
+      {-0.55557023301960222474, 0.83146961230254523708},
+      {-0.70710678118654752440, 0.70710678118654752440},
+      {-0.83146961230254523708, 0.55557023301960222474},
+      {-0.92387953251128675613, 0.38268343236508977173},
+      {-0.98078528040323044913, 0.19509032201612826785},
+  };
+  return t[k][sin_part];
+}
 
 // 32 = 2 x 16: DFT16 of the even and odd samples, twiddles w32^k
 template <bool INV, typename C> __device__ __forceinline__ void dft32(C* v) {
@@ -134,7 +140,7 @@ template <bool INV, typename C> __device__ __forceinline__ void dft32(C* v) {
   dft16<INV>(o);
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
-    const R c = static_cast<R>(c_w32[k][0]), sn = static_cast<R>(c_w32[k][1]);
+    const R c = static_cast<R>(w32_cs(k, 0)), sn = static_cast<R>(w32_cs(k, 1));
     const C t = cmul(o[k], cmk<C>(c, INV ? sn : -sn));
     v[k] = cadd(e[k], t);
     v[k + 16] = csub(e[k], t);

@@ -24,28 +24,40 @@ namespace mm {
 
 namespace {
 
-constexpr int kWrNT = 128;  // x passes: 4 warps
 constexpr int kWyNT = 256;  // y passes: 8 warps, 4 lines x 2 halves (Q = 32)
 
-// rows of one x-pass block: 4 warps x (32 / Q) groups
-template <int Q> constexpr int x_rows() { return 4 * (32 / Q); }
+// rows of one x-pass block: W warps x (32 / Q) groups
+template <int Q, int W> constexpr int x_rows() { return W * (32 / Q); }
 // Staging stride (complex values between consecutive k of the block's RB
 // rows): lanes of a half warp touch 16 distinct 8-byte banks, i.e. the stride
 // is odd for Q >= 16 (one group of 16 lanes) and 2 or 4 mod 16 for Q = 8 or 4
-// (lane groups side by side).
-template <int Q> constexpr int x_stride() { return x_rows<Q>() + (x_rows<Q>() >= 8 ? x_rows<Q>() / 8 : 1); }
-// shared memory of an x-pass block: the transpose tiles or the staged rows
-template <int Q> constexpr int x_smem() {
-  return 4 * wtile_size<Q>() > (32 * Q + 1) * x_stride<Q>() ? 4 * wtile_size<Q>() : (32 * Q + 1) * x_stride<Q>();
+// (lane groups side by side; RB is then a multiple of 16).
+template <int Q, int W> constexpr int x_stride() { return x_rows<Q, W>() + (Q >= 16 ? 1 : (Q == 8 ? 2 : 4)); }
+// shared memory of an x-pass block (complex values): the transpose tiles or
+// the staged rows
+template <int Q, int W> constexpr int x_smem() {
+  return W * wtile_size<Q>() > (32 * Q + 1) * x_stride<Q, W>() ? W * wtile_size<Q>()
+                                                                : (32 * Q + 1) * x_stride<Q, W>();
+}
+
+// Warps of an x-pass block (4 or 8; MMCUDA_XWARPS=4 selects 4).  A block
+// moves column segments of RB = W (32 / Q) rows: 8 warps write and read
+// 64-byte segments of the column-major X for Q = 32.
+int xwarps() {
+  static const int w = [] {
+    const char* e = getenv("MMCUDA_XWARPS");
+    return e && atoi(e) == 4 ? 4 : 8;
+  }();
+  return w;
 }
 
 // ---------------------------------------------------------------- x forward
 // Rows of m * mu0Ms (zero padded to Px = 2 Lc) -> X column-major.
-template <int Q>
-__global__ void __launch_bounds__(kWrNT) k_xfwd_w(const float* __restrict__ m, const float* __restrict__ Ms,
-                                                 float2* __restrict__ X, DemagGeom g, const float2* __restrict__ twx) {
-  constexpr int RB = x_rows<Q>(), L = 32 * Q, S = x_stride<Q>();
-  __shared__ __align__(16) float2 sm[x_smem<Q>()];
+template <int Q, int W>
+__global__ void __launch_bounds__(32 * W, 24 / W) k_xfwd_w(const float* __restrict__ m, const float* __restrict__ Ms,
+                                                  float2* __restrict__ X, DemagGeom g, const float2* __restrict__ twx) {
+  constexpr int RB = x_rows<Q, W>(), L = 32 * Q, S = x_stride<Q, W>();
+  extern __shared__ __align__(16) float2 sm[];  // x_smem<Q, W>() values
   if (g.gate && !*g.gate) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gq = lane / Q, q = lane % Q;
@@ -73,7 +85,7 @@ __global__ void __launch_bounds__(kWrNT) k_xfwd_w(const float* __restrict__ m, c
   for (int r = 0; r < 32; ++r) sm[(q + Q * (r / Q) + 32 * (r % Q)) * S + rl] = v[r];
   __syncthreads();
   // X[k] = E + w_Px^k O, E = (Z[k] + conj Z[Lc-k]) / 2, O = (Z[k] - conj Z[Lc-k]) / 2i
-  for (int e = threadIdx.x; e < Hx * RB; e += kWrNT) {
+  for (int e = threadIdx.x; e < Hx * RB; e += 32 * W) {
     const int k = e / RB, r = e - k * RB;
     const float2 zk = sm[(k == L ? 0 : k) * S + r];
     float2 zc = sm[(k == 0 ? 0 : L - k) * S + r];
@@ -86,11 +98,11 @@ __global__ void __launch_bounds__(kWrNT) k_xfwd_w(const float* __restrict__ m, c
 
 // ---------------------------------------------------------------- x inverse
 // X column-major -> real rows (c2r, unnormalised), keeps x < nx.
-template <int Q>
-__global__ void __launch_bounds__(kWrNT) k_xinv_w(const float2* __restrict__ X, float* __restrict__ H, DemagGeom g,
-                                                 const float2* __restrict__ twx) {
-  constexpr int RB = x_rows<Q>(), L = 32 * Q, S = x_stride<Q>();
-  __shared__ __align__(16) float2 sm[x_smem<Q>()];
+template <int Q, int W>
+__global__ void __launch_bounds__(32 * W, 24 / W) k_xinv_w(const float2* __restrict__ X, float* __restrict__ H, DemagGeom g,
+                                                  const float2* __restrict__ twx) {
+  constexpr int RB = x_rows<Q, W>(), L = 32 * Q, S = x_stride<Q, W>();
+  extern __shared__ __align__(16) float2 sm[];  // x_smem<Q, W>() values
   if (g.gate && !*g.gate) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gq = lane / Q, q = lane % Q;
@@ -99,7 +111,7 @@ __global__ void __launch_bounds__(kWrNT) k_xinv_w(const float2* __restrict__ X, 
   const int line0 = blockIdx.x * RB;
   const int c = line0 / rows, row0 = line0 - c * rows;
   const int rl = warp * (32 / Q) + gq;
-  for (int e = threadIdx.x; e < Hx * RB; e += kWrNT) {
+  for (int e = threadIdx.x; e < Hx * RB; e += 32 * W) {
     const int k = e / RB, r = e - k * RB;
     sm[k * S + r] = X[(static_cast<int64_t>(c) * Hx + k) * rows + row0 + r];
   }
@@ -217,25 +229,135 @@ __global__ void __launch_bounds__(kWyNT, 3) k_yinv_w(const float2* __restrict__ 
   }
 }
 
+// ------------------------------------------------- y passes, warp-direct
+// The same transforms with no block-wide barrier: every group reads its
+// inputs from and writes its outputs to HBM directly, so the warps of a
+// block run their load, transform and store phases independently and the
+// loads of some warps overlap the arithmetic of others.  Half s of a line
+// touches every other complex value of the padded column (Y[2k + s]); the two
+// halves of a line (the two groups of a warp for Q = 16, a warp pair for
+// Q = 32) cover whole 32-byte sectors between them.
+constexpr int kWdNT = 256;
+
+// The warp-direct y passes unless MMCUDA_YDIRECT=0 keeps the block-staged ones
+bool ydirect_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MMCUDA_YDIRECT");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+template <int Q>
+__global__ void __launch_bounds__(kWdNT, 3) k_yfwd_d(const float2* __restrict__ X, float2* __restrict__ Y, DemagGeom g,
+                                                 const float2* __restrict__ twy, int nlines) {
+  constexpr int Py = 64 * Q;
+  extern __shared__ __align__(16) float2 tiles[];  // (kWdNT / 32) warp tiles
+  if (g.gate && !*g.gate) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gq = lane / Q, q = lane % Q;
+  const int u = (blockIdx.x * (kWdNT / 32) + warp) * (32 / Q) + gq, s = u & 1;
+  const int line = u >> 1;
+  if (line >= nlines) return;  // both halves of a line (whole warps) leave together
+  const float2* xc = X + static_cast<int64_t>(line) * (Py / 2);
+  float2 v[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    float2 a = xc[q + Q * j];
+    if (s) a = cmul(a, __ldg(twy + q + Q * j));
+    v[j] = a;
+  }
+  wfft<Q, false, 2>(v, tiles + warp * wtile_size<Q>(), twy);
+  float2* yc = Y + static_cast<int64_t>(line) * Py + s;
+#pragma unroll
+  for (int r = 0; r < 32; ++r) yc[2 * (q + Q * (r / Q) + 32 * (r % Q))] = v[r];
+}
+
+template <int Q>
+__global__ void __launch_bounds__(kWdNT, 3) k_yinv_d(const float2* __restrict__ Y, float2* __restrict__ X, DemagGeom g,
+                                                 const float2* __restrict__ twy, int nlines) {
+  constexpr int Py = 64 * Q, ny = 32 * Q;
+  extern __shared__ __align__(16) float2 tiles[];  // (kWdNT / 32) warp tiles
+  if (g.gate && !*g.gate) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gq = lane / Q, q = lane % Q;
+  const int u = (blockIdx.x * (kWdNT / 32) + warp) * (32 / Q) + gq, s = u & 1;
+  const int line = u >> 1;
+  // a Q = 32 warp pair meets at a named barrier: both warps of a pair hold
+  // the same line, so they stay or leave together
+  if (line >= nlines) return;
+  const float2* yc = Y + static_cast<int64_t>(line) * Py + s;
+  float2 v[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = yc[2 * (q + Q * j)];
+  float2* tile = tiles + warp * wtile_size<Q>();
+  wfft<Q, true, 2>(v, tile, twy);
+  if (s) {
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+      float2 w = __ldg(twy + q + Q * (r / Q) + 32 * (r % Q));
+      w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+  }
+  // x[y] = u0[y] + w^(-y) u1[y], y = q + Q (r / Q) + 32 (r % Q): half s keeps
+  // the registers r with r % 2 == s and receives those from its partner
+  float2* xo = X + static_cast<int64_t>(line) * ny;
+  if constexpr (Q == 32) {
+    // partner = the other warp of the pair: send through this warp's tile
+#pragma unroll
+    for (int i = 0; i < 16; ++i) tile[i * 32 + lane] = s ? v[2 * i] : v[2 * i + 1];
+    asm volatile("bar.sync %0, 64;\n" ::"r"(1 + (warp >> 1)) : "memory");
+    const float2* pt = tiles + (warp ^ 1) * wtile_size<Q>();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const float2 a = s ? v[2 * i + 1] : v[2 * i], b = pt[i * 32 + lane];
+      xo[q + 32 * (2 * i + s)] = make_float2(a.x + b.x, a.y + b.y);
+    }
+  } else {
+    // partner = the other group of this warp (lane ^ Q)
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const float2 mine = s ? v[2 * i + 1] : v[2 * i], send = s ? v[2 * i] : v[2 * i + 1];
+      const float bx = __shfl_xor_sync(0xffffffffu, send.x, Q);
+      const float by = __shfl_xor_sync(0xffffffffu, send.y, Q);
+      const int r = 2 * i + s;
+      xo[q + Q * (r / Q) + 32 * (r % Q)] = make_float2(mine.x + bx, mine.y + by);
+    }
+  }
+}
+
 template <int Q>
 void launch_q(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,
               const float2* twx, const float2* twy, cudaStream_t st) {
   const int rows = g.ny * g.nz;
   const int ylines = 3 * g.Hx * g.nz;
-  constexpr int NL = 4 * (32 / Q);
+  constexpr int NL = 4 * (32 / Q), DL = (kWdNT / 32) * (32 / Q) / 2;
   const size_t ysm = static_cast<size_t>(8) * wtile_size<Q>() * sizeof(float2);
   switch (which) {
     case 0:
-      k_xfwd_w<Q><<<3 * rows / x_rows<Q>(), kWrNT, 0, st>>>(m, Ms, X, g, twx);
+      if (xwarps() == 4)
+        k_xfwd_w<Q, 4><<<3 * rows / x_rows<Q, 4>(), 128, x_smem<Q, 4>() * sizeof(float2), st>>>(m, Ms, X, g, twx);
+      else
+        k_xfwd_w<Q, 8><<<3 * rows / x_rows<Q, 8>(), 256, x_smem<Q, 8>() * sizeof(float2), st>>>(m, Ms, X, g, twx);
       break;
     case 1:
-      k_yfwd_w<Q><<<(ylines + NL - 1) / NL, kWyNT, ysm, st>>>(X, Y, g, twy, ylines);
+      if (ydirect_enabled())
+        k_yfwd_d<Q><<<(ylines + DL - 1) / DL, kWdNT, ysm, st>>>(X, Y, g, twy, ylines);
+      else
+        k_yfwd_w<Q><<<(ylines + NL - 1) / NL, kWyNT, ysm, st>>>(X, Y, g, twy, ylines);
       break;
     case 3:
-      k_yinv_w<Q><<<(ylines + NL - 1) / NL, kWyNT, ysm, st>>>(Y, X, g, twy, ylines);
+      if (ydirect_enabled())
+        k_yinv_d<Q><<<(ylines + DL - 1) / DL, kWdNT, ysm, st>>>(Y, X, g, twy, ylines);
+      else
+        k_yinv_w<Q><<<(ylines + NL - 1) / NL, kWyNT, ysm, st>>>(Y, X, g, twy, ylines);
       break;
     case 4:
-      k_xinv_w<Q><<<3 * rows / x_rows<Q>(), kWrNT, 0, st>>>(X, H, g, twx);
+      if (xwarps() == 4)
+        k_xinv_w<Q, 4><<<3 * rows / x_rows<Q, 4>(), 128, x_smem<Q, 4>() * sizeof(float2), st>>>(X, H, g, twx);
+      else
+        k_xinv_w<Q, 8><<<3 * rows / x_rows<Q, 8>(), 256, x_smem<Q, 8>() * sizeof(float2), st>>>(X, H, g, twx);
       break;
     default:
       break;
@@ -247,6 +369,16 @@ void set_attrs_q() {
   const int b = 8 * wtile_size<Q>() * static_cast<int>(sizeof(float2));
   cudaFuncSetAttribute(k_yfwd_w<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   cudaFuncSetAttribute(k_yinv_w<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  cudaFuncSetAttribute(k_yfwd_d<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  cudaFuncSetAttribute(k_yinv_d<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  cudaFuncSetAttribute(k_xfwd_w<Q, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(x_smem<Q, 4>() * sizeof(float2)));
+  cudaFuncSetAttribute(k_xinv_w<Q, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(x_smem<Q, 4>() * sizeof(float2)));
+  cudaFuncSetAttribute(k_xfwd_w<Q, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(x_smem<Q, 8>() * sizeof(float2)));
+  cudaFuncSetAttribute(k_xinv_w<Q, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(x_smem<Q, 8>() * sizeof(float2)));
 }
 
 int wq(int n) {

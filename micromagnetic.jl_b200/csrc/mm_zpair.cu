@@ -27,10 +27,15 @@ namespace {
 
 constexpr int kZpNT = 256;
 constexpr int kZpLines = kZpNT / 2;  // lines per block
+// Shared tensor row (one component, one kz quadrant row, the block's 128
+// lines) padded by 16 floats: the two halves of a thread pair read rows kzq
+// and kzq +/- 1, which then fall 16 banks apart.
+constexpr int kZpRow = kZpLines + 16;
+constexpr int kZpTzq = 17;  // kz quadrant rows of Pz = 32
 
-// tensor entries a block uses: 6 components x 17 kz quadrant rows x the
+// tensor entries a block stages: 6 components x 17 kz quadrant rows x the
 // block's 128 lines (their ky mirror index, or kx, is one contiguous run)
-constexpr int kZpTensor = 6 * 17 * kZpLines;
+constexpr int kZpTensor = 6 * kZpTzq * kZpRow;
 
 __device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
   const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -44,7 +49,7 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
   if (g.gate && !*g.gate) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int t = lane & 15, s = lane >> 4;
-  const int Hx = g.Hx, Py = g.Py, nz = g.nz, Tyq = g.Tyq, Tzq = g.Tzq;
+  const int Hx = g.Hx, Py = g.Py, nz = g.nz, Tyq = g.Tyq;
   const int line0 = blockIdx.x * kZpLines;
   const int line = line0 + warp * 16 + t;
   int kx, ky;
@@ -56,28 +61,34 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
     kx = line;
   }
   const bool live = YT ? ky < Py : kx < Hx;
-  const int64_t Ts = static_cast<int64_t>(Tzq) * Tyq * Hx;
   // Prefetch the block's tensor entries into shared memory (cp.async), in
   // flight while the rows load and the forward transforms run: entry
-  // (c6 * 17 + kzq, line l) at tn[(c6 * 17 + kzq) * 128 + l], the tensor row
-  // of line l's mirror index (ky or Py - ky, column-major) or its kx.
+  // (c6, kzq) of block line l at tn[(c6 * 17 + kzq) * kZpRow + l], from the
+  // tensor row of line l's mirror index (ky or Py - ky, column-major) or kx.
+  // Thread (l, h) copies line l's entries of components 3h .. 3h + 2.
   {
-    const int nlines = min(kZpLines, (YT ? Py : Hx) - line0);
-    for (int e = threadIdx.x; e < 6 * 17 * kZpLines; e += kZpNT) {
-      const int r = e / kZpLines, l = e - r * kZpLines;  // r = c6 * 17 + kzq
-      if (l >= nlines) continue;
-      const int c6 = r / 17, kzq = r - c6 * 17;
-      if (kzq >= Tzq) continue;
-      int64_t src;
+    const int l = threadIdx.x & (kZpLines - 1), h = threadIdx.x >> 7;
+    if (l < (YT ? Py : Hx) - line0) {
+      const int64_t Ts = static_cast<int64_t>(kZpTzq) * Tyq * Hx;  // component stride
+      const int64_t kzs = static_cast<int64_t>(Tyq) * Hx;            // kz quadrant row stride
+      int64_t off;
       if (YT) {
         const int kyl = line0 + l;
-        const int kyq = kyl > Py / 2 ? Py - kyl : kyl;
-        src = c6 * Ts + (static_cast<int64_t>(kzq) * Hx + kx) * Tyq + kyq;
+        off = static_cast<int64_t>(kx) * Tyq + (kyl > Py / 2 ? Py - kyl : kyl);
       } else {
-        const int kyq = ky > Py / 2 ? Py - ky : ky;
-        src = c6 * Ts + (static_cast<int64_t>(kzq) * Tyq + kyq) * Hx + line0 + l;
+        off = static_cast<int64_t>(ky > Py / 2 ? Py - ky : ky) * Hx + line0 + l;
       }
-      cp_async4(tn + e, Nhat + src);
+      const float* src = Nhat + 3 * h * Ts + off;
+      float* dst = tn + 3 * h * kZpTzq * kZpRow + l;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const float* sp = src + j * Ts;
+#pragma unroll
+        for (int kzq = 0; kzq < kZpTzq; ++kzq) {
+          cp_async4(dst + (j * kZpTzq + kzq) * kZpRow, sp);
+          sp += kzs;
+        }
+      }
     }
     asm volatile("cp.async.commit_group;\n" ::);
   }
@@ -97,7 +108,7 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
     if (s) {
 #pragma unroll
       for (int n = 1; n < 16; ++n) {
-        const float wr = static_cast<float>(c_w32[n][0]), wi = -static_cast<float>(c_w32[n][1]);
+        const float wr = static_cast<float>(w32_cs(n, 0)), wi = -static_cast<float>(w32_cs(n, 1));
         v[c][n] = cmul(v[c][n], make_float2(wr, wi));
       }
     }
@@ -106,21 +117,21 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
   asm volatile("cp.async.wait_group 0;\n" ::);
   __syncthreads();
   // tensor product at kz = 2k + s (one quadrant stored; xy odd in ky, xz in
-  // kz, yz in both)
+  // kz, yz in both): kz <= 15 for k < 8 (kzq = kz), kz >= 18 for k > 8
+  // (kzq = 32 - kz, xz and yz negated), and k = 8 gives kz = 16 (s = 0) or
+  // the mirrored 17 -> 15 (s = 1)
   if (live) {
-    const bool fy = ky > Py / 2;
-    const float sy = fy ? -1.f : 1.f;
+    const float sy = ky > Py / 2 ? -1.f : 1.f;
     const int l = line - line0;
+    const float* lo = tn + s * kZpRow + l;          // row s (+ 2k)
+    const float* hi = tn + (16 - s) * kZpRow + l;   // row 16 - s (+ 16 - 2k)
+    constexpr int cr = kZpTzq * kZpRow;             // component stride
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-      const int kz = 2 * k + s;
-      const bool fz = kz > 16;
-      const int kzq = fz ? 32 - kz : kz;
-      const float sz = fz ? -1.f : 1.f;
-      const float* tb = tn + kzq * kZpLines + l;
-      constexpr int cs = 17 * kZpLines;
-      const float xx = tb[0], yy = tb[cs], zz = tb[2 * cs];
-      const float xy = sy * tb[3 * cs], xz = sz * tb[4 * cs], yz = sy * sz * tb[5 * cs];
+      const float* tb = k < 8 ? lo + 2 * k * kZpRow : hi + (16 - 2 * k) * kZpRow;
+      const float sz = k < 8 ? 1.f : (k > 8 ? -1.f : (s ? -1.f : 1.f));
+      const float xx = tb[0], yy = tb[cr], zz = tb[2 * cr];
+      const float xy = sy * tb[3 * cr], xz = sz * tb[4 * cr], yz = sy * sz * tb[5 * cr];
       const C p0 = v[0][k], p1 = v[1][k], p2 = v[2][k];
       v[0][k] = make_float2(xx * p0.x + xy * p1.x + xz * p2.x, xx * p0.y + xy * p1.y + xz * p2.y);
       v[1][k] = make_float2(xy * p0.x + yy * p1.x + yz * p2.x, xy * p0.y + yy * p1.y + yz * p2.y);
@@ -134,7 +145,7 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
     if (s) {
 #pragma unroll
       for (int n = 1; n < 16; ++n) {
-        const float wr = static_cast<float>(c_w32[n][0]), wi = static_cast<float>(c_w32[n][1]);
+        const float wr = static_cast<float>(w32_cs(n, 0)), wi = static_cast<float>(w32_cs(n, 1));
         v[c][n] = cmul(v[c][n], make_float2(wr, wi));
       }
     }
@@ -157,7 +168,7 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
 
 }  // namespace
 
-bool zpair_applies(const DemagGeom& g) { return g.Pz == 32 && g.nz <= 16 && g.nz >= 1; }
+bool zpair_applies(const DemagGeom& g) { return g.Pz == 32 && g.Tzq == kZpTzq && g.nz <= 16 && g.nz >= 1; }
 
 void launch_zpair_f32(const DemagGeom& g, float2* Y, const float* Nhat, cudaStream_t st) {
   const size_t sm = sizeof(float) * kZpTensor;

@@ -90,6 +90,10 @@ int mm_create(const mm_mesh_desc* mesh, int form, int device, mm_handle** out);
 int mm_destroy(mm_handle* h);
 /* CUDA stream (cudaStream_t) the handle launches on. */
 int mm_get_stream(mm_handle* h, void** stream);
+/* Waits for the handle's stream.  MM_ERR_TIMEOUT: a bounded device wait of a
+ * demag pass (the bulk-copy fed y passes and z convolution of the FP32
+ * register path) ran out on this device since the last call; the fields
+ * computed meanwhile are incomplete. */
 int mm_synchronize(mm_handle* h);
 /* Bytes of device memory held by the handle. */
 int mm_device_bytes(mm_handle* h, size_t* bytes);

@@ -1518,6 +1518,10 @@ int mm_synchronize(mm_handle* h) {
   MM_HANDLE(h);
   cudaError_t e = cudaStreamSynchronize(h->eng->stream());
   if (e != cudaSuccess) return fail(MM_ERR_CUDA, "%s", cudaGetErrorString(e));
+  const bool y_timeout = mm::wreg_take_timeout(), z_timeout = mm::zpair_take_timeout();
+  if (y_timeout || z_timeout)
+    return fail(MM_ERR_TIMEOUT, "demag %s pass: a bounded bulk-copy wait ran out (fields of that pass are incomplete)",
+                y_timeout ? "y" : "z");
   return MM_OK;
 }
 

@@ -205,16 +205,16 @@ __global__ void __launch_bounds__(NT, (zconv2_minb<R, NT>())) k_zconv2(cplx_t<R>
   lstage<RA, true, true, NT>(A, dst, L, nlines, fnl, RB, twz, 1);
 }
 
-// FP64 tensor quadrant [6][Tzq][Tyq][Hx] to RO, column-major [6][Tzq][Hx][Tyq]
-// (films: Tzq = 1)
+// FP64 tensor quadrant [6][Tzq][Tyq][Hx] to RO, column-major [6][Tzq][Hx][Tys]
+// (rows of Tyq values at stride Tys >= Tyq; films: Tzq = 1)
 template <typename RO>
-__global__ void k_cast_cols(const double* __restrict__ a, RO* __restrict__ b, int Tyq, int Hx, int Tzq) {
+__global__ void k_cast_cols(const double* __restrict__ a, RO* __restrict__ b, int Tyq, int Tys, int Hx, int Tzq) {
   const int64_t plane = static_cast<int64_t>(Tyq) * Hx, n = 6LL * Tzq * plane;
   for (int64_t o = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; o < n;
        o += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t c = o / plane, r = o - c * plane;
     const int64_t kx = r / Tyq, ky = r - kx * Tyq;
-    b[o] = static_cast<RO>(a[c * plane + ky * Hx + kx]);
+    b[(c * Hx + kx) * Tys + ky] = static_cast<RO>(a[c * plane + ky * Hx + kx]);
   }
 }
 
@@ -529,6 +529,7 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
   g.Hx = g.Px > 1 ? g.Lc + 1 : 1;
   g.Tyq = g.Py / 2 + 1;
   g.Tzq = g.Pz / 2 + 1;
+  g.Tys = g.Tyq;
   // one line (x, y; the three components of a z line) with its ping-pong
   // buffer must fit one block's shared memory, in the FP64 tensor passes too
   // x and y lines longer than one block holds (FP64 tensor passes included)
@@ -606,10 +607,17 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
     if (cudaMalloc(&Zx, sizeof(C) * nZ) != cudaSuccess || cudaMalloc(&Zx2, sizeof(C) * nZ) != cudaSuccess) return 2;
     bytes_ += 2 * sizeof(C) * nZ;
   }
-  const int64_t nT = 6LL * g.Tzq * g.Tyq * g.Hx;
+  if (sizeof(R) == 4 && g.yT && zpair_enabled() && zpair_applies(g)) g.Tys = (g.Tyq + 3) & ~3;
+  const int64_t nT = 6LL * g.Tzq * g.Tys * g.Hx;
   if (cudaMalloc(&Nhat, sizeof(R) * nT) != cudaSuccess) return 2;
   bytes_ += sizeof(R) * nT;
   cudaMemsetAsync(Nhat, 0, sizeof(R) * nT, st);
+  if constexpr (sizeof(R) == 4) {
+    if (g.yT && zpair_enabled() && zpair_applies(g) && !zpair_tensor_map(g, Nhat, zmap)) {
+      snprintf(err, nerr, "demag: tensor map of the z convolution could not be encoded");
+      return -1;
+    }
+  }
   if (g.Px > 1 && !(twx = upload_twiddles<C>(g.Px, bytes_, st))) return 2;
   if (!(twy = upload_twiddles<C>(g.Py, bytes_, st))) return 2;
   if (!(twz = upload_twiddles<C>(g.Pz, bytes_, st))) return 2;
@@ -1078,11 +1086,11 @@ static bool try_zsmall(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, cudaStre
 
 template <typename R>
 static void launch_zconv(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const cplx_t<R>* twz, cudaStream_t st,
-                         int Wforce = 0) {
+                         int Wforce, const void* zmap) {
   using C = cplx_t<R>;
   if constexpr (sizeof(R) == 4) {
     if (zpair_enabled() && zpair_applies(g)) {
-      launch_zpair_f32(g, Y, Nhat, st);
+      launch_zpair_f32(g, Y, Nhat, zmap, st);
       return;
     }
   }
@@ -1138,7 +1146,7 @@ static bool run_pass(const DemagPlan<R>& p, DemagGeom g, int which, const R* m, 
       else if (p.long_y && g.Pz == 1)
         k_gproduct_film<R><<<gblocks(static_cast<int64_t>(g.Py) * g.Hx), 256, 0, st>>>(p.Y, p.Nhat, g.Py, g.Hx, g.Tyq,
                                                                                     g.gate);
-      else launch_zconv<R>(g, p.Y, p.Nhat, p.twz, st, p.tile[2]);
+      else launch_zconv<R>(g, p.Y, p.Nhat, p.twz, st, p.tile[2], p.zmap);
       return true;
     case 3:
       if (p.fused2d) return false;
@@ -1373,7 +1381,7 @@ int DemagPlan<R>::set_tensor(const double* T6N, cudaStream_t st) {
         launch_zpass<double, ZM_TENSOR_Q, NT>(g64, Y64, nullptr, Tq + c * Ts, 1, g.Tyq, tz, sz, scale, st);
       }
     }
-    if (g.xT || g.yT) k_cast_cols<R><<<1024, 256, 0, st>>>(Tq, Nhat, g.Tyq, g.Hx, g.Tzq);
+    if (g.xT || g.yT) k_cast_cols<R><<<1024, 256, 0, st>>>(Tq, Nhat, g.Tyq, g.Tys, g.Hx, g.Tzq);
     else k_cast<R><<<1024, 256, 0, st>>>(Tq, Nhat, 6 * Ts);
     rc = static_cast<int>(cudaGetLastError());
     cudaStreamSynchronize(st);

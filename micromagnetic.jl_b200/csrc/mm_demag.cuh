@@ -23,6 +23,11 @@ struct DemagGeom {
   int Px, Py, Pz;  // padded lengths
   int Lc, Hx;      // Lc = Px/2 (0 when Px == 1), Hx = Lc + 1 (1 when Px == 1)
   int Tyq, Tzq;    // Py/2 + 1, Pz/2 + 1
+  // ky row stride of the column-major 3-D tensor, Nhat[((c*Tzq + kz)*Hx +
+  // kx)*Tys + ky]: Tyq, or Tyq rounded up to a multiple of 4 (16-byte rows,
+  // zero padded) where the register z convolution loads its tensor slice
+  // with tiled bulk copies
+  int Tys;
   FftPlan1 plx, ply, plz;
   FastDiv fLc, fHx, fPy, fPz, fny, fnz, frows, fpady, fpadz;
   // films on the fused y-convolution path keep the x spectrum column-major,
@@ -92,6 +97,7 @@ class DemagPlan {
   C* X = nullptr;
   C* Y = nullptr;
   R* Nhat = nullptr;
+  alignas(64) unsigned char zmap[128] = {};  // tensor map of the z convolution's slice loads (FP32, yT)
   C* twx = nullptr;
   C* twy = nullptr;
   C* twz = nullptr;
@@ -103,12 +109,23 @@ class DemagPlan {
 // Register-resident z convolution for Pz = 32 (nz <= 16), FP32 form
 // (mm_zpair.cu): in place on Y, either spectrum layout.
 bool zpair_applies(const DemagGeom& g);
-void launch_zpair_f32(const DemagGeom& g, float2* Y, const float* Nhat, cudaStream_t st);
+// Column-major spectra (g.yT): the block's tensor slice arrives by one tiled
+// bulk copy through a tensor map over Nhat (built by zpair_tensor_map, 128
+// bytes); the row-major layout copies it with cp.async.
+bool zpair_tensor_map(const DemagGeom& g, const float* Nhat, void* map128);
+void launch_zpair_f32(const DemagGeom& g, float2* Y, const float* Nhat, const void* map128, cudaStream_t st);
+// Tries of a bounded bulk-copy wait (MMCUDA_COPY_SPINS overrides; 0 makes
+// every first wait run out, which the tests use to check the timeout path).
+unsigned copy_wait_spins();
+bool zpair_take_timeout();
 
 // Register-resident x and y passes, FP32 form (mm_wreg.cu): which = 0 fwd-x
 // (m, Ms -> X), 1 fwd-y (X -> Y), 3 inv-y (Y -> X), 4 inv-x (X -> H).
 bool wreg_applies(int nx, int ny, int nz, int Px, int Py);
 void wreg_set_attrs();
+// True (and cleared) when a bounded wait of a bulk-copy y pass ran out on the
+// current device since the last call (synchronises the device).
+bool wreg_take_timeout();
 void launch_wreg_f32(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,
                      const float2* twx, const float2* twy, cudaStream_t st);
 

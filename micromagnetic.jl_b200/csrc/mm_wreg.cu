@@ -17,6 +17,9 @@
 //     Y[2k + s] = DFT_ny(x[n] w_Py^(n s))[k],
 // and the inverse keeps y < ny as u0[y] + w_Py^(-y) u1[y], us the ny-point
 // inverse transform of Y[2k + s].  (src/micro/demag.jl:102-131.)
+#include <algorithm>
+#include <cstdlib>
+
 #include "mm_demag.cuh"
 #include "mm_wfft.cuh"
 
@@ -40,21 +43,18 @@ template <int Q, int W> constexpr int x_smem() {
                                                                 : (32 * Q + 1) * x_stride<Q, W>();
 }
 
-// Warps of an x-pass block (4 or 8; MMCUDA_XWARPS=4 selects 4).  A block
-// moves column segments of RB = W (32 / Q) rows: 8 warps write and read
-// 64-byte segments of the column-major X for Q = 32.
-int xwarps() {
-  static const int w = [] {
-    const char* e = getenv("MMCUDA_XWARPS");
-    return e && atoi(e) == 4 ? 4 : 8;
-  }();
-  return w;
-}
+// Warps of an x-pass block: the forward pass runs 4 (no register cap: 87
+// registers, five blocks an SM by shared memory), the inverse pass 8 (80
+// registers, three blocks an SM), which moves column segments of RB = 8 rows
+// (64 bytes for Q = 32).  Measured on c5 (1024 x 1024 x 16, Q = 32):
+// forward 0.248 ms with 4 warps, 0.273 with 8 (0.287 with 4 capped at 96
+// registers); inverse 0.287 ms with 4 warps, 0.273 with 8.
+constexpr int kXfW = 4, kXiW = 8;
 
 // ---------------------------------------------------------------- x forward
 // Rows of m * mu0Ms (zero padded to Px = 2 Lc) -> X column-major.
 template <int Q, int W>
-__global__ void __launch_bounds__(32 * W, 24 / W) k_xfwd_w(const float* __restrict__ m, const float* __restrict__ Ms,
+__global__ void __launch_bounds__(32 * W) k_xfwd_w(const float* __restrict__ m, const float* __restrict__ Ms,
                                                   float2* __restrict__ X, DemagGeom g, const float2* __restrict__ twx) {
   constexpr int RB = x_rows<Q, W>(), L = 32 * Q, S = x_stride<Q, W>();
   extern __shared__ __align__(16) float2 sm[];  // x_smem<Q, W>() values
@@ -327,6 +327,166 @@ __global__ void __launch_bounds__(kWdNT, 3) k_yinv_d(const float2* __restrict__ 
   }
 }
 
+// ------------------------------------------ y passes, Q = 32, bulk-copy fed
+// One block of two warps (the two output parities of a line) walks lines
+// blockIdx.x, blockIdx.x + gridDim.x, ...  Its input line arrives in shared
+// memory by one bulk copy (cp.async.bulk, completion counted on an
+// mbarrier); as soon as both warps hold the line in registers the copy of
+// the block's next line is issued into the same buffer, so the load of line
+// i + 1 overlaps the transform and the stores of line i.  Waits on the
+// mbarrier are bounded (copy_wait_spins() tries): a wait that runs out sets
+// g_wreg_timeout, waits once more (a fixed, larger bound) for the copy in
+// flight, and the block leaves; mm_synchronize reports it as MM_ERR_TIMEOUT.
+constexpr int kWpNT = 64;
+constexpr unsigned kDrainSpins = 1u << 24;  // the second wait, after a timeout
+__device__ int g_wreg_timeout;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// one arrival that also expects `bytes` of copies, then the copy itself
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // earlier reads of dst before the copy's writes
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned spins) {
+  const unsigned a = smem_addr(bar);
+  for (unsigned i = 0; i < spins; ++i) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+// the bounded wait of every thread of the block, with one outcome for all
+__device__ __forceinline__ bool block_wait(unsigned long long* bar, unsigned parity, unsigned spins) {
+  const bool ok = mbar_wait(bar, parity, spins);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(&g_wreg_timeout, 1);
+    mbar_wait(bar, parity, kDrainSpins);  // the copy in flight lands before the block leaves
+    return false;
+  }
+  return true;
+}
+
+// forward: X column (1024 values) -> Y column (2048), Y[2k + s] from warp s
+__global__ void __launch_bounds__(kWpNT, 8) k_yfwd_p(const float2* __restrict__ X, float2* __restrict__ Y, DemagGeom g,
+                                                     const float2* __restrict__ twy, int nlines, unsigned spins) {
+  constexpr int NY = 1024, Py = 2048;
+  extern __shared__ __align__(128) float2 sp[];
+  float2* buf = sp;                                                          // NY
+  float2* tile = sp + NY + (threadIdx.x >> 5) * wtile_size<32>();           // this warp's
+  auto* bar = reinterpret_cast<unsigned long long*>(sp + NY + 2 * wtile_size<32>());
+  if (g.gate && !*g.gate) return;
+  int line = blockIdx.x;
+  if (line >= nlines) return;
+  const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    mbar_init(bar);
+    bulk_load(buf, X + static_cast<int64_t>(line) * NY, NY * sizeof(float2), bar);
+  }
+  __syncthreads();
+  for (unsigned it = 0; line < nlines; ++it, line += gridDim.x) {
+    if (!block_wait(bar, it & 1, spins)) return;
+    float2 v[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      float2 a = buf[lane + 32 * j];
+      if (s) a = cmul(a, __ldg(twy + lane + 32 * j));
+      v[j] = a;
+    }
+    __syncthreads();  // both warps hold the line: the buffer takes the next one
+    if (threadIdx.x == 0 && line + static_cast<int>(gridDim.x) < nlines)
+      bulk_load(buf, X + static_cast<int64_t>(line + gridDim.x) * NY, NY * sizeof(float2), bar);
+    wfft<32, false, 2>(v, tile, twy);
+    float2* yc = Y + static_cast<int64_t>(line) * Py + s;
+#pragma unroll
+    for (int r = 0; r < 32; ++r) yc[2 * (lane + 32 * r)] = v[r];
+  }
+}
+
+// inverse: Y column (2048 values) -> X column (y < 1024); warp s transforms
+// Y[2k + s] and the pair adds u0[y] + w^(-y) u1[y] through the warp tiles
+__global__ void __launch_bounds__(kWpNT, 6) k_yinv_p(const float2* __restrict__ Y, float2* __restrict__ X, DemagGeom g,
+                                                     const float2* __restrict__ twy, int nlines, unsigned spins) {
+  constexpr int NY = 1024, Py = 2048;
+  extern __shared__ __align__(128) float2 sp[];
+  float2* buf = sp;                                          // Py
+  float2* tiles = sp + Py;                                   // two warp tiles
+  auto* bar = reinterpret_cast<unsigned long long*>(sp + Py + 2 * wtile_size<32>());
+  if (g.gate && !*g.gate) return;
+  int line = blockIdx.x;
+  if (line >= nlines) return;
+  const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
+  float2* tile = tiles + s * wtile_size<32>();
+  const float2* pt = tiles + (s ^ 1) * wtile_size<32>();
+  if (threadIdx.x == 0) {
+    mbar_init(bar);
+    bulk_load(buf, Y + static_cast<int64_t>(line) * Py, Py * sizeof(float2), bar);
+  }
+  __syncthreads();
+  for (unsigned it = 0; line < nlines; ++it, line += gridDim.x) {
+    if (!block_wait(bar, it & 1, spins)) return;
+    float2 v[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = buf[2 * (lane + 32 * j) + s];
+    __syncthreads();  // both warps hold the line (and are done with last line's tiles)
+    if (threadIdx.x == 0 && line + static_cast<int>(gridDim.x) < nlines)
+      bulk_load(buf, Y + static_cast<int64_t>(line + gridDim.x) * Py, Py * sizeof(float2), bar);
+    wfft<32, true, 2>(v, tile, twy);
+    if (s) {
+#pragma unroll
+      for (int r = 0; r < 32; ++r) {
+        float2 w = __ldg(twy + lane + 32 * r);
+        w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    // y = lane + 32 r: warp s keeps r % 2 == s and sends the others
+#pragma unroll
+    for (int i = 0; i < 16; ++i) tile[i * 32 + lane] = s ? v[2 * i] : v[2 * i + 1];
+    __syncthreads();
+    float2* xo = X + static_cast<int64_t>(line) * NY;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const float2 a = s ? v[2 * i + 1] : v[2 * i], b = pt[i * 32 + lane];
+      xo[lane + 32 * (2 * i + s)] = make_float2(a.x + b.x, a.y + b.y);
+    }
+  }
+}
+
+constexpr size_t kYfpSmem = (1024 + 2 * wtile_size<32>()) * sizeof(float2) + 8;
+constexpr size_t kYipSmem = (2048 + 2 * wtile_size<32>()) * sizeof(float2) + 8;
+
+// The bulk-copy y passes for Q = 32 unless MMCUDA_YPIPE=0 (warp-direct ones)
+bool ypipe_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MMCUDA_YPIPE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+// resident blocks of a persistent pass on the current device
+int resident_blocks(const void* kernel, int nt, size_t smem) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, nt, smem);
+  return std::max(1, sms) * std::max(1, per);
+}
+
 template <int Q>
 void launch_q(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,
               const float2* twx, const float2* twy, cudaStream_t st) {
@@ -336,28 +496,30 @@ void launch_q(int which, const DemagGeom& g, const float* m, const float* Ms, fl
   const size_t ysm = static_cast<size_t>(8) * wtile_size<Q>() * sizeof(float2);
   switch (which) {
     case 0:
-      if (xwarps() == 4)
-        k_xfwd_w<Q, 4><<<3 * rows / x_rows<Q, 4>(), 128, x_smem<Q, 4>() * sizeof(float2), st>>>(m, Ms, X, g, twx);
-      else
-        k_xfwd_w<Q, 8><<<3 * rows / x_rows<Q, 8>(), 256, x_smem<Q, 8>() * sizeof(float2), st>>>(m, Ms, X, g, twx);
+      k_xfwd_w<Q, kXfW><<<3 * rows / x_rows<Q, kXfW>(), 32 * kXfW, x_smem<Q, kXfW>() * sizeof(float2), st>>>(m, Ms, X,
+                                                                                                         g, twx);
       break;
     case 1:
-      if (ydirect_enabled())
+      if (Q == 32 && ypipe_enabled()) {
+        static const int nb = resident_blocks(reinterpret_cast<const void*>(&k_yfwd_p), kWpNT, kYfpSmem);
+        k_yfwd_p<<<std::min(ylines, nb), kWpNT, kYfpSmem, st>>>(X, Y, g, twy, ylines, copy_wait_spins());
+      } else if (ydirect_enabled())
         k_yfwd_d<Q><<<(ylines + DL - 1) / DL, kWdNT, ysm, st>>>(X, Y, g, twy, ylines);
       else
         k_yfwd_w<Q><<<(ylines + NL - 1) / NL, kWyNT, ysm, st>>>(X, Y, g, twy, ylines);
       break;
     case 3:
-      if (ydirect_enabled())
+      if (Q == 32 && ypipe_enabled()) {
+        static const int nb = resident_blocks(reinterpret_cast<const void*>(&k_yinv_p), kWpNT, kYipSmem);
+        k_yinv_p<<<std::min(ylines, nb), kWpNT, kYipSmem, st>>>(Y, X, g, twy, ylines, copy_wait_spins());
+      } else if (ydirect_enabled())
         k_yinv_d<Q><<<(ylines + DL - 1) / DL, kWdNT, ysm, st>>>(Y, X, g, twy, ylines);
       else
         k_yinv_w<Q><<<(ylines + NL - 1) / NL, kWyNT, ysm, st>>>(Y, X, g, twy, ylines);
       break;
     case 4:
-      if (xwarps() == 4)
-        k_xinv_w<Q, 4><<<3 * rows / x_rows<Q, 4>(), 128, x_smem<Q, 4>() * sizeof(float2), st>>>(X, H, g, twx);
-      else
-        k_xinv_w<Q, 8><<<3 * rows / x_rows<Q, 8>(), 256, x_smem<Q, 8>() * sizeof(float2), st>>>(X, H, g, twx);
+      k_xinv_w<Q, kXiW><<<3 * rows / x_rows<Q, kXiW>(), 32 * kXiW, x_smem<Q, kXiW>() * sizeof(float2), st>>>(X, H, g,
+                                                                                                         twx);
       break;
     default:
       break;
@@ -371,14 +533,10 @@ void set_attrs_q() {
   cudaFuncSetAttribute(k_yinv_w<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   cudaFuncSetAttribute(k_yfwd_d<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   cudaFuncSetAttribute(k_yinv_d<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-  cudaFuncSetAttribute(k_xfwd_w<Q, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(x_smem<Q, 4>() * sizeof(float2)));
-  cudaFuncSetAttribute(k_xinv_w<Q, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(x_smem<Q, 4>() * sizeof(float2)));
-  cudaFuncSetAttribute(k_xfwd_w<Q, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(x_smem<Q, 8>() * sizeof(float2)));
-  cudaFuncSetAttribute(k_xinv_w<Q, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(x_smem<Q, 8>() * sizeof(float2)));
+  cudaFuncSetAttribute(k_xfwd_w<Q, kXfW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(x_smem<Q, kXfW>() * sizeof(float2)));
+  cudaFuncSetAttribute(k_xinv_w<Q, kXiW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(x_smem<Q, kXiW>() * sizeof(float2)));
 }
 
 int wq(int n) {
@@ -405,6 +563,14 @@ void wreg_set_attrs() {
   set_attrs_q<8>();
   set_attrs_q<16>();
   set_attrs_q<32>();
+}
+
+bool wreg_take_timeout() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_wreg_timeout, sizeof(int)) != cudaSuccess || !v) return false;
+  const int zero = 0;
+  cudaMemcpyToSymbol(g_wreg_timeout, &zero, sizeof(int));
+  return true;
 }
 
 void launch_wreg_f32(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,

@@ -10,13 +10,21 @@
 // so the pair of threads (s = 0, 1) of a line each run 16-point transforms on
 // 16 values a component held in registers, apply the tensor at their 16 kz,
 // and exchange half of their results once (shfl.xor 16).  Each thread issues
-// its 48 row loads up front; the block's tensor entries are prefetched into
-// shared memory (cp.async) meanwhile, with one barrier before the product.
+// its 48 row loads up front; the block's tensor entries arrive in shared
+// memory meanwhile -- by one tiled bulk copy through a tensor map
+// (cp.async.bulk.tensor, completion counted on an mbarrier; column-major
+// spectra) or by cp.async (row-major) -- with one barrier before the product.
 //
 // Lanes: t = lane & 15 is the line within the warp, s = lane >> 4 the half.
 // A block of 8 warps takes 128 consecutive lines along the fastest spectrum
 // index: ky of one kx column (column-major spectra, DemagGeom::yT) or kx of
 // one ky row (row-major).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstdlib>
+#include <cstring>
+
 #include "mm_demag.cuh"
 #include "mm_fft.cuh"
 #include "mm_launch.cuh"
@@ -37,15 +45,57 @@ constexpr int kZpTzq = 17;  // kz quadrant rows of Pz = 32
 // block's 128 lines (their ky mirror index, or kx, is one contiguous run)
 constexpr int kZpTensor = 6 * kZpTzq * kZpRow;
 
+// ky width of the tiled copy of a column-major block: its 128 lines map to a
+// contiguous run of at most 128 tensor rows (ascending, or descending past
+// Py / 2), which starts up to 3 entries after the 16-byte-aligned copy start
+static_assert(kZpRow >= kZpLines + 3, "tensor box holds the block's rows");
+constexpr unsigned kZpBoxBytes = 6u * kZpTzq * kZpRow * sizeof(float);
+constexpr unsigned kZpDrainSpins = 1u << 24;
+__device__ int g_zpair_timeout;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+// bounded wait of every thread of the block on the slice's mbarrier, with
+// one outcome for all; on a timeout the copy in flight is drained first
+__device__ __forceinline__ bool slice_wait(unsigned long long* bar, unsigned spins) {
+  const unsigned a = smem_addr(bar);
+  bool ok = false;
+  for (unsigned i = 0; i < spins && !ok; ++i) {
+    unsigned r;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(r)
+        : "r"(a)
+        : "memory");
+    ok = r != 0;
+  }
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(&g_zpair_timeout, 1);
+    for (unsigned i = 0; i < kZpDrainSpins; ++i) {
+      unsigned r;
+      asm volatile(
+          "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+          : "=r"(r)
+          : "r"(a)
+          : "memory");
+      if (r) break;
+    }
+    return false;
+  }
+  return true;
+}
+
 __device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
   const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(a), "l"(gmem));
 }
 
 template <bool YT>
-__global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, const float* __restrict__ Nhat, DemagGeom g) {
+__global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, const float* __restrict__ Nhat, DemagGeom g,
+                                                    const __grid_constant__ CUtensorMap tmap, unsigned spins) {
   using C = float2;
-  extern __shared__ __align__(16) float tn[];  // kZpTensor entries
+  extern __shared__ __align__(128) float tn[];  // kZpTensor entries, then the mbarrier (YT)
   if (g.gate && !*g.gate) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int t = lane & 15, s = lane >> 4;
@@ -61,23 +111,41 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
     kx = line;
   }
   const bool live = YT ? ky < Py : kx < Hx;
-  // Prefetch the block's tensor entries into shared memory (cp.async), in
-  // flight while the rows load and the forward transforms run: entry
-  // (c6, kzq) of block line l at tn[(c6 * 17 + kzq) * kZpRow + l], from the
-  // tensor row of line l's mirror index (ky or Py - ky, column-major) or kx.
-  // Thread (l, h) copies line l's entries of components 3h .. 3h + 2.
-  {
+  // The block's tensor entries: entry (c6, kzq) of block line l at
+  // tn[(c6 * 17 + kzq) * kZpRow + col(l)], from the tensor row of line l's
+  // mirror index (ky or Py - ky, column-major) or its kx, in flight while the
+  // rows load and the forward transforms run.
+  int col;           // this thread's line's column in the shared rows
+  unsigned long long* bar = nullptr;
+  if constexpr (YT) {
+    // one tiled bulk copy of the box {kZpRow ky, 1 kx, 17 kz, 6 c} starting
+    // at the 16-byte-aligned ky0 at or below the block's smallest row index
+    const int nl = min(kZpLines, Py - line0);
+    const int last = line0 + nl - 1;
+    const int kmin = last <= Py / 2 ? line0 : min(line0, Py - last);
+    const int ky0 = kmin & ~3;
+    col = (ky > Py / 2 ? Py - ky : ky) - ky0;
+    bar = reinterpret_cast<unsigned long long*>(tn + kZpTensor);
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(kZpBoxBytes)
+                   : "memory");
+      asm volatile(
+          "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+          "[%6];\n" ::"r"(smem_addr(tn)),
+          "l"(reinterpret_cast<unsigned long long>(&tmap)), "r"(ky0), "r"(kx), "r"(0), "r"(0), "r"(smem_addr(bar))
+          : "memory");
+    }
+    __syncthreads();  // the mbarrier is initialised before anyone waits on it
+  } else {
+    // cp.async: thread (l, h) copies line l's entries of components 3h .. 3h + 2
+    col = line - line0;
     const int l = threadIdx.x & (kZpLines - 1), h = threadIdx.x >> 7;
-    if (l < (YT ? Py : Hx) - line0) {
+    if (l < Hx - line0) {
       const int64_t Ts = static_cast<int64_t>(kZpTzq) * Tyq * Hx;  // component stride
       const int64_t kzs = static_cast<int64_t>(Tyq) * Hx;            // kz quadrant row stride
-      int64_t off;
-      if (YT) {
-        const int kyl = line0 + l;
-        off = static_cast<int64_t>(kx) * Tyq + (kyl > Py / 2 ? Py - kyl : kyl);
-      } else {
-        off = static_cast<int64_t>(ky > Py / 2 ? Py - ky : ky) * Hx + line0 + l;
-      }
+      const int64_t off = static_cast<int64_t>(ky > Py / 2 ? Py - ky : ky) * Hx + line0 + l;
       const float* src = Nhat + 3 * h * Ts + off;
       float* dst = tn + 3 * h * kZpTzq * kZpRow + l;
 #pragma unroll
@@ -114,17 +182,20 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
     }
     dft16<false>(v[c]);
   }
-  asm volatile("cp.async.wait_group 0;\n" ::);
-  __syncthreads();
+  if constexpr (YT) {
+    if (!slice_wait(bar, spins)) return;
+  } else {
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncthreads();
+  }
   // tensor product at kz = 2k + s (one quadrant stored; xy odd in ky, xz in
   // kz, yz in both): kz <= 15 for k < 8 (kzq = kz), kz >= 18 for k > 8
   // (kzq = 32 - kz, xz and yz negated), and k = 8 gives kz = 16 (s = 0) or
   // the mirrored 17 -> 15 (s = 1)
   if (live) {
     const float sy = ky > Py / 2 ? -1.f : 1.f;
-    const int l = line - line0;
-    const float* lo = tn + s * kZpRow + l;          // row s (+ 2k)
-    const float* hi = tn + (16 - s) * kZpRow + l;   // row 16 - s (+ 16 - 2k)
+    const float* lo = tn + s * kZpRow + col;          // row s (+ 2k)
+    const float* hi = tn + (16 - s) * kZpRow + col;   // row 16 - s (+ 16 - 2k)
     constexpr int cr = kZpTzq * kZpRow;             // component stride
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
@@ -170,16 +241,64 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
 
 bool zpair_applies(const DemagGeom& g) { return g.Pz == 32 && g.Tzq == kZpTzq && g.nz <= 16 && g.nz >= 1; }
 
-void launch_zpair_f32(const DemagGeom& g, float2* Y, const float* Nhat, cudaStream_t st) {
-  const size_t sm = sizeof(float) * kZpTensor;
+unsigned copy_wait_spins() {
+  static const unsigned v = [] {
+    const char* e = getenv("MMCUDA_COPY_SPINS");
+    return e ? static_cast<unsigned>(strtoul(e, nullptr, 10)) : (1u << 22);
+  }();
+  return v;
+}
+
+bool zpair_take_timeout() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_zpair_timeout, sizeof(int)) != cudaSuccess || !v) return false;
+  const int zero = 0;
+  cudaMemcpyToSymbol(g_zpair_timeout, &zero, sizeof(int));
+  return true;
+}
+
+// Nhat[((c*17 + kz)*Hx + kx)*Tys + ky] as a 4-D FP32 tensor (ky fastest,
+// extent Tyq: the zero padding up to Tys is never read), box {kZpRow, 1, 17, 6}
+bool zpair_tensor_map(const DemagGeom& g, const float* Nhat, void* map128) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }();
+  if (!encode || (g.Tys & 3) || (reinterpret_cast<uintptr_t>(Nhat) & 15)) return false;
+  const cuuint64_t dims[4] = {static_cast<cuuint64_t>(g.Tyq), static_cast<cuuint64_t>(g.Hx),
+                              static_cast<cuuint64_t>(kZpTzq), 6};
+  const cuuint64_t row = static_cast<cuuint64_t>(g.Tys) * sizeof(float);
+  const cuuint64_t strides[3] = {row, row * g.Hx, row * g.Hx * kZpTzq};
+  const cuuint32_t box[4] = {static_cast<cuuint32_t>(kZpRow), 1, static_cast<cuuint32_t>(kZpTzq), 6};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUtensorMap m;
+  std::memset(&m, 0, sizeof(m));
+  const CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(Nhat), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return false;
+  static_assert(sizeof(CUtensorMap) == 128, "tensor map size");
+  std::memcpy(map128, &m, sizeof(m));
+  return true;
+}
+
+void launch_zpair_f32(const DemagGeom& g, float2* Y, const float* Nhat, const void* map128, cudaStream_t st) {
+  CUtensorMap m;
+  std::memcpy(&m, map128, sizeof(m));
   if (g.yT) {
+    const size_t sm = sizeof(float) * kZpTensor + 16;  // + the mbarrier
     smem_optin(reinterpret_cast<const void*>(&k_zpair<true>));
     dim3 grid((g.Py + kZpLines - 1) / kZpLines, g.Hx, 1);
-    k_zpair<true><<<grid, kZpNT, sm, st>>>(Y, Nhat, g);
+    k_zpair<true><<<grid, kZpNT, sm, st>>>(Y, Nhat, g, m, copy_wait_spins());
   } else {
+    const size_t sm = sizeof(float) * kZpTensor;
     smem_optin(reinterpret_cast<const void*>(&k_zpair<false>));
     dim3 grid((g.Hx + kZpLines - 1) / kZpLines, g.Py, 1);
-    k_zpair<false><<<grid, kZpNT, sm, st>>>(Y, Nhat, g);
+    k_zpair<false><<<grid, kZpNT, sm, st>>>(Y, Nhat, g, m, copy_wait_spins());
   }
 }
 

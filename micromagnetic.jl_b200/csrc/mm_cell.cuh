@@ -96,13 +96,20 @@ template <typename R> struct TileNb {
   int cs, c0, sx, dm, dp;
 };
 
-template <typename R, bool ENERGY, bool EXTRA = false, bool TILE = false>
+// FIX != 0: the term set is the compile-time mask FIX and every parameter is
+// uniform (no A, D, Ku or Zeeman array), so the branches on terms that are
+// absent and on per-cell parameters compile away; FIX == 0 reads the mask.
+template <typename R, bool ENERGY, bool EXTRA = false, bool TILE = false, unsigned FIX = 0>
 __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __restrict__ y, int I, int i, int j,
                                           int k, R m[3], R h[3], double* e, const TileNb<R>& tn = TileNb<R>{}) {
   const int64_t N = a.N;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int nxy = nx * ny;
-  const unsigned mask = a.mask;
+  const unsigned mask = FIX ? FIX : a.mask;
+  const R* const pA = FIX ? nullptr : a.A;
+  const R* const pD = FIX ? nullptr : a.D;
+  const R* const pKu = FIX ? nullptr : a.Ku;
+  const R* const pHz = FIX ? nullptr : a.Hz;
   const bool local = (mask & (TB_EXCH | TB_DMI_BULK | TB_DMI_INTERFACIAL | TB_ANIS)) != 0 ||
                      (EXTRA && (mask & TB_STT_ZL));
   // Every load is issued before any use: neighbour indices are clamped to the
@@ -145,18 +152,18 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
     }
   }
   R An[6] = {R(0), R(0), R(0), R(0), R(0), R(0)}, AI = R(0);
-  if ((mask & TB_EXCH) && a.A) {
-    AI = a.A[I];
+  if ((mask & TB_EXCH) && pA) {
+    AI = pA[I];
 #pragma unroll
-    for (int d = 0; d < 6; ++d) An[d] = __ldg(a.A + nb[d]);
+    for (int d = 0; d < 6; ++d) An[d] = __ldg(pA + nb[d]);
   }
   R Dn[4] = {R(0), R(0), R(0), R(0)}, DI = a.D_uni;
-  if ((mask & TB_DMI_INTERFACIAL) && a.D) {
-    DI = a.D[I];
+  if ((mask & TB_DMI_INTERFACIAL) && pD) {
+    DI = pD[I];
 #pragma unroll
-    for (int d = 0; d < 4; ++d) Dn[d] = __ldg(a.D + nb[d]);
+    for (int d = 0; d < 4; ++d) Dn[d] = __ldg(pD + nb[d]);
   }
-  const R Ku = ((mask & TB_ANIS) && a.Ku) ? a.Ku[I] : a.Ku_uni;
+  const R Ku = ((mask & TB_ANIS) && pKu) ? pKu[I] : a.Ku_uni;
   R hd[3] = {R(0), R(0), R(0)};
   if (mask & TB_DEMAG) {
     hd[0] = a.Hd[I];
@@ -164,10 +171,10 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
     hd[2] = a.Hd[2 * N + I];
   }
   R zx = a.hz_x, zy = a.hz_y, zz = a.hz_z;  // uniform part plus the per-cell part
-  if ((mask & TB_ZEEMAN) && a.Hz) {
-    zx += a.Hz[I];
-    zy += a.Hz[N + I];
-    zz += a.Hz[2 * N + I];
+  if ((mask & TB_ZEEMAN) && pHz) {
+    zx += pHz[I];
+    zy += pHz[N + I];
+    zz += pHz[2 * N + I];
   }
 
   h[0] = h[1] = h[2] = R(0);
@@ -181,13 +188,13 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
     if (mask & TB_EXCH) {
       R fx = 0, fy = 0, fz = 0;
       const R coef[6] = {a.ex_x, a.ex_x, a.ex_y, a.ex_y, a.ex_z, a.ex_z};
-      const bool on = a.A ? (AI != R(0)) : true;
+      const bool on = pA ? (AI != R(0)) : true;
       if (on) {
 #pragma unroll
         for (int d = 0; d < 6; ++d) {
           if ((nbm >> d) & 1u) {
             R c = coef[d];
-            if (a.A) {
+            if (pA) {
               if (An[d] == R(0)) continue;
               const R Aeff = 2 * AI * An[d] / (AI + An[d]);
               c = Aeff * coef[d];
@@ -246,7 +253,7 @@ __device__ __forceinline__ void cell_heff(const FieldArgs<R>& a, const R* __rest
       for (int d = 0; d < 4; ++d) {
         if (!((nbm >> d) & 1u)) continue;
         R c;
-        if (a.D) {
+        if (pD) {
           if (Dn[d] == R(0)) continue;
           c = (2 * DI * Dn[d] / (DI + Dn[d])) * dd[d];
         } else {
@@ -454,7 +461,7 @@ __device__ __forceinline__ void rk4_update(const FieldArgs<R>& a, const StageArg
 // RK4 / Heun stage, one cell a thread and one z plane a block (k_stage's
 // SM_RK4 mode without the further terms) as a descriptor, so that batches can
 // merge it; blocks are 1-D, the cell tile bx x by comes with the arguments.
-template <typename R>
+template <typename R, unsigned FIX = 0>
 struct StagePlain {
   static constexpr int kNT = kStageThreads, kMinB = sizeof(R) == 4 ? 3 : 2;
   struct Args {
@@ -483,10 +490,18 @@ struct StagePlain {
       av[c] = s.stage > 1 ? s.acc[c * N + I] : R(0);
     }
     R m[3], h[3];
-    cell_heff<R, false, false>(a, args.y, I, i, j, k, m, h, nullptr);
+    cell_heff<R, false, false, false, FIX>(a, args.y, I, i, j, k, m, h, nullptr);
     rk4_update(a, s, I, m, h, mN, mL, av);
   }
 };
+
+// Term sets with a compiled stage kernel of their own (all parameters
+// uniform): exchange + demag (c5), + Zeeman (fig9, c1), exchange + bulk DMI +
+// anisotropy + demag (c2), exchange + interfacial DMI + demag (c3 films)
+constexpr unsigned kFixExDemag = TB_EXCH | TB_DEMAG;
+constexpr unsigned kFixExDemagZee = TB_EXCH | TB_DEMAG | TB_ZEEMAN;
+constexpr unsigned kFixExBulkAnisDemag = TB_EXCH | TB_DMI_BULK | TB_ANIS | TB_DEMAG;
+constexpr unsigned kFixExIntDemag = TB_EXCH | TB_DMI_INTERFACIAL | TB_DEMAG;
 
 template <typename R> struct PersistKind<StagePlain<R>> { static constexpr int value = 11; };
 

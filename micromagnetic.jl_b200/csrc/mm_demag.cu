@@ -33,6 +33,31 @@ static int ilog2(int v) {
 
 // Shared-memory budget of one strided-pass block; the kx tile W is the
 // largest power of two (up to 128 bytes of row segment) that fits.
+// Multiprocessors of the current device (cached on first use)
+static int sm_count() {
+  static const int v = [] {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+  }();
+  return v;
+}
+
+// Lines a shared-memory x-pass block transforms: as many as fill its tile
+// (cap / Lc), but for a mesh launched alone no more than spread `lines` over
+// two blocks an SM -- on small meshes (c1: 150 lines of 200 points) more,
+// shorter blocks finish sooner than a few full ones.  A pass recorded for a
+// batch keeps full tiles: its launch covers the lines of every mesh.  Each
+// line's arithmetic is the same whatever block it lands in.
+template <typename R, int NT>
+static int x_lines_per_block(int lines, int Lc) {
+  const int full = std::max(1, PassCfg<R, NT>::cap / Lc);
+  if (launch_recorder()) return full;
+  const int spread = std::max(1, (lines + 2 * sm_count() - 1) / (2 * sm_count()));
+  return std::min(full, spread);
+}
+
 static int smem_budget_bytes() {
   static int v = [] {
     const char* e = getenv("MMCUDA_LINES_SMEM_KB");
@@ -884,7 +909,7 @@ static void launch_fwd_x(const DemagGeom& g, const R* m, const R* Ms, const doub
     k_fwd_x1<R, MODE><<<(lines + 255) / 256, 256, 0, st>>>(m, Ms, Tr, X, rows, lines, g.gate);
     return;
   }
-  const int nl = std::max(1, PassCfg<R, NT>::cap / g.Lc);
+  const int nl = x_lines_per_block<R, NT>(lines, g.Lc);
   const int blocks = (lines + nl - 1) / nl;
   const int half = nl * (g.Lc | 1);
   const size_t sm = 2 * sizeof(C) * half;
@@ -1169,7 +1194,7 @@ static bool run_pass(const DemagPlan<R>& p, DemagGeom g, int which, const R* m, 
       if (g.Px == 1) {
         k_inv_x1<R><<<(lines + 255) / 256, 256, 0, st>>>(p.X, Hd, lines, g.gate);
       } else {
-        const int nl = std::max(1, PassCfg<R, NT>::cap / g.Lc);
+        const int nl = x_lines_per_block<R, NT>(lines, g.Lc);
         const int half = nl * (g.Lc | 1);
         const size_t sm = 2 * sizeof(C) * half;
         launch_k<InvX<R, NT>>(dim3((lines + nl - 1) / nl), sm, st, {p.X, Hd, g, lines, nl, p.twx, half, make_fastdiv(nl), dim3()});

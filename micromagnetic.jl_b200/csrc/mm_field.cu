@@ -357,6 +357,20 @@ static bool stage_tile_enabled() {
   return on;
 }
 
+// The compiled term sets of the RK4 / Heun stage unless MMCUDA_STAGE_FIX=0
+static bool stage_fix_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MMCUDA_STAGE_FIX");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+template <typename R, unsigned FIX>
+typename StagePlain<R, FIX>::Args fix_args(const typename StagePlain<R>::Args& a) {
+  return {a.a, a.y, a.s, a.bx, a.by, a.grid};
+}
+
 template <typename R>
 bool stage_descriptor_used(const FieldArgs<R>& fa) {
   return !((fa.mask & kExtraBits) || ((fa.mask & TB_DMI_BULK) && fa.x.bD[0]));
@@ -384,7 +398,20 @@ void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<
     return;
   }
   if (mode == SM_RK4) {
-    launch_k<StagePlain<R>>(g.grid, 0, st, {fa, y, sa, static_cast<int>(g.block.x), static_cast<int>(g.block.y), dim3()});
+    const typename StagePlain<R>::Args args{fa, y, sa, static_cast<int>(g.block.x), static_cast<int>(g.block.y), dim3()};
+    // a compiled term set when the handle's terms are exactly one of them
+    // with uniform parameters (MMCUDA_STAGE_FIX=0 keeps the general kernel)
+    const bool uni = !fa.A && !fa.D && !fa.Ku && !fa.Hz && stage_fix_enabled();
+    const unsigned fx = uni ? fa.mask : 0u;
+    switch (fx) {
+      case kFixExDemag: launch_k<StagePlain<R, kFixExDemag>>(g.grid, 0, st, fix_args<R, kFixExDemag>(args)); break;
+      case kFixExDemagZee: launch_k<StagePlain<R, kFixExDemagZee>>(g.grid, 0, st, fix_args<R, kFixExDemagZee>(args)); break;
+      case kFixExBulkAnisDemag:
+        launch_k<StagePlain<R, kFixExBulkAnisDemag>>(g.grid, 0, st, fix_args<R, kFixExBulkAnisDemag>(args));
+        break;
+      case kFixExIntDemag: launch_k<StagePlain<R, kFixExIntDemag>>(g.grid, 0, st, fix_args<R, kFixExIntDemag>(args)); break;
+      default: launch_k<StagePlain<R>>(g.grid, 0, st, args); break;
+    }
     return;
   }
   switch (mode) {

@@ -85,14 +85,19 @@ __global__ void __launch_bounds__(32 * W) k_xfwd_w(const float* __restrict__ m, 
   for (int r = 0; r < 32; ++r) sm[(q + Q * (r / Q) + 32 * (r % Q)) * S + rl] = v[r];
   __syncthreads();
   // X[k] = E + w_Px^k O, E = (Z[k] + conj Z[Lc-k]) / 2, O = (Z[k] - conj Z[Lc-k]) / 2i
-  for (int e = threadIdx.x; e < Hx * RB; e += 32 * W) {
-    const int k = e / RB, r = e - k * RB;
-    const float2 zk = sm[(k == L ? 0 : k) * S + r];
-    float2 zc = sm[(k == 0 ? 0 : L - k) * S + r];
+  // (Z is L-periodic: k = L reads Z[0]).  Thread (k0, r) writes row r of
+  // k = k0, k0 + KS, ... through a pointer stepped by KS columns.
+  constexpr int KS = 32 * W / RB;
+  const int r = threadIdx.x & (RB - 1), k0 = threadIdx.x / RB;
+  const int64_t step = static_cast<int64_t>(KS) * rows;
+  float2* xp = X + (static_cast<int64_t>(c) * Hx + k0) * rows + row0 + r;
+  for (int k = k0; k < Hx; k += KS, xp += step) {
+    const float2 zk = sm[(k & (L - 1)) * S + r];
+    float2 zc = sm[((L - k) & (L - 1)) * S + r];
     zc.y = -zc.y;
     const float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
     const float2 od = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
-    X[(static_cast<int64_t>(c) * Hx + k) * rows + row0 + r] = cadd(ev, cmul(__ldg(twx + k), od));
+    *xp = cadd(ev, cmul(__ldg(twx + k), od));
   }
 }
 
@@ -111,9 +116,22 @@ __global__ void __launch_bounds__(32 * W, 24 / W) k_xinv_w(const float2* __restr
   const int line0 = blockIdx.x * RB;
   const int c = line0 / rows, row0 = line0 - c * rows;
   const int rl = warp * (32 / Q) + gq;
-  for (int e = threadIdx.x; e < Hx * RB; e += 32 * W) {
-    const int k = e / RB, r = e - k * RB;
-    sm[k * S + r] = X[(static_cast<int64_t>(c) * Hx + k) * rows + row0 + r];
+  {
+    // thread (k0, r) stages row r of k = k0, k0 + KS, ..., eight loads in
+    // flight at a time
+    constexpr int KS = 32 * W / RB, U = 8;
+    const int r = threadIdx.x & (RB - 1), k0 = threadIdx.x / RB;
+    const int64_t step = static_cast<int64_t>(KS) * rows;
+    const float2* xp = X + (static_cast<int64_t>(c) * Hx + k0) * rows + row0 + r;
+    float2* sp = sm + k0 * S + r;
+    for (int kb = k0; kb < Hx; kb += U * KS, xp += U * step, sp += U * KS * S) {
+      float2 t[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) t[u] = kb + u * KS < Hx ? xp[u * step] : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (kb + u * KS < Hx) sp[u * KS * S] = t[u];
+    }
   }
   __syncthreads();
   // Z'[k] = (A + B) + i (A - B) conj(w_Px^k), A = X[k], B = conj X[Lc - k]
@@ -411,9 +429,17 @@ __global__ void __launch_bounds__(kWpNT, 8) k_yfwd_p(const float2* __restrict__ 
     if (threadIdx.x == 0 && line + static_cast<int>(gridDim.x) < nlines)
       bulk_load(buf, X + static_cast<int64_t>(line + gridDim.x) * NY, NY * sizeof(float2), bar);
     wfft<32, false, 2>(v, tile, twy);
-    float2* yc = Y + static_cast<int64_t>(line) * Py + s;
+    // the two parities interleave in the tiles' space (2048 values), which
+    // the block then writes as 16-byte pairs (Y[2k], Y[2k + 1])
+    __syncthreads();
+    float2* stg = sp + NY;
 #pragma unroll
-    for (int r = 0; r < 32; ++r) yc[2 * (lane + 32 * r)] = v[r];
+    for (int r = 0; r < 32; ++r) stg[2 * (lane + 32 * r) + s] = v[r];
+    __syncthreads();
+    const float4* st4 = reinterpret_cast<const float4*>(stg);
+    float4* y4 = reinterpret_cast<float4*>(Y + static_cast<int64_t>(line) * Py);
+#pragma unroll
+    for (int i = 0; i < Py / 2 / kWpNT; ++i) y4[threadIdx.x + kWpNT * i] = st4[threadIdx.x + kWpNT * i];
   }
 }
 
@@ -467,6 +493,7 @@ __global__ void __launch_bounds__(kWpNT, 6) k_yinv_p(const float2* __restrict__ 
   }
 }
 
+static_assert(2 * wtile_size<32>() >= 2048, "the forward pass stages a padded line in its warp tiles");
 constexpr size_t kYfpSmem = (1024 + 2 * wtile_size<32>()) * sizeof(float2) + 8;
 constexpr size_t kYipSmem = (2048 + 2 * wtile_size<32>()) * sizeof(float2) + 8;
 

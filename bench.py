@@ -742,7 +742,7 @@ def run_dopri(args, w, wname, n, forms, rank, ws, device, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=150)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default="c5", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(ADJOINT))
     ap.add_argument("--impl", default="native", choices=["native", "reference"])

@@ -117,21 +117,17 @@ __global__ void __launch_bounds__(32 * W, 24 / W) k_xinv_w(const float2* __restr
   const int c = line0 / rows, row0 = line0 - c * rows;
   const int rl = warp * (32 / Q) + gq;
   {
-    // thread (k0, r) stages row r of k = k0, k0 + KS, ..., eight loads in
-    // flight at a time
-    constexpr int KS = 32 * W / RB, U = 8;
+    // thread (k0, r) stages row r of k = k0, k0 + KS, ... with cp.async, so
+    // that all of its copies are in flight at once without holding registers
+    constexpr int KS = 32 * W / RB;
     const int r = threadIdx.x & (RB - 1), k0 = threadIdx.x / RB;
     const int64_t step = static_cast<int64_t>(KS) * rows;
     const float2* xp = X + (static_cast<int64_t>(c) * Hx + k0) * rows + row0 + r;
-    float2* sp = sm + k0 * S + r;
-    for (int kb = k0; kb < Hx; kb += U * KS, xp += U * step, sp += U * KS * S) {
-      float2 t[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) t[u] = kb + u * KS < Hx ? xp[u * step] : make_float2(0.f, 0.f);
-#pragma unroll
-      for (int u = 0; u < U; ++u)
-        if (kb + u * KS < Hx) sp[u * KS * S] = t[u];
-    }
+    unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(sm + k0 * S + r));
+    for (int k = k0; k < Hx; k += KS, xp += step, sa += KS * S * sizeof(float2))
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(xp) : "memory");
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   }
   __syncthreads();
   // Z'[k] = (A + B) + i (A - B) conj(w_Px^k), A = X[k], B = conj X[Lc - k]

@@ -91,7 +91,9 @@ __device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(a), "l"(gmem));
 }
 
-template <bool YT>
+// FULL: nz = 16 and every line of every block is live (column-major, Py a
+// multiple of 128), so no load or store is predicated
+template <bool YT, bool FULL>
 __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, const float* __restrict__ Nhat, DemagGeom g,
                                                     const __grid_constant__ CUtensorMap tmap, unsigned spins) {
   using C = float2;
@@ -110,7 +112,7 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
     ky = blockIdx.y;
     kx = line;
   }
-  const bool live = YT ? ky < Py : kx < Hx;
+  const bool live = FULL || (YT ? ky < Py : kx < Hx);
   // The block's tensor entries: entry (c6, kzq) of block line l at
   // tn[(c6 * 17 + kzq) * kZpRow + col(l)], from the tensor row of line l's
   // mirror index (ky or Py - ky, column-major) or its kx, in flight while the
@@ -169,7 +171,12 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
-    for (int n = 0; n < 16; ++n) v[c][n] = (live && n < nz) ? Y[c * cs + n * zs + base] : make_float2(0.f, 0.f);
+    for (int n = 0; n < 16; ++n) {
+      if constexpr (FULL)
+        v[c][n] = Y[c * cs + n * zs + base];
+      else
+        v[c][n] = (live && n < nz) ? Y[c * cs + n * zs + base] : make_float2(0.f, 0.f);
+    }
   // forward: x[n] w32^(n s), DFT16 -> X[2k + s]
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -191,48 +198,66 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
   // tensor product at kz = 2k + s (one quadrant stored; xy odd in ky, xz in
   // kz, yz in both): kz <= 15 for k < 8 (kzq = kz), kz >= 18 for k > 8
   // (kzq = 32 - kz, xz and yz negated), and k = 8 gives kz = 16 (s = 0) or
-  // the mirrored 17 -> 15 (s = 1)
+  // the mirrored 17 -> 15 (s = 1).  The odd half also takes (-1)^k, which
+  // rotates its inverse transform by 8: register r then holds u1[(r + 8) % 16]
+  // and both halves keep registers 0..7 and send 8..15 (no selects).
   if (live) {
     const float sy = ky > Py / 2 ? -1.f : 1.f;
+    const float so = s ? -1.f : 1.f, syo = sy * so;
     const float* lo = tn + s * kZpRow + col;          // row s (+ 2k)
     const float* hi = tn + (16 - s) * kZpRow + col;   // row 16 - s (+ 16 - 2k)
     constexpr int cr = kZpTzq * kZpRow;             // component stride
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
       const float* tb = k < 8 ? lo + 2 * k * kZpRow : hi + (16 - 2 * k) * kZpRow;
-      const float sz = k < 8 ? 1.f : (k > 8 ? -1.f : (s ? -1.f : 1.f));
-      const float xx = tb[0], yy = tb[cr], zz = tb[2 * cr];
-      const float xy = sy * tb[3 * cr], xz = sz * tb[4 * cr], yz = sy * sz * tb[5 * cr];
+      float xx = tb[0], yy = tb[cr], zz = tb[2 * cr], xy, xz, yz;
+      if (k & 1) {  // odd k: never 8, so the kz sign is fixed
+        const float szk = k < 8 ? 1.f : -1.f;
+        xx *= so;
+        yy *= so;
+        zz *= so;
+        xy = syo * tb[3 * cr];
+        xz = (szk * so) * tb[4 * cr];
+        yz = (syo * szk) * tb[5 * cr];
+      } else {
+        const float sz = k < 8 ? 1.f : (k > 8 ? -1.f : (s ? -1.f : 1.f));
+        xy = sy * tb[3 * cr];
+        xz = sz * tb[4 * cr];
+        yz = sy * sz * tb[5 * cr];
+      }
       const C p0 = v[0][k], p1 = v[1][k], p2 = v[2][k];
       v[0][k] = make_float2(xx * p0.x + xy * p1.x + xz * p2.x, xx * p0.y + xy * p1.y + xz * p2.y);
       v[1][k] = make_float2(xy * p0.x + yy * p1.x + yz * p2.x, xy * p0.y + yy * p1.y + yz * p2.y);
       v[2][k] = make_float2(xz * p0.x + yz * p1.x + zz * p2.x, xz * p0.y + yz * p1.y + zz * p2.y);
     }
   }
-  // inverse: u_s = DFT16^-1(X[2k + s]); the odd half is twiddled by w32^(-n)
+  // inverse: u_s = DFT16^-1(X[2k + s]); the odd half (rotated by 8) is
+  // twiddled by w32^(-n), n = (r + 8) % 16 in register r
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     dft16<true>(v[c]);
     if (s) {
 #pragma unroll
-      for (int n = 1; n < 16; ++n) {
+      for (int r = 0; r < 16; ++r) {
+        const int n = (r + 8) & 15;
+        if (n == 0) continue;
         const float wr = static_cast<float>(w32_cs(n, 0)), wi = static_cast<float>(w32_cs(n, 1));
-        v[c][n] = cmul(v[c][n], make_float2(wr, wi));
+        v[c][r] = cmul(v[c][r], make_float2(wr, wi));
       }
     }
   }
-  // y[n] = u0[n] + w32^(-n) u1[n]: the s = 0 thread keeps n < 8, the s = 1
-  // thread n >= 8; each sends the other half to its partner (lane ^ 16)
+  // y[z] = u0[z] + w32^(-z) u1[z]: the s = 0 thread keeps z < 8 (registers
+  // 0..7 of u0), the s = 1 thread z >= 8 (registers 0..7 of the rotated u1);
+  // each sends registers 8..15 to its partner (lane ^ 16)
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const C mine = s ? v[c][8 + i] : v[c][i];
-      const C send = s ? v[c][i] : v[c][8 + i];
+      const C mine = v[c][i], send = v[c][8 + i];
       const float rx = __shfl_xor_sync(0xffffffffu, send.x, 16);
       const float ry = __shfl_xor_sync(0xffffffffu, send.y, 16);
       const int z = i + 8 * s;
-      if (live && z < nz) Y[c * cs + z * zs + base] = make_float2(mine.x + rx, mine.y + ry);
+      if (FULL || (live && z < nz)) Y[c * cs + z * zs + base] = make_float2(mine.x + rx, mine.y + ry);
     }
   }
 }
@@ -291,14 +316,19 @@ void launch_zpair_f32(const DemagGeom& g, float2* Y, const float* Nhat, const vo
   std::memcpy(&m, map128, sizeof(m));
   if (g.yT) {
     const size_t sm = sizeof(float) * kZpTensor + 16;  // + the mbarrier
-    smem_optin(reinterpret_cast<const void*>(&k_zpair<true>));
     dim3 grid((g.Py + kZpLines - 1) / kZpLines, g.Hx, 1);
-    k_zpair<true><<<grid, kZpNT, sm, st>>>(Y, Nhat, g, m, copy_wait_spins());
+    if (g.nz == 16 && g.Py % kZpLines == 0) {
+      smem_optin(reinterpret_cast<const void*>(&k_zpair<true, true>));
+      k_zpair<true, true><<<grid, kZpNT, sm, st>>>(Y, Nhat, g, m, copy_wait_spins());
+    } else {
+      smem_optin(reinterpret_cast<const void*>(&k_zpair<true, false>));
+      k_zpair<true, false><<<grid, kZpNT, sm, st>>>(Y, Nhat, g, m, copy_wait_spins());
+    }
   } else {
     const size_t sm = sizeof(float) * kZpTensor;
-    smem_optin(reinterpret_cast<const void*>(&k_zpair<false>));
+    smem_optin(reinterpret_cast<const void*>(&k_zpair<false, false>));
     dim3 grid((g.Hx + kZpLines - 1) / kZpLines, g.Py, 1);
-    k_zpair<false><<<grid, kZpNT, sm, st>>>(Y, Nhat, g, m, copy_wait_spins());
+    k_zpair<false, false><<<grid, kZpNT, sm, st>>>(Y, Nhat, g, m, copy_wait_spins());
   }
 }
 

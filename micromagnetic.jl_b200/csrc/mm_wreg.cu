@@ -91,6 +91,7 @@ __global__ void __launch_bounds__(32 * W) k_xfwd_w(const float* __restrict__ m, 
   const int r = threadIdx.x & (RB - 1), k0 = threadIdx.x / RB;
   const int64_t step = static_cast<int64_t>(KS) * rows;
   float2* xp = X + (static_cast<int64_t>(c) * Hx + k0) * rows + row0 + r;
+#pragma unroll 4
   for (int k = k0; k < Hx; k += KS, xp += step) {
     const float2 zk = sm[(k & (L - 1)) * S + r];
     float2 zc = sm[((L - k) & (L - 1)) * S + r];
@@ -118,14 +119,16 @@ __global__ void __launch_bounds__(32 * W, 24 / W) k_xinv_w(const float2* __restr
   const int rl = warp * (32 / Q) + gq;
   {
     // thread (k0, r) stages row r of k = k0, k0 + KS, ... with cp.async, so
-    // that all of its copies are in flight at once without holding registers
+    // that all of its copies are in flight at once without holding registers;
+    // each miss fetches 256 bytes into L2 (the column segments of the next
+    // three blocks, which run alongside this one)
     constexpr int KS = 32 * W / RB;
     const int r = threadIdx.x & (RB - 1), k0 = threadIdx.x / RB;
     const int64_t step = static_cast<int64_t>(KS) * rows;
     const float2* xp = X + (static_cast<int64_t>(c) * Hx + k0) * rows + row0 + r;
     unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(sm + k0 * S + r));
     for (int k = k0; k < Hx; k += KS, xp += step, sa += KS * S * sizeof(float2))
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(xp) : "memory");
+      asm volatile("cp.async.ca.shared.global.L2::256B [%0], [%1], 8;\n" ::"r"(sa), "l"(xp) : "memory");
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   }

@@ -422,6 +422,19 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def fp64_kernels(res, peak):
+    """The FP64 form's per-kernel CUDA-event times and its step's fraction of
+    the measured bandwidth (absent in --quick runs)."""
+    kern = res.get("kernels")
+    if not kern:
+        return {}
+    step = kern.get("rk4_step", {})
+    return {"step_roofline": {"alg_bytes": step.get("alg_bytes"), "ms": step.get("ms"), "GBps": step.get("GBps"),
+                              "frac": (step.get("GBps") or 0) / peak},
+            "kernels": {k: {"ms": round(v["ms"], 5), "GBps": round(v["GBps"] or 0, 1), "frac": round((v["GBps"] or 0) / peak, 3)}
+                        for k, v in kern.items()}}
+
+
 def profiled_traffic(wname, form_name):
     """ncu DRAM bytes per launch of each kernel, from the committed summary."""
     try:
@@ -640,7 +653,8 @@ def run_native(args):
             "fp64": ({"value": evals * results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
                       "fp32_over_fp64": r["value"] / results["fp64"]["value"],
                       "fp32_rel_err_vs_fp64": fp32_err, "err_after_steps": args.warmup + args.steps,
-                      "fp32_rel_err_vs_fp64_50_steps": fp32_err_50}
+                      "fp32_rel_err_vs_fp64_50_steps": fp32_err_50,
+                      **fp64_kernels(results["fp64"], peak)}
                      if "fp64" in results else None),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "peak_kind": peak_kind,

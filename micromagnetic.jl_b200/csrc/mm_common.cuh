@@ -24,6 +24,36 @@ template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
   return cmk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 template <typename C> __device__ __forceinline__ C cconj(C a) { return cmk<C>(a.x, -a.y); }
+
+// ------------------------------------------- programmatic dependent launch --
+// The kernels of an RK step follow one another on one stream, each reading
+// what the previous one wrote.  Launched with the programmatic-serialisation
+// attribute (launch_pdl), a kernel may be launched as the previous kernel's
+// blocks exit, before that grid's completion has been processed; pdl_enter(),
+// the first statement of every such kernel, waits until the previous grid has
+// completed and its writes are visible.  A grid is therefore complete only
+// after its predecessor is.  (No block triggers its dependents early: blocks
+// of the next kernel made resident during a pass's last wave, waiting there,
+// made every multi-wave workload slower.)  Kernels without pdl_enter() are
+// launched the ordinary way; in one launched without the attribute the wait
+// returns at once.
+__device__ __forceinline__ void pdl_enter() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+// MMCUDA_PDL=0 launches every kernel the ordinary way (default: on).
+bool pdl_enabled();
+template <typename... KA, typename... A>
+cudaError_t launch_pdl(void (*kern)(KA...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KA>(args)...);
+}
 template <typename C, typename R> __device__ __forceinline__ C cscale(C a, R s) { return cmk<C>(a.x * s, a.y * s); }
 // multiply by (sgn * i): sgn = -1 for the forward transform, +1 for the inverse
 template <bool INV, typename C> __device__ __forceinline__ C crot(C a) {

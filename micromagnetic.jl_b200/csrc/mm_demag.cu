@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(NT, (zconv2_minb<R, NT>())) k_zconv2(cplx_t<R>
   constexpr int L = RA * RB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* a = reinterpret_cast<C*>(smem_raw);
+  pdl_enter();
   if (g.gate && !*g.gate) return;
   const int LS = L | 1, Hx = g.Hx, Py = g.Py, nz = g.nz;
   const int W = 1 << lgW;
@@ -447,6 +448,14 @@ int newell_tensor_device(int nx, int ny, int nz, double dx, double dy, double dz
 LaunchRecorder*& launch_recorder() {
   thread_local LaunchRecorder* r = nullptr;
   return r;
+}
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MMCUDA_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }
 
 void smem_optin(const void* kernel) {
@@ -1040,9 +1049,9 @@ static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const
   if (g.yT) {
     dim3 grid(g.Hx, (g.Py + W - 1) / W, 1);
     if (offsets_fit_int(g))
-      k_zconv2<R, RA, RB, NTZ, true, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz, g.Hx);
+      launch_pdl(k_zconv2<R, RA, RB, NTZ, true, true>, grid, dim3(NTZ), sm, st, Y, Nhat, g, ilog2(W), fnl, twz, g.Hx);
     else
-      k_zconv2<R, RA, RB, NTZ, false, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz, g.Hx);
+      launch_pdl(k_zconv2<R, RA, RB, NTZ, false, true>, grid, dim3(NTZ), sm, st, Y, Nhat, g, ilog2(W), fnl, twz, g.Hx);
     return;
   }
   // full kx tiles; up to W/4 leftover columns run as ky tiles in the same grid
@@ -1051,9 +1060,9 @@ static void launch_zconv2(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const
   const int ncols = nfull * W >= g.Hx ? 0 : g.Hx - nfull * W;
   dim3 grid(nfull + ncols, g.Py, 1);
   if (offsets_fit_int(g))
-    k_zconv2<R, RA, RB, NTZ, true><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz, nfull);
+    launch_pdl(k_zconv2<R, RA, RB, NTZ, true>, grid, dim3(NTZ), sm, st, Y, Nhat, g, ilog2(W), fnl, twz, nfull);
   else
-    k_zconv2<R, RA, RB, NTZ, false><<<grid, NTZ, sm, st>>>(Y, Nhat, g, ilog2(W), fnl, twz, nfull);
+    launch_pdl(k_zconv2<R, RA, RB, NTZ, false>, grid, dim3(NTZ), sm, st, Y, Nhat, g, ilog2(W), fnl, twz, nfull);
 }
 
 // Power-of-two z lengths with a fused-middle kernel: L = RA * RB

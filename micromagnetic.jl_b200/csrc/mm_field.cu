@@ -94,6 +94,7 @@ const RkTableau& rk_tableau(int method) { return h_rk[method]; }
 template <typename R, int MODE, bool EXTRA>
 __global__ void __launch_bounds__(kStageThreads, sizeof(R) == 4 ? 3 : 2) k_stage(FieldArgs<R> a, const R* __restrict__ y, StageArgs<R> s) {
   constexpr bool kF32 = sizeof(R) == 4;
+  pdl_enter();
   if (MODE == SM_DOPRI && !s.ctrl->active) return;
   const int64_t N = a.N;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -382,11 +383,11 @@ void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<
   // handles without the extra terms run the kernel compiled without them
   if ((fa.mask & kExtraBits) || ((fa.mask & TB_DMI_BULK) && fa.x.bD[0])) {
     switch (mode) {
-      case SM_FIELD: k_stage<R, SM_FIELD, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-      case SM_RHS: k_stage<R, SM_RHS, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-      case SM_RK4: k_stage<R, SM_RK4, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-      case SM_ENERGY: k_stage<R, SM_ENERGY, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-      default: k_stage<R, SM_DOPRI, true><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+      case SM_FIELD: launch_pdl(k_stage<R, SM_FIELD, true>, g.grid, g.block, 0, st, fa, y, sa); break;
+      case SM_RHS: launch_pdl(k_stage<R, SM_RHS, true>, g.grid, g.block, 0, st, fa, y, sa); break;
+      case SM_RK4: launch_pdl(k_stage<R, SM_RK4, true>, g.grid, g.block, 0, st, fa, y, sa); break;
+      case SM_ENERGY: launch_pdl(k_stage<R, SM_ENERGY, true>, g.grid, g.block, 0, st, fa, y, sa); break;
+      default: launch_pdl(k_stage<R, SM_DOPRI, true>, g.grid, g.block, 0, st, fa, y, sa); break;
     }
     return;
   }
@@ -415,10 +416,10 @@ void launch_stage(int mode, const FieldArgs<R>& fa, const R* y, const StageArgs<
     return;
   }
   switch (mode) {
-    case SM_FIELD: k_stage<R, SM_FIELD, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-    case SM_RHS: k_stage<R, SM_RHS, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-    case SM_ENERGY: k_stage<R, SM_ENERGY, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
-    default: k_stage<R, SM_DOPRI, false><<<g.grid, g.block, 0, st>>>(fa, y, sa); break;
+    case SM_FIELD: launch_pdl(k_stage<R, SM_FIELD, false>, g.grid, g.block, 0, st, fa, y, sa); break;
+    case SM_RHS: launch_pdl(k_stage<R, SM_RHS, false>, g.grid, g.block, 0, st, fa, y, sa); break;
+    case SM_ENERGY: launch_pdl(k_stage<R, SM_ENERGY, false>, g.grid, g.block, 0, st, fa, y, sa); break;
+    default: launch_pdl(k_stage<R, SM_DOPRI, false>, g.grid, g.block, 0, st, fa, y, sa); break;
   }
 }
 

@@ -17,16 +17,20 @@
 #include <cstring>
 #include <vector>
 
+#include "mm_common.cuh"
+
 namespace mm {
 
 template <class K>
 __global__ void __launch_bounds__(K::kNT, K::kMinB) k_one(const typename K::Args a) {
+  pdl_enter();
   K::body(a, blockIdx);
 }
 
 template <class K>
 __global__ void __launch_bounds__(K::kNT, K::kMinB) k_many(const typename K::Args* __restrict__ A,
                                                            const int* __restrict__ begins, int n) {
+  pdl_enter();
   int lo = 0, hi = n - 1;
   const int b = static_cast<int>(blockIdx.x);
   while (lo < hi) {
@@ -84,6 +88,8 @@ void smem_optin(const void* kernel);
 template <class K>
 cudaError_t launch_many(const void* args_dev, const int* begins_dev, int n, int blocks, size_t smem, cudaStream_t st) {
   if (smem > 48 * 1024) smem_optin(reinterpret_cast<const void*>(&k_many<K>));
+  // an ordinary launch: with the programmatic attribute the merged NEB batch
+  // (32 images of 128 x 128, 16 launches a step) took 0.42 ms a step, not 0.36
   k_many<K><<<blocks, K::kNT, smem, st>>>(static_cast<const typename K::Args*>(args_dev), begins_dev, n);
   return cudaGetLastError();
 }
@@ -106,7 +112,7 @@ void launch_k(dim3 grid, size_t smem, cudaStream_t st, typename K::Args a) {
     return;
   }
   if (smem > 48 * 1024) smem_optin(reinterpret_cast<const void*>(&k_one<K>));
-  k_one<K><<<grid, K::kNT, smem, st>>>(a);
+  launch_pdl(k_one<K>, grid, dim3(K::kNT), smem, st, a);
 }
 
 }  // namespace mm

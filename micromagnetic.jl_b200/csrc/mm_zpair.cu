@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(kZpNT, 2) k_zpair(float2* __restrict__ Y, cons
                                                     const __grid_constant__ CUtensorMap tmap, unsigned spins) {
   using C = float2;
   extern __shared__ __align__(128) float tn[];  // kZpTensor entries, then the mbarrier (YT)
+  pdl_enter();
   if (g.gate && !*g.gate) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int t = lane & 15, s = lane >> 4;
@@ -319,16 +320,16 @@ void launch_zpair_f32(const DemagGeom& g, float2* Y, const float* Nhat, const vo
     dim3 grid((g.Py + kZpLines - 1) / kZpLines, g.Hx, 1);
     if (g.nz == 16 && g.Py % kZpLines == 0) {
       smem_optin(reinterpret_cast<const void*>(&k_zpair<true, true>));
-      k_zpair<true, true><<<grid, kZpNT, sm, st>>>(Y, Nhat, g, m, copy_wait_spins());
+      launch_pdl(k_zpair<true, true>, grid, dim3(kZpNT), sm, st, Y, Nhat, g, m, copy_wait_spins());
     } else {
       smem_optin(reinterpret_cast<const void*>(&k_zpair<true, false>));
-      k_zpair<true, false><<<grid, kZpNT, sm, st>>>(Y, Nhat, g, m, copy_wait_spins());
+      launch_pdl(k_zpair<true, false>, grid, dim3(kZpNT), sm, st, Y, Nhat, g, m, copy_wait_spins());
     }
   } else {
     const size_t sm = sizeof(float) * kZpTensor;
     smem_optin(reinterpret_cast<const void*>(&k_zpair<false, false>));
     dim3 grid((g.Hx + kZpLines - 1) / kZpLines, g.Py, 1);
-    k_zpair<false, false><<<grid, kZpNT, sm, st>>>(Y, Nhat, g, m, copy_wait_spins());
+    launch_pdl(k_zpair<false, false>, grid, dim3(kZpNT), sm, st, Y, Nhat, g, m, copy_wait_spins());
   }
 }
 

@@ -532,7 +532,7 @@ static void set_smem_attrs() {
   if (tracked && ((done_mask >> dev) & 1ull)) return;
   set_smem_attrs_nt<R, kHotNT>();
   if (sizeof(R) == 8) set_smem_attrs_nt<double, kTensorNT>();
-  if (sizeof(R) == 4) wreg_set_attrs();
+  wreg_set_attrs();
   if (tracked) done_mask |= 1ull << dev;
 }
 
@@ -600,8 +600,8 @@ int DemagPlan<R>::init(int nx, int ny, int nz, cudaStream_t st, char* err, size_
     if (lines_tile<R>(g.Hx, g.Py, 1, std::max(1, line_fft_buffers(py))) < 8) g.yT = g.xT = 1;
   }
   g.wreg = 0;
-  if (sizeof(R) == 4 && g.Pz > 1 && !long_x && !long_y && zc2 && wreg_enabled() &&
-      wreg_applies(nx, ny, nz, g.Px, g.Py))
+  if (g.Pz > 1 && !long_x && !long_y && zc2 && wreg_enabled() &&
+      wreg_applies(nx, ny, nz, g.Px, g.Py, sizeof(R) == 8))
     g.wreg = g.yT = g.xT = 1;
   if ((long_x && !make_fft_plan(g.Lc, gplx, 8)) || (long_y && !make_fft_plan(g.Py, gply, 8))) {
     snprintf(err, nerr, "demag: no radix plan");
@@ -1146,11 +1146,9 @@ static bool run_pass(const DemagPlan<R>& p, DemagGeom g, int which, const R* m, 
   using C = cplx_t<R>;
   constexpr int NT = kHotNT;
   const int64_t xlines = 3LL * g.ny * g.nz, ncz = 3LL * g.nz;
-  if constexpr (sizeof(R) == 4) {
-    if (g.wreg && which != 2) {
-      launch_wreg_f32(which, g, m, mu0Ms, p.X, p.Y, Hd, p.twx, p.twy, st);
-      return true;
-    }
+  if (g.wreg && which != 2) {
+    launch_wreg(which, g, m, mu0Ms, p.X, p.Y, Hd, p.twx, p.twy, st);
+    return true;
   }
   switch (which) {
     case 0:

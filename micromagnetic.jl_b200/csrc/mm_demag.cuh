@@ -41,9 +41,9 @@ struct DemagGeom {
   // x pass to the forward y pass (xT is set), and row-major again from the
   // inverse y pass to the inverse x pass
   int yT;
-  // FP32 power-of-two meshes (nx, ny = 32 Q, Px = 2 nx, Py = 2 ny, 3-D): the
-  // x and y passes run register-resident (mm_wreg.cu) with X column-major in
-  // both directions (yT and xT are set too)
+  // power-of-two meshes (nx, ny = 32 Q, Px = 2 nx, Py = 2 ny, 3-D; FP64:
+  // nx = 512 or 1024, ny = 1024): the x and y passes run register-resident
+  // (mm_wreg.cu) with X column-major in both directions (yT and xT are set)
   int wreg;
   const int* gate;  // device flag: kernels return at once when *gate == 0 (null: always run)
 };
@@ -119,15 +119,18 @@ void launch_zpair_f32(const DemagGeom& g, float2* Y, const float* Nhat, const vo
 unsigned copy_wait_spins();
 bool zpair_take_timeout();
 
-// Register-resident x and y passes, FP32 form (mm_wreg.cu): which = 0 fwd-x
-// (m, Ms -> X), 1 fwd-y (X -> Y), 3 inv-y (Y -> X), 4 inv-x (X -> H).
-bool wreg_applies(int nx, int ny, int nz, int Px, int Py);
+// Register-resident x and y passes (mm_wreg.cu): which = 0 fwd-x (m, Ms ->
+// X), 1 fwd-y (X -> Y), 3 inv-y (Y -> X), 4 inv-x (X -> H); both forms (the
+// FP64 form for fewer shapes, f64).
+bool wreg_applies(int nx, int ny, int nz, int Px, int Py, bool f64);
 void wreg_set_attrs();
 // True (and cleared) when a bounded wait of a bulk-copy y pass ran out on the
 // current device since the last call (synchronises the device).
 bool wreg_take_timeout();
-void launch_wreg_f32(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,
-                     const float2* twx, const float2* twy, cudaStream_t st);
+void launch_wreg(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,
+                 const float2* twx, const float2* twy, cudaStream_t st);
+void launch_wreg(int which, const DemagGeom& g, const double* m, const double* Ms, double2* X, double2* Y, double* H,
+                 const double2* twx, const double2* twy, cudaStream_t st);
 
 // FP64 Newell tensor (real space) with macro-PBC images, on the device:
 // out[c*N + I], c = xx yy zz xy xz yz.  dx,dy,dz are the raw cell sizes.

@@ -1,6 +1,6 @@
 // mm_wfft.cuh -- register-resident FFT of lines of L = 32 Q points (Q = 4, 8,
-// 16 or 32) by groups of Q lanes of one warp (32 / Q lines a warp), FP32
-// (internal).
+// 16 or 32) by groups of Q lanes of one warp (32 / Q lines a warp), FP32 or
+// FP64 (C = float2 or double2; internal).
 //
 // Four-step decomposition L = 32 x Q.  Lane q of a group holds the 32 values
 // x[q + Q j], j < 32, in registers:
@@ -30,14 +30,14 @@ __device__ __forceinline__ int wtile_at(int g, int k1, int q) {
   return g * (32 * (Q + 1)) + k1 * (Q + 1) + q;
 }
 
-template <int Q, bool INV, int TWS = 1>
-__device__ __forceinline__ void wfft(float2 (&v)[32], float2* __restrict__ tile, const float2* __restrict__ tw) {
+template <int Q, bool INV, int TWS = 1, typename C>
+__device__ __forceinline__ void wfft(C (&v)[32], C* __restrict__ tile, const C* __restrict__ tw) {
   const int lane = threadIdx.x & 31;
   const int g = lane / Q, q = lane % Q;
   dft32<INV>(v);
 #pragma unroll
   for (int k1 = 1; k1 < 32; ++k1) {
-    float2 w = __ldg(tw + TWS * q * k1);  // q k1 < 32 Q = L
+    C w = __ldg(tw + TWS * q * k1);  // q k1 < 32 Q = L
     if (INV) w.y = -w.y;
     v[k1] = cmul(v[k1], w);
   }
@@ -47,7 +47,7 @@ __device__ __forceinline__ void wfft(float2 (&v)[32], float2* __restrict__ tile,
   __syncwarp();
 #pragma unroll
   for (int i = 0; i < 32 / Q; ++i) {
-    float2 u[Q];
+    C u[Q];
 #pragma unroll
     for (int r = 0; r < Q; ++r) u[r] = tile[wtile_at<Q>(g, q + Q * i, r)];
     dftR<Q, INV>(u);

@@ -43,24 +43,30 @@ template <int Q, int W> constexpr int x_smem() {
                                                                 : (32 * Q + 1) * x_stride<Q, W>();
 }
 
-// Warps of an x-pass block: the forward pass runs 4 (no register cap: 87
-// registers, five blocks an SM by shared memory), the inverse pass 8 (80
-// registers, three blocks an SM), which moves column segments of RB = 8 rows
-// (64 bytes for Q = 32).  Measured on c5 (1024 x 1024 x 16, Q = 32):
-// forward 0.248 ms with 4 warps, 0.273 with 8 (0.287 with 4 capped at 96
-// registers); inverse 0.287 ms with 4 warps, 0.273 with 8.
-constexpr int kXfW = 4, kXiW = 8;
+// Warps of an x-pass block: the FP32 forward pass runs 4 (five blocks an SM
+// by shared memory), the inverse pass 8 (three blocks an SM), which moves
+// column segments of RB = 8 rows (64 bytes for Q = 32).  Measured on c5
+// (1024 x 1024 x 16, Q = 32): forward 0.248 ms with 4 warps, 0.273 with 8
+// (0.287 with 4 capped at 96 registers); inverse 0.287 ms with 4 warps, 0.273
+// with 8.  FP64 blocks run 4 warps in both directions (RB = 4 rows of 16-byte
+// values: 64-byte segments, 82 KB of shared memory, two blocks an SM).
+template <typename R> constexpr int x_fwd_warps() { return 4; }
+template <typename R> constexpr int x_inv_warps() { return sizeof(R) == 4 ? 8 : 4; }
+template <typename R, int W> constexpr int x_fwd_minb() { return sizeof(R) == 4 ? 4 : 2; }
+template <typename R, int W> constexpr int x_inv_minb() { return sizeof(R) == 4 ? 24 / W : 2; }
 
 // ---------------------------------------------------------------- x forward
 // Rows of m * mu0Ms (zero padded to Px = 2 Lc) -> X column-major.  A block
 // transforms its RB rows for the three components in turn, so that each row
 // of Ms is read from HBM once (the later reads hit the caches; c5: 0.243 ->
 // 0.235 ms against blocks of one component).
-template <int Q, int W>
-__global__ void __launch_bounds__(32 * W, 4) k_xfwd_w(const float* __restrict__ m, const float* __restrict__ Ms,
-                                                  float2* __restrict__ X, DemagGeom g, const float2* __restrict__ twx) {
+template <int Q, int W, typename R>
+__global__ void __launch_bounds__(32 * W, (x_fwd_minb<R, W>())) k_xfwd_w(const R* __restrict__ m, const R* __restrict__ Ms,
+                                                  cplx_t<R>* __restrict__ X, DemagGeom g, const cplx_t<R>* __restrict__ twx) {
+  using C = cplx_t<R>;
   constexpr int RB = x_rows<Q, W>(), L = 32 * Q, S = x_stride<Q, W>();
-  extern __shared__ __align__(16) float2 sm[];  // x_smem<Q, W>() values
+  extern __shared__ __align__(16) unsigned char xsm_raw[];  // x_smem<Q, W>() values
+  C* sm = reinterpret_cast<C*>(xsm_raw);
   pdl_enter();
   if (g.gate && !*g.gate) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -70,21 +76,21 @@ __global__ void __launch_bounds__(32 * W, 4) k_xfwd_w(const float* __restrict__ 
   const int row0 = blockIdx.x * RB;  // rows % RB == 0
   const int rl = warp * (32 / Q) + gq;
   const int64_t rb = static_cast<int64_t>(row0 + rl) * nx;
-  const float2* s2 = reinterpret_cast<const float2*>(Ms + rb);
+  const C* s2 = reinterpret_cast<const C*>(Ms + rb);
   constexpr int KS = 32 * W / RB;
   const int r = threadIdx.x & (RB - 1), k0 = threadIdx.x / RB;
   const int64_t step = static_cast<int64_t>(KS) * rows;
 #pragma unroll 1
   for (int c = 0; c < 3; ++c) {
-    const float2* m2 = reinterpret_cast<const float2*>(m + c * N + rb);
-    float2 v[32];
+    const C* m2 = reinterpret_cast<const C*>(m + c * N + rb);
+    C v[32];
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
       if (j < 16) {  // z[n] = (x[2n], x[2n+1]), nonzero for n < Lc / 2
-        const float2 a = m2[q + Q * j], b = s2[q + Q * j];
-        v[j] = make_float2(a.x * b.x, a.y * b.y);
+        const C a = m2[q + Q * j], b = s2[q + Q * j];
+        v[j] = cmk<C>(a.x * b.x, a.y * b.y);
       } else {
-        v[j] = make_float2(0.f, 0.f);
+        v[j] = cmk<C>(R(0), R(0));
       }
     }
     if (c > 0) __syncthreads();  // the previous component's staged rows are written out
@@ -96,14 +102,14 @@ __global__ void __launch_bounds__(32 * W, 4) k_xfwd_w(const float* __restrict__ 
     // X[k] = E + w_Px^k O, E = (Z[k] + conj Z[Lc-k]) / 2, O = (Z[k] - conj Z[Lc-k]) / 2i
     // (Z is L-periodic: k = L reads Z[0]).  Thread (k0, r) writes row r of
     // k = k0, k0 + KS, ... through a pointer stepped by KS columns.
-    float2* xp = X + (static_cast<int64_t>(c) * Hx + k0) * rows + row0 + r;
+    C* xp = X + (static_cast<int64_t>(c) * Hx + k0) * rows + row0 + r;
 #pragma unroll 4
     for (int k = k0; k < Hx; k += KS, xp += step) {
-      const float2 zk = sm[(k & (L - 1)) * S + r];
-      float2 zc = sm[((L - k) & (L - 1)) * S + r];
+      const C zk = sm[(k & (L - 1)) * S + r];
+      C zc = sm[((L - k) & (L - 1)) * S + r];
       zc.y = -zc.y;
-      const float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
-      const float2 od = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
+      const C ev = cmk<C>(R(0.5) * (zk.x + zc.x), R(0.5) * (zk.y + zc.y));
+      const C od = cmk<C>(R(0.5) * (zk.y - zc.y), R(-0.5) * (zk.x - zc.x));
       *xp = cadd(ev, cmul(__ldg(twx + k), od));
     }
   }
@@ -111,11 +117,13 @@ __global__ void __launch_bounds__(32 * W, 4) k_xfwd_w(const float* __restrict__ 
 
 // ---------------------------------------------------------------- x inverse
 // X column-major -> real rows (c2r, unnormalised), keeps x < nx.
-template <int Q, int W>
-__global__ void __launch_bounds__(32 * W, 24 / W) k_xinv_w(const float2* __restrict__ X, float* __restrict__ H, DemagGeom g,
-                                                  const float2* __restrict__ twx) {
+template <int Q, int W, typename R>
+__global__ void __launch_bounds__(32 * W, (x_inv_minb<R, W>())) k_xinv_w(const cplx_t<R>* __restrict__ X, R* __restrict__ H,
+                                                  DemagGeom g, const cplx_t<R>* __restrict__ twx) {
+  using C = cplx_t<R>;
   constexpr int RB = x_rows<Q, W>(), L = 32 * Q, S = x_stride<Q, W>();
-  extern __shared__ __align__(16) float2 sm[];  // x_smem<Q, W>() values
+  extern __shared__ __align__(16) unsigned char xsm_raw[];  // x_smem<Q, W>() values
+  C* sm = reinterpret_cast<C*>(xsm_raw);
   pdl_enter();
   if (g.gate && !*g.gate) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -129,35 +137,39 @@ __global__ void __launch_bounds__(32 * W, 24 / W) k_xinv_w(const float2* __restr
     // thread (k0, r) stages row r of k = k0, k0 + KS, ... with cp.async, so
     // that all of its copies are in flight at once without holding registers;
     // each miss fetches 256 bytes into L2 (the column segments of the next
-    // three blocks, which run alongside this one)
+    // blocks, which run alongside this one)
     constexpr int KS = 32 * W / RB;
     const int r = threadIdx.x & (RB - 1), k0 = threadIdx.x / RB;
     const int64_t step = static_cast<int64_t>(KS) * rows;
-    const float2* xp = X + (static_cast<int64_t>(c) * Hx + k0) * rows + row0 + r;
+    const C* xp = X + (static_cast<int64_t>(c) * Hx + k0) * rows + row0 + r;
     unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(sm + k0 * S + r));
-    for (int k = k0; k < Hx; k += KS, xp += step, sa += KS * S * sizeof(float2))
-      asm volatile("cp.async.ca.shared.global.L2::256B [%0], [%1], 8;\n" ::"r"(sa), "l"(xp) : "memory");
+    for (int k = k0; k < Hx; k += KS, xp += step, sa += KS * S * sizeof(C)) {
+      if constexpr (sizeof(C) == 8)
+        asm volatile("cp.async.ca.shared.global.L2::256B [%0], [%1], 8;\n" ::"r"(sa), "l"(xp) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global.L2::256B [%0], [%1], 16;\n" ::"r"(sa), "l"(xp) : "memory");
+    }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   }
   __syncthreads();
   // Z'[k] = (A + B) + i (A - B) conj(w_Px^k), A = X[k], B = conj X[Lc - k]
-  float2 v[32];
+  C v[32];
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     const int k = q + Q * j;
-    const float2 a = sm[k * S + rl];
-    float2 b = sm[(L - k) * S + rl];
+    const C a = sm[k * S + rl];
+    C b = sm[(L - k) * S + rl];
     b.y = -b.y;
-    float2 w = __ldg(twx + k);
+    C w = __ldg(twx + k);
     w.y = -w.y;
-    const float2 d = cmul(csub(a, b), w);
-    v[j] = make_float2(a.x + b.x - d.y, a.y + b.y + d.x);
+    const C d = cmul(csub(a, b), w);
+    v[j] = cmk<C>(a.x + b.x - d.y, a.y + b.y + d.x);
   }
   __syncthreads();  // the staging tile becomes the transpose tiles
   wfft<Q, true, 2>(v, sm + warp * wtile_size<Q>(), twx);
   // z[n] = (x[2n], x[2n+1]) for n < Lc / 2: registers with k2 = r % Q < Q / 2
-  float2* h2 = reinterpret_cast<float2*>(H + c * N + static_cast<int64_t>(row0 + rl) * nx);
+  C* h2 = reinterpret_cast<C*>(H + c * N + static_cast<int64_t>(row0 + rl) * nx);
 #pragma unroll
   for (int r = 0; r < 32; ++r) {
     if (r % Q < Q / 2) h2[q + Q * (r / Q) + 32 * (r % Q)] = v[r];
@@ -425,13 +437,18 @@ __device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned 
 // The staged output line leaves by one bulk copy issued by thread 0: the
 // warps go on to the next line at once, and the staging tiles are reused only
 // after that copy has read them (c5: 0.358 -> 0.272 ms against 16-byte stores
-// of every thread).
-__global__ void __launch_bounds__(kWpNT, 8) k_yfwd_p(const float2* __restrict__ X, float2* __restrict__ Y, DemagGeom g,
-                                                     const float2* __restrict__ twy, int nlines, unsigned spins) {
+// of every thread).  FP32 and FP64 (C = float2 or double2).
+template <typename R>
+__global__ void __launch_bounds__(kWpNT, sizeof(R) == 4 ? 8 : 4) k_yfwd_p(const cplx_t<R>* __restrict__ X,
+                                                                        cplx_t<R>* __restrict__ Y, DemagGeom g,
+                                                                        const cplx_t<R>* __restrict__ twy, int nlines,
+                                                                        unsigned spins) {
+  using C = cplx_t<R>;
   constexpr int NY = 1024, Py = 2048;
-  extern __shared__ __align__(128) float2 sp[];
-  float2* buf = sp;                                                          // NY
-  float2* tile = sp + NY + (threadIdx.x >> 5) * wtile_size<32>();           // this warp's
+  extern __shared__ __align__(128) unsigned char yfp_raw[];
+  C* sp = reinterpret_cast<C*>(yfp_raw);
+  C* buf = sp;                                                          // NY
+  C* tile = sp + NY + (threadIdx.x >> 5) * wtile_size<32>();           // this warp's
   auto* bar = reinterpret_cast<unsigned long long*>(sp + NY + 2 * wtile_size<32>());
   pdl_enter();
   if (g.gate && !*g.gate) return;
@@ -440,15 +457,15 @@ __global__ void __launch_bounds__(kWpNT, 8) k_yfwd_p(const float2* __restrict__ 
   const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
     mbar_init(bar);
-    bulk_load(buf, X + static_cast<int64_t>(line) * NY, NY * sizeof(float2), bar);
+    bulk_load(buf, X + static_cast<int64_t>(line) * NY, NY * sizeof(C), bar);
   }
   __syncthreads();
   for (unsigned it = 0; line < nlines; ++it, line += gridDim.x) {
     if (!block_wait(bar, it & 1, spins)) return;
-    float2 v[32];
+    C v[32];
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
-      float2 a = buf[lane + 32 * j];
+      C a = buf[lane + 32 * j];
       if (s) a = cmul(a, __ldg(twy + lane + 32 * j));
       v[j] = a;
     }
@@ -456,17 +473,17 @@ __global__ void __launch_bounds__(kWpNT, 8) k_yfwd_p(const float2* __restrict__ 
     if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
     __syncthreads();  // both warps hold the line: the buffer takes the next one
     if (threadIdx.x == 0 && line + static_cast<int>(gridDim.x) < nlines)
-      bulk_load(buf, X + static_cast<int64_t>(line + gridDim.x) * NY, NY * sizeof(float2), bar);
+      bulk_load(buf, X + static_cast<int64_t>(line + gridDim.x) * NY, NY * sizeof(C), bar);
     wfft<32, false, 2>(v, tile, twy);
     // the two parities interleave in the tiles' space (2048 values), which
-    // the block then writes as 16-byte pairs (Y[2k], Y[2k + 1])
+    // leave as one copy (Y[2k], Y[2k + 1], ...)
     __syncthreads();
-    float2* stg = sp + NY;
+    C* stg = sp + NY;
 #pragma unroll
     for (int r = 0; r < 32; ++r) stg[2 * (lane + 32 * r) + s] = v[r];
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // the staged line, to the copy engine
     __syncthreads();
-    if (threadIdx.x == 0) bulk_store(Y + static_cast<int64_t>(line) * Py, stg, Py * sizeof(float2));
+    if (threadIdx.x == 0) bulk_store(Y + static_cast<int64_t>(line) * Py, stg, Py * sizeof(C));
   }
   // the shared memory of the last store stays valid until the copy is done
   if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
@@ -474,38 +491,43 @@ __global__ void __launch_bounds__(kWpNT, 8) k_yfwd_p(const float2* __restrict__ 
 
 // inverse: Y column (2048 values) -> X column (y < 1024); warp s transforms
 // Y[2k + s] and the pair adds u0[y] + w^(-y) u1[y] through the warp tiles
-__global__ void __launch_bounds__(kWpNT, 6) k_yinv_p(const float2* __restrict__ Y, float2* __restrict__ X, DemagGeom g,
-                                                     const float2* __restrict__ twy, int nlines, unsigned spins) {
+template <typename R>
+__global__ void __launch_bounds__(kWpNT, sizeof(R) == 4 ? 6 : 3) k_yinv_p(const cplx_t<R>* __restrict__ Y,
+                                                                        cplx_t<R>* __restrict__ X, DemagGeom g,
+                                                                        const cplx_t<R>* __restrict__ twy, int nlines,
+                                                                        unsigned spins) {
+  using C = cplx_t<R>;
   constexpr int NY = 1024, Py = 2048;
-  extern __shared__ __align__(128) float2 sp[];
-  float2* buf = sp;                                          // Py
-  float2* tiles = sp + Py;                                   // two warp tiles
+  extern __shared__ __align__(128) unsigned char yip_raw[];
+  C* sp = reinterpret_cast<C*>(yip_raw);
+  C* buf = sp;                                          // Py
+  C* tiles = sp + Py;                                   // two warp tiles
   auto* bar = reinterpret_cast<unsigned long long*>(sp + Py + 2 * wtile_size<32>());
   pdl_enter();
   if (g.gate && !*g.gate) return;
   int line = blockIdx.x;
   if (line >= nlines) return;
   const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
-  float2* tile = tiles + s * wtile_size<32>();
-  const float2* pt = tiles + (s ^ 1) * wtile_size<32>();
+  C* tile = tiles + s * wtile_size<32>();
+  const C* pt = tiles + (s ^ 1) * wtile_size<32>();
   if (threadIdx.x == 0) {
     mbar_init(bar);
-    bulk_load(buf, Y + static_cast<int64_t>(line) * Py, Py * sizeof(float2), bar);
+    bulk_load(buf, Y + static_cast<int64_t>(line) * Py, Py * sizeof(C), bar);
   }
   __syncthreads();
   for (unsigned it = 0; line < nlines; ++it, line += gridDim.x) {
     if (!block_wait(bar, it & 1, spins)) return;
-    float2 v[32];
+    C v[32];
 #pragma unroll
     for (int j = 0; j < 32; ++j) v[j] = buf[2 * (lane + 32 * j) + s];
     __syncthreads();  // both warps hold the line (and are done with last line's tiles)
     if (threadIdx.x == 0 && line + static_cast<int>(gridDim.x) < nlines)
-      bulk_load(buf, Y + static_cast<int64_t>(line + gridDim.x) * Py, Py * sizeof(float2), bar);
+      bulk_load(buf, Y + static_cast<int64_t>(line + gridDim.x) * Py, Py * sizeof(C), bar);
     wfft<32, true, 2>(v, tile, twy);
     if (s) {
 #pragma unroll
       for (int r = 0; r < 32; ++r) {
-        float2 w = __ldg(twy + lane + 32 * r);
+        C w = __ldg(twy + lane + 32 * r);
         w.y = -w.y;
         v[r] = cmul(v[r], w);
       }
@@ -514,18 +536,18 @@ __global__ void __launch_bounds__(kWpNT, 6) k_yinv_p(const float2* __restrict__ 
 #pragma unroll
     for (int i = 0; i < 16; ++i) tile[i * 32 + lane] = s ? v[2 * i] : v[2 * i + 1];
     __syncthreads();
-    float2* xo = X + static_cast<int64_t>(line) * NY;
+    C* xo = X + static_cast<int64_t>(line) * NY;
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
-      const float2 a = s ? v[2 * i + 1] : v[2 * i], b = pt[i * 32 + lane];
-      xo[lane + 32 * (2 * i + s)] = make_float2(a.x + b.x, a.y + b.y);
+      const C a = s ? v[2 * i + 1] : v[2 * i], b = pt[i * 32 + lane];
+      xo[lane + 32 * (2 * i + s)] = cmk<C>(a.x + b.x, a.y + b.y);
     }
   }
 }
 
 static_assert(2 * wtile_size<32>() >= 2048, "the forward pass stages a padded line in its warp tiles");
-constexpr size_t kYfpSmem = (1024 + 2 * wtile_size<32>()) * sizeof(float2) + 8;
-constexpr size_t kYipSmem = (2048 + 2 * wtile_size<32>()) * sizeof(float2) + 8;
+template <typename R> constexpr size_t yfp_smem() { return (1024 + 2 * wtile_size<32>()) * sizeof(cplx_t<R>) + 8; }
+template <typename R> constexpr size_t yip_smem() { return (2048 + 2 * wtile_size<32>()) * sizeof(cplx_t<R>) + 8; }
 
 // The bulk-copy y passes for Q = 32 unless MMCUDA_YPIPE=0 (warp-direct ones)
 bool ypipe_enabled() {
@@ -544,41 +566,49 @@ int resident_blocks(const void* kernel, int nt, size_t smem) {
   return std::max(1, sms) * std::max(1, per);
 }
 
-template <int Q>
-void launch_q(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,
-              const float2* twx, const float2* twy, cudaStream_t st) {
+template <int Q, typename R>
+void launch_q(int which, const DemagGeom& g, const R* m, const R* Ms, cplx_t<R>* X, cplx_t<R>* Y, R* H,
+              const cplx_t<R>* twx, const cplx_t<R>* twy, cudaStream_t st) {
+  using C = cplx_t<R>;
+  constexpr int XF = x_fwd_warps<R>(), XI = x_inv_warps<R>();
   const int rows = g.ny * g.nz;
   const int ylines = 3 * g.Hx * g.nz;
-  constexpr int NL = 4 * (32 / Q), DL = (kWdNT / 32) * (32 / Q) / 2;
-  const size_t ysm = static_cast<size_t>(8) * wtile_size<Q>() * sizeof(float2);
   switch (which) {
     case 0:
-      launch_pdl(k_xfwd_w<Q, kXfW>, dim3(rows / x_rows<Q, kXfW>()), dim3(32 * kXfW),
-                 x_smem<Q, kXfW>() * sizeof(float2), st, m, Ms, X, g, twx);
+      launch_pdl(k_xfwd_w<Q, XF, R>, dim3(rows / x_rows<Q, XF>()), dim3(32 * XF), x_smem<Q, XF>() * sizeof(C), st, m,
+                 Ms, X, g, twx);
       break;
     case 1:
-      if (Q == 32 && ypipe_enabled()) {
-        static const int nb = resident_blocks(reinterpret_cast<const void*>(&k_yfwd_p), kWpNT, kYfpSmem);
-        launch_pdl(k_yfwd_p, dim3(std::min(ylines, nb)), dim3(kWpNT), kYfpSmem, st, X, Y, g, twy, ylines,
+      if (Q == 32 && (sizeof(R) == 8 || ypipe_enabled())) {
+        static const int nb = resident_blocks(reinterpret_cast<const void*>(&k_yfwd_p<R>), kWpNT, yfp_smem<R>());
+        launch_pdl(k_yfwd_p<R>, dim3(std::min(ylines, nb)), dim3(kWpNT), yfp_smem<R>(), st, X, Y, g, twy, ylines,
                    copy_wait_spins());
-      } else if (ydirect_enabled())
-        launch_pdl(k_yfwd_d<Q>, dim3((ylines + DL - 1) / DL), dim3(kWdNT), ysm, st, X, Y, g, twy, ylines);
-      else
-        launch_pdl(k_yfwd_w<Q>, dim3((ylines + NL - 1) / NL), dim3(kWyNT), ysm, st, X, Y, g, twy, ylines);
+      } else if constexpr (sizeof(R) == 4) {
+        constexpr int NL = 4 * (32 / Q), DL = (kWdNT / 32) * (32 / Q) / 2;
+        const size_t ysm = static_cast<size_t>(8) * wtile_size<Q>() * sizeof(float2);
+        if (ydirect_enabled())
+          launch_pdl(k_yfwd_d<Q>, dim3((ylines + DL - 1) / DL), dim3(kWdNT), ysm, st, X, Y, g, twy, ylines);
+        else
+          launch_pdl(k_yfwd_w<Q>, dim3((ylines + NL - 1) / NL), dim3(kWyNT), ysm, st, X, Y, g, twy, ylines);
+      }
       break;
     case 3:
-      if (Q == 32 && ypipe_enabled()) {
-        static const int nb = resident_blocks(reinterpret_cast<const void*>(&k_yinv_p), kWpNT, kYipSmem);
-        launch_pdl(k_yinv_p, dim3(std::min(ylines, nb)), dim3(kWpNT), kYipSmem, st, Y, X, g, twy, ylines,
+      if (Q == 32 && (sizeof(R) == 8 || ypipe_enabled())) {
+        static const int nb = resident_blocks(reinterpret_cast<const void*>(&k_yinv_p<R>), kWpNT, yip_smem<R>());
+        launch_pdl(k_yinv_p<R>, dim3(std::min(ylines, nb)), dim3(kWpNT), yip_smem<R>(), st, Y, X, g, twy, ylines,
                    copy_wait_spins());
-      } else if (ydirect_enabled())
-        launch_pdl(k_yinv_d<Q>, dim3((ylines + DL - 1) / DL), dim3(kWdNT), ysm, st, Y, X, g, twy, ylines);
-      else
-        launch_pdl(k_yinv_w<Q>, dim3((ylines + NL - 1) / NL), dim3(kWyNT), ysm, st, Y, X, g, twy, ylines);
+      } else if constexpr (sizeof(R) == 4) {
+        constexpr int NL = 4 * (32 / Q), DL = (kWdNT / 32) * (32 / Q) / 2;
+        const size_t ysm = static_cast<size_t>(8) * wtile_size<Q>() * sizeof(float2);
+        if (ydirect_enabled())
+          launch_pdl(k_yinv_d<Q>, dim3((ylines + DL - 1) / DL), dim3(kWdNT), ysm, st, Y, X, g, twy, ylines);
+        else
+          launch_pdl(k_yinv_w<Q>, dim3((ylines + NL - 1) / NL), dim3(kWyNT), ysm, st, Y, X, g, twy, ylines);
+      }
       break;
     case 4:
-      launch_pdl(k_xinv_w<Q, kXiW>, dim3(3 * rows / x_rows<Q, kXiW>()), dim3(32 * kXiW),
-                 x_smem<Q, kXiW>() * sizeof(float2), st, X, H, g, twx);
+      launch_pdl(k_xinv_w<Q, XI, R>, dim3(3 * rows / x_rows<Q, XI>()), dim3(32 * XI), x_smem<Q, XI>() * sizeof(C), st,
+                 X, H, g, twx);
       break;
     default:
       break;
@@ -592,10 +622,21 @@ void set_attrs_q() {
   cudaFuncSetAttribute(k_yinv_w<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   cudaFuncSetAttribute(k_yfwd_d<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   cudaFuncSetAttribute(k_yinv_d<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-  cudaFuncSetAttribute(k_xfwd_w<Q, kXfW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(x_smem<Q, kXfW>() * sizeof(float2)));
-  cudaFuncSetAttribute(k_xinv_w<Q, kXiW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(x_smem<Q, kXiW>() * sizeof(float2)));
+  constexpr int XF = x_fwd_warps<float>(), XI = x_inv_warps<float>();
+  cudaFuncSetAttribute(k_xfwd_w<Q, XF, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(x_smem<Q, XF>() * sizeof(float2)));
+  cudaFuncSetAttribute(k_xinv_w<Q, XI, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(x_smem<Q, XI>() * sizeof(float2)));
+}
+
+// FP64: x passes for Q = 16, 32, y passes for Q = 32
+template <int Q>
+void set_attrs_q64() {
+  constexpr int XF = x_fwd_warps<double>(), XI = x_inv_warps<double>();
+  cudaFuncSetAttribute(k_xfwd_w<Q, XF, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(x_smem<Q, XF>() * sizeof(double2)));
+  cudaFuncSetAttribute(k_xinv_w<Q, XI, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(x_smem<Q, XI>() * sizeof(double2)));
 }
 
 int wq(int n) {
@@ -612,9 +653,11 @@ int wq(int n) {
 
 // ny >= 512: with shorter y lines the shared-memory y passes (wide row tiles)
 // and the row-major z kernel measured faster (c2, 256 x 256 x 64: 2.77 vs
-// 2.71 ms a step; c5, 1024 x 1024 x 16: 10.3 vs 12.7 ms)
-bool wreg_applies(int nx, int ny, int nz, int Px, int Py) {
-  return nz > 1 && wq(nx) && wq(ny) && ny >= 512 && Px == 2 * nx && Py == 2 * ny;
+// 2.71 ms a step; c5, 1024 x 1024 x 16: 10.3 vs 12.7 ms).  The FP64 form
+// takes nx = 512 or 1024 and ny = 1024 (the bulk-copy y passes).
+bool wreg_applies(int nx, int ny, int nz, int Px, int Py, bool f64) {
+  if (!(nz > 1 && wq(nx) && wq(ny) && ny >= 512 && Px == 2 * nx && Py == 2 * ny)) return false;
+  return !f64 || (wq(nx) >= 16 && ny == 1024);
 }
 
 void wreg_set_attrs() {
@@ -622,6 +665,12 @@ void wreg_set_attrs() {
   set_attrs_q<8>();
   set_attrs_q<16>();
   set_attrs_q<32>();
+  set_attrs_q64<16>();
+  set_attrs_q64<32>();
+  cudaFuncSetAttribute(k_yfwd_p<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(yfp_smem<double>()));
+  cudaFuncSetAttribute(k_yinv_p<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(yip_smem<double>()));
 }
 
 bool wreg_take_timeout() {
@@ -632,8 +681,8 @@ bool wreg_take_timeout() {
   return true;
 }
 
-void launch_wreg_f32(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,
-                     const float2* twx, const float2* twy, cudaStream_t st) {
+void launch_wreg(int which, const DemagGeom& g, const float* m, const float* Ms, float2* X, float2* Y, float* H,
+                 const float2* twx, const float2* twy, cudaStream_t st) {
   // the x passes run on rows (Q of nx), the y passes on columns (Q of ny)
   const int q = (which == 0 || which == 4) ? wq(g.nx) : wq(g.ny);
   switch (q) {
@@ -642,6 +691,13 @@ void launch_wreg_f32(int which, const DemagGeom& g, const float* m, const float*
     case 16: launch_q<16>(which, g, m, Ms, X, Y, H, twx, twy, st); break;
     default: launch_q<32>(which, g, m, Ms, X, Y, H, twx, twy, st); break;
   }
+}
+
+void launch_wreg(int which, const DemagGeom& g, const double* m, const double* Ms, double2* X, double2* Y, double* H,
+                 const double2* twx, const double2* twy, cudaStream_t st) {
+  const int q = (which == 0 || which == 4) ? wq(g.nx) : wq(g.ny);
+  if (q == 16) launch_q<16>(which, g, m, Ms, X, Y, H, twx, twy, st);
+  else launch_q<32>(which, g, m, Ms, X, Y, H, twx, twy, st);
 }
 
 }  // namespace mm

@@ -487,6 +487,25 @@ def test_register_passes_fp32(mesh):
         assert rel_maxnorm(g32.m(), o.get_m()) <= TOL32
 
 
+@pytest.mark.parametrize("mesh", [(512, 1024, 2), (1024, 1024, 4)])
+def test_register_passes_fp64(mesh):
+    """FP64 meshes with nx = 512 or 1024 and ny = 1024 run the register-resident
+    x passes (lane groups Q = 16, 32) and the bulk-copy y passes in FP64, with
+    the shared-memory z convolution between them: H_eff and two RK4 steps
+    against the oracle."""
+    from oracle.oracle import demag_tensor
+
+    nx, ny, nz = mesh
+    cfg = random_config(47 + nx + nz, nx, ny, nz, "", terms=("exch", "demag"), spatial=False)
+    T = demag_tensor(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, _ = build_oracle(cfg, tensor=T)
+    g = GpuSim(cfg, form=0, tensor=T)
+    assert rel_maxnorm(g.field(), o.effective_field()) <= TOL64
+    o.rk4(2e-14, 2)
+    g.rk4(2e-14, 2)
+    assert rel_maxnorm(g.m(), o.get_m()) <= TOL64
+
+
 def test_stage_tile_opt_in():
     """The halo-tiled stage kernel (MMCUDA_STAGETILE=1, off by default) gives
     the same RK4 steps as the default kernel: FP64 to 1e-12 against the

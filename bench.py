@@ -56,6 +56,10 @@ WORKLOADS = {
     # small enough for full ncu captures
     "c5_small": dict(nx=256, ny=1024, nz=16, dx=3e-9, dy=3e-9, dz=3e-9, Ms=8e5, A=1.3e-11, Dbulk=None, Ku=None,
                      axis=(0, 0, 1), demag=True, alpha=0.1, gamma=2.211e5, dt=5e-14, seed=105, zeeman=None),
+    # profiling case of the FP64 register passes (nx = 512, ny = 1024: the
+    # same x / y line lengths as c5 for y, Q = 16 for x), about 2 GB in FP64
+    "c5_half": dict(nx=512, ny=1024, nz=16, dx=3e-9, dy=3e-9, dz=3e-9, Ms=8e5, A=1.3e-11, Dbulk=None, Ku=None,
+                    axis=(0, 0, 1), demag=True, alpha=0.1, gamma=2.211e5, dt=5e-14, seed=105, zeeman=None),
     # profiling case of the global-memory x stages: x/2 = 16000 is beyond one
     # block's shared memory
     "long_lines": dict(nx=16000, ny=64, nz=1, dx=4e-9, dy=4e-9, dz=4e-9, Ms=8e5, A=1.3e-11, Dbulk=None, Ku=None,
@@ -91,8 +95,8 @@ BATCHES = {
 ADJOINT = {"c4": dict(nx=128, ny=128, nz=4, dx=2e-9, A=1.3e-11, D=3e-3, Ku=4e5, alpha=0.1, gamma=2.211e5,
                       dt=5e-14, nsteps=2000, ckpt=100, seed=104)}
 # the CPU baseline times a bounded block of the same physics
-CPU_SAMPLE = {"c2": (128, 128, 32), "c5": (256, 256, 16), "c5_small": (256, 256, 16), "c1": (200, 50, 1),
-              "long_lines": (2000, 64, 1), "fig9": (1000, 1000, 1),
+CPU_SAMPLE = {"c2": (128, 128, 32), "c5": (256, 256, 16), "c5_small": (256, 256, 16), "c5_half": (256, 256, 16),
+              "c1": (200, 50, 1), "long_lines": (2000, 64, 1), "fig9": (1000, 1000, 1),
               "fig9_4000": (1000, 1000, 1), "fig9_8000": (1000, 1000, 1), "fig9_10000": (1000, 1000, 1)}
 
 

@@ -1127,6 +1127,11 @@ static void launch_zconv(const DemagGeom& g, cplx_t<R>* Y, const R* Nhat, const 
       launch_zpair_f32(g, Y, Nhat, zmap, st);
       return;
     }
+  } else {
+    if (zquad_applies(g)) {
+      launch_zquad_f64(g, Y, Nhat, st);
+      return;
+    }
   }
   if (try_zconv2<R>(g, Y, Nhat, twz, st, Wforce)) return;
   if (try_zsmall<R>(g, Y, Nhat, st)) return;
@@ -1264,6 +1269,7 @@ int DemagPlan<R>::autotune(const R* m, const R* mu0Ms, R* Hd, cudaStream_t st) {
     if (fused2d && which != 2) continue;
     if (long_y && (which != 2 || g.Pz == 1)) continue;  // global-memory stages have no tile
     if (g.wreg && which != 2) continue;                  // register passes have no tile
+    if (which == 2 && (sizeof(R) == 4 ? zpair_enabled() && zpair_applies(g) : zquad_applies(g))) continue;
     // the static rule's W is the incumbent; another W must be 3 % faster
     // (timing noise, e.g. under a profiler, then cannot move the choice)
     tile[which] = 0;

@@ -119,6 +119,12 @@ void launch_zpair_f32(const DemagGeom& g, float2* Y, const float* Nhat, const vo
 unsigned copy_wait_spins();
 bool zpair_take_timeout();
 
+// Register-resident z convolution for Pz = 32 (nz <= 16), FP64 form,
+// column-major spectra (mm_zquad.cu): in place on Y.  MMCUDA_ZQUAD=0 keeps
+// the shared-memory kernel.
+bool zquad_applies(const DemagGeom& g);
+void launch_zquad_f64(const DemagGeom& g, double2* Y, const double* Nhat, cudaStream_t st);
+
 // Register-resident x and y passes (mm_wreg.cu): which = 0 fwd-x (m, Ms ->
 // X), 1 fwd-y (X -> Y), 3 inv-y (Y -> X), 4 inv-x (X -> H); both forms (the
 // FP64 form for fewer shapes, f64).

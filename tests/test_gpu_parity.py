@@ -506,6 +506,25 @@ def test_register_passes_fp64(mesh):
     assert rel_maxnorm(g.m(), o.get_m()) <= TOL64
 
 
+@pytest.mark.parametrize("mesh", [(64, 500, 16), (32, 1024, 16)])
+def test_zquad_fp64(mesh):
+    """FP64 column-major meshes with nz = 16 (Pz = 32) run the register z
+    convolution of four threads a line: Py = 1000 (blocks past the last ky
+    line, predicated) and Py = 2048 (every block full), the shared-memory x
+    and y passes around it; H_eff and two RK4 steps against the oracle."""
+    from oracle.oracle import demag_tensor
+
+    nx, ny, nz = mesh
+    cfg = random_config(53 + nx + ny, nx, ny, nz, "", terms=("exch", "dmi_bulk", "anis", "demag"), spatial=False)
+    T = demag_tensor(nx, ny, nz, cfg["dx"], cfg["dy"], cfg["dz"])
+    o, _ = build_oracle(cfg, tensor=T)
+    g = GpuSim(cfg, form=0, tensor=T)
+    assert rel_maxnorm(g.field(), o.effective_field()) <= TOL64
+    o.rk4(2e-14, 2)
+    g.rk4(2e-14, 2)
+    assert rel_maxnorm(g.m(), o.get_m()) <= TOL64
+
+
 def test_stage_tile_opt_in():
     """The halo-tiled stage kernel (MMCUDA_STAGETILE=1, off by default) gives
     the same RK4 steps as the default kernel: FP64 to 1e-12 against the

@@ -45,5 +45,10 @@ def test_autotuned_tiles_give_identical_fields(mesh, form):
     f_tuned, t_tuned = _field(cfg, form, True)
     assert t_static == [0, 0, 0, 0, 0]
     used = [2] if mesh[2] == 1 else [1, 2, 3]
+    # nz = 16 pads z to 32: the register z convolution takes no tile (FP32
+    # always; FP64 where the spectra are column-major, padded y = 420 here)
+    if mesh[2] == 16 and (form == 1 or mesh[1] == 210):
+        used.remove(2)
+        assert t_tuned[2] == 0, t_tuned
     assert all(t_tuned[i] >= 1 for i in used), t_tuned
     np.testing.assert_array_equal(f_tuned, f_static)

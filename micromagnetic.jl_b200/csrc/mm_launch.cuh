@@ -89,7 +89,8 @@ template <class K>
 cudaError_t launch_many(const void* args_dev, const int* begins_dev, int n, int blocks, size_t smem, cudaStream_t st) {
   if (smem > 48 * 1024) smem_optin(reinterpret_cast<const void*>(&k_many<K>));
   // an ordinary launch: with the programmatic attribute the merged NEB batch
-  // (32 images of 128 x 128, 16 launches a step) took 0.42 ms a step, not 0.36
+  // (32 images of 128 x 128, 16 launches a step) took 0.42 ms a step against
+  // 0.36 in paired runs (that batch also varies between the two run to run)
   k_many<K><<<blocks, K::kNT, smem, st>>>(static_cast<const typename K::Args*>(args_dev), begins_dev, n);
   return cudaGetLastError();
 }

@@ -44,7 +44,7 @@ template <int Q, int W> constexpr int x_smem() {
 }
 
 // Warps of an x-pass block: the FP32 forward pass runs 4 (128 registers,
-// four blocks an SM), the inverse pass 8 (three blocks an SM), which moves
+// four blocks an SM), the inverse pass 8 (128 registers, two blocks an SM), which moves
 // column segments of RB = 8 rows (64 bytes for Q = 32).  Measured on c5
 // (1024 x 1024 x 16, Q = 32): forward 0.248 ms with 4 warps, 0.273 with 8
 // (0.287 with 4 capped at 96 registers); inverse 0.287 ms with 4 warps, 0.273
@@ -53,7 +53,9 @@ template <int Q, int W> constexpr int x_smem() {
 template <typename R> constexpr int x_fwd_warps() { return 4; }
 template <typename R> constexpr int x_inv_warps() { return sizeof(R) == 4 ? 8 : 4; }
 template <typename R, int W> constexpr int x_fwd_minb() { return sizeof(R) == 4 ? 4 : 2; }
-template <typename R, int W> constexpr int x_inv_minb() { return sizeof(R) == 4 ? 24 / W : 2; }
+// two blocks an SM: the FP32 inverse pass capped at 80 registers (three
+// blocks) spilled, and took 0.258 ms on c5 against 0.200 with 128 registers
+template <typename R, int W> constexpr int x_inv_minb() { return 2; }
 
 // ---------------------------------------------------------------- x forward
 // Rows of m * mu0Ms (zero padded to Px = 2 Lc) -> X column-major.  A block
